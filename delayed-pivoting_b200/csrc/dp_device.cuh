@@ -1,0 +1,85 @@
+// Device-side building blocks shared by every kernel of the delayed-pivoting
+// LU: index helpers, the per-factorisation state block that keeps all pivot
+// decisions on the device, and bounded spin waits.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dp {
+
+// Status codes shared by kernels and host (values of the C ABI).
+enum : int {
+  kOk = 0,
+  kInvalidArgument = 1,
+  kAllocationFailed = 2,
+  kCudaFailure = 3,
+  kLibraryFailure = 4,  // reference name: cublas_failure
+  kDeviceTimeout = 5,   // a bounded device wait gave up
+};
+
+__host__ __device__ inline size_t idx(long long row, long long col, long long ld) {
+  return static_cast<size_t>(row) + static_cast<size_t>(col) * static_cast<size_t>(ld);
+}
+
+// One pivot candidate of the full (2-D) search.  Ordering follows the
+// reference (delayed_lu_cuda/delayed_dgetrf_cuda.cu:13-20): larger magnitude
+// wins; equal magnitudes go to the earlier element in column-major order
+// (smaller column, then smaller row); NaN never wins.
+struct Cand {
+  double val;
+  int row;
+  int col;
+};
+
+__device__ __forceinline__ bool cand_better(const Cand& a, const Cand& b) {
+  // true iff a beats b
+  if (a.val > b.val) return true;
+  if (a.val == b.val) {
+    if (a.col != b.col) return a.col < b.col;
+    return a.row < b.row;
+  }
+  return false;
+}
+
+// Device-resident state of one factorisation.  Written by kernels, read by
+// the host once per panel (a few bytes) or once per fallback.
+struct State {
+  int status;      // kOk or an error code (e.g. kDeviceTimeout)
+  int stop_k;      // panel stopped at this step (no acceptable column pivot), -1 if not
+  int swap_count;  // number of (dst, src) pairs below the panel in the swap list
+  int block_changed;  // block rows [begin, end) whose content changed in the last panel
+  Cand fallback;   // result of the last 2-D / column-fallback search
+  unsigned int search_done;  // last-block-done counter of the search kernels
+  unsigned int barrier_exit; // exit counter of the panel kernel
+  int pad1[2];
+};
+
+// Bounded wait: every spin in this library gives up after kSpinLimitNs of
+// wall time, records kDeviceTimeout in the state and lets the caller return.
+constexpr unsigned long long kSpinLimitNs = 4000000000ull;  // 4 s
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.volatile.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_volatile_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.volatile.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ int ld_volatile_i32(const int* p) {
+  int v;
+  asm volatile("ld.volatile.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+}  // namespace dp

@@ -1,0 +1,67 @@
+// Kernel parameter blocks and host-side launch wrappers of the
+// delayed-pivoting LU.  Internal to the library (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "dp_device.cuh"
+
+namespace dp {
+
+struct PanelParams {
+  double* a;
+  long long lda;
+  int m;
+  int begin, end;     // panel columns [begin, end), rows [begin, m)
+  int rows_per_cta;   // R
+  int positioned;     // pivot of the first step already sits at (begin, begin)
+  int parity;         // which of the two slot buffers this launch uses
+  int max_ctas;       // slot buffer stride
+  int w_max;          // row-data buffer stride - 1
+  double threshold;
+  int* ipiv;          // device swap history (global step index)
+  State* state;
+  unsigned long long* slots;  // [2][4][max_ctas][2] tagged words
+  double* xdata;              // [4][max_ctas][w_max + 1]
+  double* rowk;               // [4][w_max + 1]
+  int* swap_block;            // [end - begin]: source row of block row begin + i
+  int* swap_extra;            // [2 * (end - begin)]: (dst, src) pairs below `end`
+};
+
+__global__ void panel_factor_kernel(PanelParams p);
+constexpr int kPanelThreadsHost = 256;
+size_t panel_smem_bytes(int w, int rows_per_cta);
+
+// Applies the composite row permutation of one panel (swap list written by
+// panel_factor_kernel) to columns [c0, c1) and [c2, c3).
+void launch_laswp(double* a, long long lda, int begin, int nblock, const int* swap_block,
+                  const int* swap_extra, const State* state, int c0, int c1, int c2, int c3,
+                  cudaStream_t s);
+
+// B(w x nc) <- L^{-1} B, L unit lower (w x w) at a(r0, r0), B at a(r0, c0).
+void launch_trsm_unit_lower(double* a, long long lda, int r0, int w, int c0, int nc,
+                            cudaStream_t s);
+
+// C(M x N) -= A(M x K) * B(K x N); all three inside the same column-major
+// matrix (or any column-major operands).
+void launch_gemm_minus(int M, int N, int K, const double* A, long long lda, const double* B,
+                       long long ldb, double* C, long long ldc, cudaStream_t s);
+
+// Full-pivot search over a(k:m, k:n); result in state->fallback.
+void launch_search_active(const double* a, long long lda, int m, int n, int k, State* state,
+                          Cand* block_cands, int max_blocks, cudaStream_t s);
+
+// Column-fallback search (delayed_dgetrf_column.cpp:30-45): right-most column
+// j in (k, n) whose active part has a magnitude > threshold, and its argmax row.
+void launch_search_nonzero_column(const double* a, long long lda, int m, int n, int k,
+                                  double threshold, State* state, cudaStream_t s);
+
+// Swap full rows r1 <-> r2 over columns [0, n) and full columns c1 <-> c2 over
+// rows [0, m) (either may be a no-op when the indices are equal).
+void launch_swap_row(double* a, long long lda, int n, int r1, int r2, cudaStream_t s);
+void launch_swap_col(double* a, long long lda, int m, int c1, int c2, cudaStream_t s);
+
+void launch_identity_records(int* ipiv, int* jpiv, int count, cudaStream_t s);
+void launch_set_record(int* ipiv, int* jpiv, int k, int p, int q, cudaStream_t s);
+
+}  // namespace dp

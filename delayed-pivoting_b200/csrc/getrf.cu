@@ -1,0 +1,553 @@
+// Host driver of the delayed-pivoting LU and the library's entry points
+// (C++ drop-in symbols of delayed_lu_cuda/delayed_dgetrf_cuda.hpp and the
+// extern "C" ABI of include/delayed_pivoting_b200.h).
+//
+// Control flow follows delayed_lu/delayed_dgetrf.cpp:129-251 and its GPU twin
+// delayed_lu_cuda/delayed_dgetrf_cuda.cu:251-368, with the per-pivot work moved
+// to the device: one cooperative panel launch factors a whole panel (all
+// column searches, acceptance tests, swaps, scalings and rank-1 updates stay
+// on the GPU) and the host reads a 64-byte state block once per panel, where
+// the reference made 2 launches + a D2H copy + a stream sync per column.
+//   normal panel  : laswp (rows outside the panel) -> TRSM (U12) -> GEMM (A22)
+//   panel stopped at k (no acceptable column pivot, dgetrf.cpp:182-218):
+//                   laswp of the executed steps -> materialize far columns
+//                   (TRSM + GEMM of width k - begin) -> full or column
+//                   fallback search -> delay (info = k) or swap row/column and
+//                   restart the panel at k with the pivot in place.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <vector>
+
+#include "delayed_dgetrf_cuda.hpp"
+#include "delayed_pivoting_b200.h"
+#include "dp_device.cuh"
+#include "dp_kernels.h"
+
+namespace dp {
+
+namespace {
+
+constexpr int kDefaultNb = 64;
+constexpr int kMaxPanelWidth = 128;   // TRSM stages L11 (w x w) in shared memory
+constexpr int kDefaultPanelRows = 256;
+constexpr int kMaxSearchBlocks = 1024;
+
+struct DeviceInfo {
+  int sms = 0;
+  int smem_optin = 0;
+  bool ready = false;
+};
+
+std::mutex g_dev_mutex;
+DeviceInfo g_dev[64];
+
+int device_info(DeviceInfo& out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return kCudaFailure;
+  std::lock_guard<std::mutex> lock(g_dev_mutex);
+  DeviceInfo& d = g_dev[dev];
+  if (!d.ready) {
+    if (cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&d.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) !=
+            cudaSuccess)
+      return kCudaFailure;
+    if (cudaFuncSetAttribute(panel_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             d.smem_optin - 1024) != cudaSuccess)
+      return kCudaFailure;
+    d.ready = true;
+  }
+  out = d;
+  return kOk;
+}
+
+struct Options {
+  int nb = kDefaultNb;
+  double threshold = 0.0;
+  int policy = DP_POLICY_FULL_PIVOT;
+  int panel_rows = kDefaultPanelRows;
+};
+
+struct Workspace {
+  char* base = nullptr;
+  size_t bytes = 0;
+  State* state = nullptr;
+  int* d_ipiv = nullptr;
+  int* d_jpiv = nullptr;
+  unsigned long long* slots = nullptr;
+  double* xdata = nullptr;
+  double* rowk = nullptr;
+  int* swap_block = nullptr;
+  int* swap_extra = nullptr;
+  Cand* cands = nullptr;
+  int max_ctas = 0;
+  int w_max = 0;
+};
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Lays the workspace out from `base` (nullptr: only computes the size).
+size_t layout_workspace(Workspace& ws, char* base, int pivots, int max_ctas, int w_max) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off = align_up(off + bytes, 256);
+    return base ? base + at : nullptr;
+  };
+  ws.max_ctas = max_ctas;
+  ws.w_max = w_max;
+  ws.state = reinterpret_cast<State*>(take(sizeof(State)));
+  ws.d_ipiv = reinterpret_cast<int*>(take(sizeof(int) * (size_t)std::max(pivots, 1)));
+  ws.d_jpiv = reinterpret_cast<int*>(take(sizeof(int) * (size_t)std::max(pivots, 1)));
+  ws.slots = reinterpret_cast<unsigned long long*>(take(sizeof(unsigned long long) * 2 * 4 * max_ctas * 2));
+  ws.xdata = reinterpret_cast<double*>(take(sizeof(double) * 4 * (size_t)max_ctas * (w_max + 1)));
+  ws.rowk = reinterpret_cast<double*>(take(sizeof(double) * 4 * (size_t)(w_max + 1)));
+  ws.swap_block = reinterpret_cast<int*>(take(sizeof(int) * (size_t)w_max));
+  ws.swap_extra = reinterpret_cast<int*>(take(sizeof(int) * 2 * (size_t)w_max));
+  ws.cands = reinterpret_cast<Cand*>(take(sizeof(Cand) * kMaxSearchBlocks));
+  ws.base = base;
+  ws.bytes = off;
+  return off;
+}
+
+// Picks the panel kernel's CTA count G and rows per CTA R so that the R x w
+// slice fits in shared memory; narrows the panel when it cannot fit.
+bool plan_panel(int rows, int& w, int target_rows, const DeviceInfo& di, int& G, int& R) {
+  const size_t budget = (size_t)di.smem_optin - 1024;
+  while (w >= 1) {
+    const size_t fixed = 2 * (size_t)(w + 1) * sizeof(double) + 64;
+    const long long max_r = (long long)((budget - fixed) / ((size_t)w * sizeof(double) + sizeof(int)));
+    long long g = (rows + (long long)target_rows - 1) / target_rows;
+    g = std::max(1LL, std::min<long long>(g, di.sms));
+    long long r = (rows + g - 1) / g;
+    if (r > max_r) {
+      g = std::min<long long>(di.sms, (rows + max_r - 1) / max_r);
+      r = (rows + g - 1) / g;
+    }
+    if (r <= max_r) {
+      G = (int)((rows + r - 1) / r);  // every CTA owns at least one row
+      R = (int)r;
+      return true;
+    }
+    w /= 2;
+  }
+  return false;
+}
+
+#define DP_CHECK_CUDA(call)                       \
+  do {                                            \
+    if ((call) != cudaSuccess) return kCudaFailure; \
+  } while (0)
+
+int read_state(State& hs, const Workspace& ws, cudaStream_t st) {
+  DP_CHECK_CUDA(cudaMemcpyAsync(&hs, ws.state, sizeof(State), cudaMemcpyDeviceToHost, st));
+  DP_CHECK_CUDA(cudaStreamSynchronize(st));
+  return kOk;
+}
+
+// Optional per-kernel-family device timing (dp_stats_enable): CUDA events
+// around each launch group on the launching stream, read after the call's
+// final synchronisation, plus the algorithmic flops / bytes of each group.
+std::mutex g_stats_mutex;
+dp_kernel_stats g_stats;
+bool g_stats_on = false;
+
+struct Recorder {
+  struct Mark {
+    int fam;
+    cudaEvent_t e0, e1;
+    double flops, bytes;
+    int launches;
+  };
+  bool on = false;
+  cudaStream_t st = nullptr;
+  std::vector<Mark> marks;
+  int cur = -1;
+  explicit Recorder(cudaStream_t s) : st(s) {
+    std::lock_guard<std::mutex> lock(g_stats_mutex);
+    on = g_stats_on;
+  }
+  void begin(int fam) {
+    if (!on) return;
+    Mark mk{fam, nullptr, nullptr, 0.0, 0.0, 0};
+    cudaEventCreate(&mk.e0);
+    cudaEventCreate(&mk.e1);
+    cudaEventRecord(mk.e0, st);
+    marks.push_back(mk);
+    cur = (int)marks.size() - 1;
+  }
+  void end(double flops, double bytes, int launches) {
+    if (!on || cur < 0) return;
+    Mark& mk = marks[cur];
+    cudaEventRecord(mk.e1, st);
+    mk.flops = flops;
+    mk.bytes = bytes;
+    mk.launches = launches;
+    cur = -1;
+  }
+  // Called after the stream has been synchronised.
+  void flush(bool ok) {
+    if (!on) return;
+    std::lock_guard<std::mutex> lock(g_stats_mutex);
+    for (Mark& mk : marks) {
+      float ms = 0.f;
+      if (ok && mk.e1 && cudaEventElapsedTime(&ms, mk.e0, mk.e1) == cudaSuccess) {
+        g_stats.ms[mk.fam] += ms;
+        g_stats.flops[mk.fam] += mk.flops;
+        g_stats.bytes[mk.fam] += mk.bytes;
+        g_stats.launches[mk.fam] += mk.launches;
+      }
+      cudaEventDestroy(mk.e0);
+      cudaEventDestroy(mk.e1);
+    }
+    if (ok) g_stats.calls += 1;
+    marks.clear();
+  }
+};
+
+double panel_flops(int m, int begin, int w) {
+  double f = 0.0;
+  for (int s = 0; s < w; ++s) {
+    const double below = (double)m - begin - s - 1;
+    if (below > 0) f += below * (2.0 * (w - s - 1) + 1.0);
+  }
+  return f;
+}
+
+// U12 <- L11^{-1} A12 over columns [far, n), then A(r_gemm:m, far:n) -=
+// L(r_gemm:m, begin:begin+w) * U12 (finish_panel when r_gemm == far == end,
+// materialize_partial_panel when r_gemm == k, far == panel end).
+void trsm_and_gemm(double* a, long long lda, int m, int n, int begin, int w, int r_gemm, int far,
+                   cudaStream_t st, Recorder& rec) {
+  const int nc = n - far;
+  if (w <= 0 || nc <= 0) return;
+  if (w > 1) {
+    rec.begin(DP_KFAM_TRSM);
+    launch_trsm_unit_lower(a, lda, begin, w, far, nc, st);
+    rec.end((double)w * (w - 1) * nc, 8.0 * (0.5 * w * w + 2.0 * w * nc), 1);
+  }
+  const int M = m - r_gemm;
+  if (M <= 0) return;
+  rec.begin(DP_KFAM_GEMM);
+  launch_gemm_minus(M, nc, w, a + idx(r_gemm, begin, lda), lda, a + idx(begin, far, lda), lda,
+                    a + idx(r_gemm, far, lda), lda, st);
+  rec.end(2.0 * M * (double)nc * w, 8.0 * ((double)M * w + (double)w * nc + 2.0 * M * (double)nc), 1);
+}
+
+int factorize(int m, int n, double* a, long long lda, const Options& o, Workspace& ws,
+              const DeviceInfo& di, cudaStream_t st, int& info, Recorder& rec) {
+  const int pivots = std::min(m, n);
+  rec.begin(DP_KFAM_OTHER);
+  launch_identity_records(ws.d_ipiv, ws.d_jpiv, pivots, st);
+  rec.end(0.0, 8.0 * pivots, 1);
+  DP_CHECK_CUDA(cudaGetLastError());
+  info = pivots;
+  int begin = 0, parity = 0;
+  bool positioned = false;
+  State hs;
+  while (begin < pivots) {
+    int w = std::min(std::min(o.nb, ws.w_max), pivots - begin);
+    int G = 1, R = 1;
+    if (!plan_panel(m - begin, w, o.panel_rows, di, G, R)) return kInvalidArgument;
+    const int end = begin + w;
+
+    PanelParams pp;
+    pp.a = a;
+    pp.lda = lda;
+    pp.m = m;
+    pp.begin = begin;
+    pp.end = end;
+    pp.rows_per_cta = R;
+    pp.positioned = positioned ? 1 : 0;
+    pp.parity = parity;
+    pp.max_ctas = ws.max_ctas;
+    pp.w_max = ws.w_max;
+    pp.threshold = o.threshold;
+    pp.ipiv = ws.d_ipiv;
+    pp.state = ws.state;
+    pp.slots = ws.slots;
+    pp.xdata = ws.xdata;
+    pp.rowk = ws.rowk;
+    pp.swap_block = ws.swap_block;
+    pp.swap_extra = ws.swap_extra;
+    void* args[] = {&pp};
+    rec.begin(DP_KFAM_PANEL);
+    DP_CHECK_CUDA(cudaLaunchCooperativeKernel((const void*)panel_factor_kernel, G,
+                                              kPanelThreadsHost, args, panel_smem_bytes(w, R), st));
+    rec.end(panel_flops(m, begin, w), 16.0 * (double)(m - begin) * w, 1);
+    parity ^= 1;
+    if (int e = read_state(hs, ws, st)) return e;
+    if (hs.status != kOk) return hs.status;
+
+    const int stop = hs.stop_k;
+    rec.begin(DP_KFAM_LASWP);
+    launch_laswp(a, lda, begin, w, ws.swap_block, ws.swap_extra, ws.state, 0, begin, end, n, st);
+    rec.end(0.0, 16.0 * (double)(hs.block_changed + hs.swap_count) * (double)(n - w), 1);
+    if (stop < 0) {
+      trsm_and_gemm(a, lda, m, n, begin, w, end, end, st, rec);
+      DP_CHECK_CUDA(cudaGetLastError());
+      begin = end;
+      positioned = false;
+      continue;
+    }
+
+    // Stopped at k: dgetrf.cpp:182-218.
+    const int k = stop;
+    if (k > begin) trsm_and_gemm(a, lda, m, n, begin, k - begin, k, end, st, rec);
+    rec.begin(DP_KFAM_SEARCH);
+    if (o.policy == DP_POLICY_NONZERO_COLUMN)
+      launch_search_nonzero_column(a, lda, m, n, k, o.threshold, ws.state, st);
+    else
+      launch_search_active(a, lda, m, n, k, ws.state, ws.cands, kMaxSearchBlocks, st);
+    rec.end(0.0, 8.0 * (double)(m - k) * (double)(n - k), o.policy == DP_POLICY_NONZERO_COLUMN ? 2 : 1);
+    DP_CHECK_CUDA(cudaGetLastError());
+    if (int e = read_state(hs, ws, st)) return e;
+    if (hs.status != kOk) return hs.status;
+    const Cand c = hs.fallback;
+    if (!(c.val > o.threshold)) {
+      info = k;  // the whole active submatrix is delayed
+      break;
+    }
+    rec.begin(DP_KFAM_SWAP);
+    launch_set_record(ws.d_ipiv, ws.d_jpiv, k, c.row, c.col, st);
+    launch_swap_row(a, lda, n, k, c.row, st);
+    launch_swap_col(a, lda, m, k, c.col, st);
+    rec.end(0.0, 32.0 * ((c.row != k ? (double)n : 0.0) + (c.col != k ? (double)m : 0.0)),
+            1 + (c.row != k) + (c.col != k));
+    DP_CHECK_CUDA(cudaGetLastError());
+    begin = k;
+    positioned = true;
+  }
+  return kOk;
+}
+
+bool matrix_byte_count(int lda, int n, size_t& bytes) {
+  const size_t cols = (size_t)n, ld = (size_t)lda;
+  if (cols != 0 && ld > std::numeric_limits<size_t>::max() / cols) return false;
+  const size_t el = ld * cols;
+  if (el > std::numeric_limits<size_t>::max() / sizeof(double)) return false;
+  bytes = el * sizeof(double);
+  return true;
+}
+
+// delayed_lu_cuda/delayed_dgetrf_cuda.cu:385-397
+bool valid_arguments(int m, int n, const double* a, int lda, const int* ipiv, const int* jpiv) {
+  if (m < 0 || n < 0 || lda < std::max(1, m)) return false;
+  const int pivots = std::min(m, n);
+  if ((m > 0 && n > 0 && a == nullptr) || (pivots > 0 && (ipiv == nullptr || jpiv == nullptr)))
+    return false;
+  size_t ignored = 0;
+  return matrix_byte_count(lda, n, ignored);
+}
+
+bool resolve_options(const dp_options* in, Options& o) {
+  if (!in) return true;
+  if (in->nb < 0 || in->panel_rows < 0) return false;
+  if (!(in->threshold >= 0.0)) return false;  // rejects NaN and negatives
+  if (in->policy != DP_POLICY_FULL_PIVOT && in->policy != DP_POLICY_NONZERO_COLUMN) return false;
+  o.nb = in->nb ? std::min(in->nb, kMaxPanelWidth) : kDefaultNb;
+  o.threshold = in->threshold;
+  o.policy = in->policy;
+  o.panel_rows = in->panel_rows ? in->panel_rows : kDefaultPanelRows;
+  return true;
+}
+
+}  // namespace
+
+int getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* info,
+                 cudaStream_t st, const dp_options* opt) {
+  if (info == nullptr) return kInvalidArgument;
+  *info = -1;
+  Options o;
+  if (!valid_arguments(m, n, d_a, lda, ipiv, jpiv) || !resolve_options(opt, o))
+    return kInvalidArgument;
+  const int pivots = std::min(m, n);
+  *info = pivots;
+  for (int k = 0; k < pivots; ++k) ipiv[k] = jpiv[k] = k;
+  if (pivots == 0) return kOk;
+
+  DeviceInfo di;
+  if (device_info(di) != kOk) {
+    *info = -1;
+    return kCudaFailure;
+  }
+  Workspace ws;
+  const int w_max = kMaxPanelWidth;
+  const size_t bytes = layout_workspace(ws, nullptr, pivots, di.sms, w_max);
+  char* base = nullptr;
+  if (cudaMallocAsync(reinterpret_cast<void**>(&base), bytes, st) != cudaSuccess) {
+    cudaGetLastError();
+    *info = -1;
+    return kAllocationFailed;
+  }
+  layout_workspace(ws, base, pivots, di.sms, w_max);
+  int status = kOk;
+  if (cudaMemsetAsync(base, 0, bytes, st) != cudaSuccess) status = kCudaFailure;
+  int inf = pivots;
+  Recorder rec(st);
+  if (status == kOk) status = factorize(m, n, d_a, lda, o, ws, di, st, inf, rec);
+  if (status == kOk) {
+    if (cudaMemcpyAsync(ipiv, ws.d_ipiv, sizeof(int) * pivots, cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(jpiv, ws.d_jpiv, sizeof(int) * pivots, cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess)
+      status = kCudaFailure;
+  }
+  cudaFreeAsync(base, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && status == kOk) status = kCudaFailure;
+  rec.flush(status == kOk);
+  if (status != kOk) {
+    cudaGetLastError();
+    *info = -1;
+    return status;
+  }
+  *info = inf;
+  return kOk;
+}
+
+int getrf_host(int m, int n, double* a, int lda, int* ipiv, int* jpiv, int* info,
+               cudaStream_t st, const dp_options* opt) {
+  if (info == nullptr) return kInvalidArgument;
+  *info = -1;
+  if (!valid_arguments(m, n, a, lda, ipiv, jpiv)) return kInvalidArgument;
+  const int pivots = std::min(m, n);
+  if (pivots == 0) {  // delayed_dgetrf_cuda.cu:456-460
+    *info = 0;
+    return kOk;
+  }
+  size_t bytes = 0;
+  if (!matrix_byte_count(lda, n, bytes)) return kInvalidArgument;
+  double* d_a = nullptr;
+  if (cudaMallocAsync(reinterpret_cast<void**>(&d_a), bytes, st) != cudaSuccess) {
+    cudaGetLastError();
+    return kAllocationFailed;
+  }
+  int status = kOk;
+  if (cudaMemcpyAsync(d_a, a, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) status = kCudaFailure;
+  if (status == kOk) status = getrf_device(m, n, d_a, lda, ipiv, jpiv, info, st, opt);
+  if (status == kOk) {
+    if (cudaMemcpyAsync(a, d_a, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+      *info = -1;
+      status = kCudaFailure;
+    }
+  }
+  cudaFreeAsync(d_a, st);
+  cudaStreamSynchronize(st);
+  if (status != kOk) cudaGetLastError();
+  return status;
+}
+
+}  // namespace dp
+
+// ---------------------------------------------------------------- C ABI ----
+extern "C" {
+
+void dp_options_init(dp_options* opt) {
+  if (!opt) return;
+  std::memset(opt, 0, sizeof(*opt));
+  opt->nb = 64;
+  opt->threshold = 0.0;
+  opt->policy = DP_POLICY_FULL_PIVOT;
+  opt->panel_rows = 0;
+}
+
+int dp_getrf_device_ex(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* info,
+                       void* stream, const dp_options* opt) {
+  return dp::getrf_device(m, n, d_a, lda, ipiv, jpiv, info, static_cast<cudaStream_t>(stream), opt);
+}
+
+int dp_getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* info,
+                    void* stream) {
+  return dp::getrf_device(m, n, d_a, lda, ipiv, jpiv, info, static_cast<cudaStream_t>(stream),
+                          nullptr);
+}
+
+int dp_getrf_host(int m, int n, double* a, int lda, int* ipiv, int* jpiv, int* info,
+                  void* stream) {
+  return dp::getrf_host(m, n, a, lda, ipiv, jpiv, info, static_cast<cudaStream_t>(stream), nullptr);
+}
+
+int dp_getrf_native_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* info,
+                           void* stream) {
+  return dp_getrf_device(m, n, d_a, lda, ipiv, jpiv, info, stream);
+}
+int dp_getrf_native_host(int m, int n, double* a, int lda, int* ipiv, int* jpiv, int* info,
+                         void* stream) {
+  return dp_getrf_host(m, n, a, lda, ipiv, jpiv, info, stream);
+}
+int dp_getrf_hybrid_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* info,
+                           void* stream) {
+  return dp_getrf_device(m, n, d_a, lda, ipiv, jpiv, info, stream);
+}
+int dp_getrf_hybrid_host(int m, int n, double* a, int lda, int* ipiv, int* jpiv, int* info,
+                         void* stream) {
+  return dp_getrf_host(m, n, a, lda, ipiv, jpiv, info, stream);
+}
+
+void dp_stats_enable(int on) {
+  std::lock_guard<std::mutex> lock(dp::g_stats_mutex);
+  dp::g_stats_on = on != 0;
+}
+
+void dp_stats_reset(void) {
+  std::lock_guard<std::mutex> lock(dp::g_stats_mutex);
+  std::memset(&dp::g_stats, 0, sizeof(dp::g_stats));
+}
+
+void dp_stats_get(dp_kernel_stats* out) {
+  if (!out) return;
+  std::lock_guard<std::mutex> lock(dp::g_stats_mutex);
+  *out = dp::g_stats;
+}
+
+const char* dp_status_string(int status) {
+  switch (status) {
+    case DP_SUCCESS: return "success";
+    case DP_INVALID_ARGUMENT: return "invalid argument";
+    case DP_ALLOCATION_FAILED: return "CUDA allocation failed";
+    case DP_CUDA_FAILURE: return "CUDA runtime failure";
+    case DP_LIBRARY_FAILURE: return "cuBLAS failure";
+    case DP_DEVICE_TIMEOUT: return "device wait timed out";
+  }
+  return "unknown status";
+}
+
+}  // extern "C"
+
+// ------------------------------------------------ C++ drop-in symbols ----
+namespace {
+DelayedGetrfCudaStatus to_status(int s) { return static_cast<DelayedGetrfCudaStatus>(s); }
+}  // namespace
+
+DelayedGetrfCudaStatus delayed_getrf_cuda_device(int m, int n, double* d_a, int lda, int* ipiv,
+                                                 int* jpiv, int& info, cudaStream_t stream) {
+  return to_status(dp::getrf_device(m, n, d_a, lda, ipiv, jpiv, &info, stream, nullptr));
+}
+DelayedGetrfCudaStatus delayed_getrf_cuda_host(int m, int n, double* a, int lda, int* ipiv,
+                                               int* jpiv, int& info, cudaStream_t stream) {
+  return to_status(dp::getrf_host(m, n, a, lda, ipiv, jpiv, &info, stream, nullptr));
+}
+DelayedGetrfCudaStatus delayed_getrf_cuda_native_device(int m, int n, double* d_a, int lda,
+                                                        int* ipiv, int* jpiv, int& info,
+                                                        cudaStream_t stream) {
+  return delayed_getrf_cuda_device(m, n, d_a, lda, ipiv, jpiv, info, stream);
+}
+DelayedGetrfCudaStatus delayed_getrf_cuda_native_host(int m, int n, double* a, int lda, int* ipiv,
+                                                      int* jpiv, int& info, cudaStream_t stream) {
+  return delayed_getrf_cuda_host(m, n, a, lda, ipiv, jpiv, info, stream);
+}
+DelayedGetrfCudaStatus delayed_getrf_cuda_hybrid_device(int m, int n, double* d_a, int lda,
+                                                        int* ipiv, int* jpiv, int& info,
+                                                        cudaStream_t stream) {
+  return delayed_getrf_cuda_device(m, n, d_a, lda, ipiv, jpiv, info, stream);
+}
+DelayedGetrfCudaStatus delayed_getrf_cuda_hybrid_host(int m, int n, double* a, int lda, int* ipiv,
+                                                      int* jpiv, int& info, cudaStream_t stream) {
+  return delayed_getrf_cuda_host(m, n, a, lda, ipiv, jpiv, info, stream);
+}
+const char* delayed_getrf_cuda_status_string(DelayedGetrfCudaStatus status) {
+  return dp_status_string(static_cast<int>(status));
+}

@@ -1,0 +1,321 @@
+// Panel factorisation of the delayed-pivoting LU on many SMs at once.
+//
+// Follows the inner loop of delayed_lu/delayed_dgetrf.cpp:164-240 (and its
+// GPU twin delayed_lu_cuda/delayed_dgetrf_cuda.cu:264-350) for the panel
+// columns [begin, end):
+//   column partial-pivot search (first index on ties, NaN never wins)
+//   acceptance test |alpha| > threshold (threshold 0 == the reference's
+//     `!(alpha > 0.0)`, delayed_dgetrf.cpp:178)
+//   row swap inside the panel columns (the rest of each row is swapped later
+//     by the laswp kernel from the swap list this kernel writes)
+//   scale by the reciprocal of the pivot (delayed_dgetrf.cpp:225-227)
+//   rank-1 update of the remaining panel columns (delayed_dgetrf.cpp:233-239)
+// When a column has no acceptable pivot the kernel stops at that step k,
+// records state->stop_k = k and leaves the fallback to the host driver.
+//
+// B200 layout: rows [begin, m) are split into G contiguous chunks of R rows,
+// one per CTA; each CTA keeps its R x w slice of the panel in shared memory
+// for the whole launch, so the panel crosses HBM once in and once out.  The
+// only cross-CTA traffic per column is one 16-byte candidate and one row of w
+// doubles, exchanged through L2 with tagged words (no atomics on the hot
+// path): every CTA publishes its local argmax, every CTA reads all G
+// candidates and reaches the same decision.  Launched cooperatively so all G
+// CTAs are co-resident; every wait is bounded (kSpinLimitNs).
+#include "dp_device.cuh"
+#include "dp_kernels.h"
+
+namespace dp {
+
+namespace {
+
+constexpr int kPanelThreads = 256;
+constexpr int kSlots = 4;  // exchange slots, indexed by step mod 4
+
+struct __align__(16) Best {
+  double val;
+  int row;  // local row, -1 when none
+  int pad;
+};
+
+__device__ __forceinline__ Best best_of(Best a, Best b) {
+  // larger value wins; ties (and equal values) go to the smaller row; a
+  // candidate with row -1 never wins against a real one of equal value.
+  if (b.row < 0) return a;
+  if (a.row < 0) return b;
+  if (b.val > a.val) return b;
+  if (b.val == a.val && b.row < a.row) return b;
+  return a;
+}
+
+__device__ __forceinline__ Best warp_best(Best v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    Best o;
+    o.val = __shfl_down_sync(0xffffffffu, v.val, off);
+    o.row = __shfl_down_sync(0xffffffffu, v.row, off);
+    o.pad = 0;
+    v = best_of(v, o);
+  }
+  return v;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kPanelThreads, 1)
+panel_factor_kernel(PanelParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int w = p.end - p.begin;
+  const int R = p.rows_per_cta;
+  const int G = gridDim.x;
+  const int cta = blockIdx.x;
+  const int tid = threadIdx.x;
+  const long long row0 = (long long)p.begin + (long long)cta * R;  // global row of local row 0
+  const int rows_here = (int)min((long long)R, (long long)p.m - row0);
+
+  double* sm = reinterpret_cast<double*>(smem_raw);   // [w][R]
+  double* prow = sm + (size_t)w * R;                  // [w + 1] pivot row (+orig)
+  double* krow = prow + (w + 1);                      // [w + 1] old row k (+orig)
+  int* orig = reinterpret_cast<int*>(krow + (w + 1));  // [R] source row of each local row
+  __shared__ Best red[kPanelThreads / 32];
+  __shared__ int s_flag[4];  // 0: winner row (global), 1: stop, 2: winner cta, 3: abort
+
+  unsigned long long* slots = p.slots + (size_t)(p.parity & 1) * kSlots * p.max_ctas * 2;
+  double* xdata = p.xdata;  // [kSlots][max_ctas][w_max + 1]
+  double* rowk = p.rowk;    // [kSlots][w_max + 1]
+  const int xs = p.w_max + 1;
+
+  // Zero this CTA's share (slots cta, cta + G, ...) of the other slot buffer,
+  // which the next launch uses; no CTA of this launch reads it.
+  {
+    unsigned long long* other = p.slots + (size_t)((p.parity + 1) & 1) * kSlots * p.max_ctas * 2;
+    for (int c = cta; c < p.max_ctas; c += G) {
+      for (int i = tid; i < kSlots * 2; i += blockDim.x) {
+        const int q = i >> 1, word = i & 1;
+        other[((size_t)q * p.max_ctas + c) * 2 + word] = 0ull;
+      }
+    }
+  }
+  if (cta == 0 && tid == 0) {
+    p.state->stop_k = -1;
+    p.state->swap_count = 0;
+    p.state->block_changed = 0;
+    __threadfence();
+  }
+
+  // Load the panel slice.
+  for (int c = 0; c < w; ++c) {
+    const double* src = p.a + idx(row0, p.begin + c, p.lda);
+    for (int r = tid; r < rows_here; r += blockDim.x) sm[(size_t)c * R + r] = src[r];
+  }
+  for (int r = tid; r < rows_here; r += blockDim.x) orig[r] = (int)(row0 + r);
+  __syncthreads();
+
+  const int lane = tid & 31, warp = tid >> 5;
+  bool aborted = false;
+
+  for (int s = 0; s < w; ++s) {
+    const long long k = (long long)p.begin + s;
+    const int q = s & (kSlots - 1);
+    const unsigned long long tb = (unsigned long long)(((s >> 2) & 1) ^ 1);
+    const bool positioned = (s == 0) && p.positioned;
+    const int kl = (int)(k - row0);  // local index of row k (valid if 0 <= kl < rows_here)
+    const bool own_k = kl >= 0 && kl < rows_here;
+
+    // 1. local candidate over column s, rows >= k
+    Best mine;
+    mine.val = 0.0;
+    mine.row = -1;
+    mine.pad = 0;
+    if (positioned) {
+      if (own_k && tid == 0) {
+        mine.val = __longlong_as_double(0x7ff0000000000000ll);
+        mine.row = kl;
+      }
+    } else {
+      // strict '>' from an initial magnitude of 0: zeros and NaN never
+      // become candidates; the first of equal magnitudes stays.
+      const int rstart = max(0, kl);
+      const double* col = sm + (size_t)s * R;
+      for (int r = rstart + tid; r < rows_here; r += blockDim.x) {
+        const double v = fabs(col[r]);
+        if (v > mine.val) {
+          mine.val = v;
+          mine.row = r;
+        }
+      }
+    }
+    mine = warp_best(mine);
+    if (lane == 0) red[warp] = mine;
+    __syncthreads();
+    if (warp == 0) {
+      Best v = lane < (blockDim.x >> 5) ? red[lane] : Best{0.0, -1, 0};
+      v = warp_best(v);
+      if (lane == 0) red[0] = v;
+    }
+    __syncthreads();
+    const Best cb = red[0];
+
+    // 2. publish the candidate row (and row k if this CTA owns it)
+    double* xd = xdata + ((size_t)q * p.max_ctas + cta) * xs;
+    if (cb.row >= 0) {
+      for (int j = tid; j < w; j += blockDim.x) __stcg(xd + j, sm[(size_t)j * R + cb.row]);
+      if (tid == 0) __stcg(xd + w, (double)orig[cb.row]);
+    }
+    if (own_k) {
+      double* rk = rowk + (size_t)q * xs;
+      for (int j = tid; j < w; j += blockDim.x) __stcg(rk + j, sm[(size_t)j * R + kl]);
+      if (tid == 0) __stcg(rk + w, (double)orig[kl]);
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) {
+      const unsigned long long vbits =
+          cb.row >= 0 ? (unsigned long long)__double_as_longlong(cb.val) : 0ull;
+      const unsigned long long grow = cb.row >= 0 ? (unsigned long long)(row0 + cb.row) : 0x7fffffffull;
+      unsigned long long* mys = slots + ((size_t)q * p.max_ctas + cta) * 2;
+      st_volatile_u64(mys + 1, (grow << 1) | tb);
+      st_volatile_u64(mys + 0, (vbits << 1) | tb);
+    }
+
+    // 3. warp 0 gathers all G candidates (bounded wait) and picks the winner
+    if (warp == 0) {
+      unsigned long long best_bits = 0ull;
+      long long best_row = 0x7fffffffll;
+      bool have = false;
+      const unsigned long long t0 = globaltimer_ns();
+      bool timeout = false;
+      for (int i = lane; i < G; i += 32) {
+        const unsigned long long* sl = slots + ((size_t)q * p.max_ctas + i) * 2;
+        unsigned long long kv, kr;
+        unsigned int spins = 0;
+        while (true) {
+          kv = ld_volatile_u64(sl + 0);
+          kr = ld_volatile_u64(sl + 1);
+          if ((kv & 1ull) == tb && (kr & 1ull) == tb) break;
+          if (((++spins) & 1023u) == 0u) {
+            if (globaltimer_ns() - t0 > kSpinLimitNs || ld_volatile_i32(&p.state->status) != kOk) {
+              timeout = true;
+              break;
+            }
+          }
+        }
+        if (timeout) break;
+        const unsigned long long vb = kv >> 1;
+        const long long rr = (long long)(kr >> 1);
+        if (rr == 0x7fffffffll) continue;
+        if (!have || vb > best_bits || (vb == best_bits && rr < best_row)) {
+          best_bits = vb;
+          best_row = rr;
+          have = true;
+        }
+      }
+      const bool any_timeout = __any_sync(0xffffffffu, timeout);
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const unsigned long long ob = __shfl_down_sync(0xffffffffu, best_bits, off);
+        const long long orr = __shfl_down_sync(0xffffffffu, best_row, off);
+        const int oh = __shfl_down_sync(0xffffffffu, (int)have, off);
+        if (oh && (!have || ob > best_bits || (ob == best_bits && orr < best_row))) {
+          best_bits = ob;
+          best_row = orr;
+          have = true;
+        }
+      }
+      __threadfence();
+      if (lane == 0) {
+        if (any_timeout) {
+          atomicCAS(&p.state->status, kOk, kDeviceTimeout);
+          s_flag[3] = 1;
+        } else {
+          s_flag[3] = 0;
+        }
+        const double bv = __longlong_as_double((long long)best_bits);
+        s_flag[0] = (int)best_row;
+        s_flag[1] = (!positioned && !(have && bv > p.threshold)) ? 1 : 0;
+        s_flag[2] = (int)((best_row - p.begin) / R);
+      }
+    }
+    __syncthreads();
+    if (s_flag[3]) {
+      aborted = true;
+      break;
+    }
+    if (s_flag[1]) {
+      // no acceptable pivot in this column: stop at step k
+      if (cta == 0 && tid == 0) p.state->stop_k = (int)k;
+      break;
+    }
+    const long long prow_g = s_flag[0];
+    const int wcta = s_flag[2];
+    const int pl = (int)(prow_g - row0);
+    const bool own_p = pl >= 0 && pl < rows_here;
+
+    // 4. fetch the pivot row (and old row k for the owner of the pivot row)
+    {
+      // L2-only loads (ld.cg): the same slot was read four steps ago and a
+      // stale L1 line must not be served.
+      const double* src = xdata + ((size_t)q * p.max_ctas + wcta) * xs;
+      for (int j = tid; j <= w; j += blockDim.x) prow[j] = __ldcg(src + j);
+      if (own_p && prow_g != k) {
+        const double* rk = rowk + (size_t)q * xs;
+        for (int j = tid; j <= w; j += blockDim.x) krow[j] = __ldcg(rk + j);
+      }
+    }
+    __syncthreads();
+
+    // 5. swap rows k and p inside the panel columns
+    if (own_k) {
+      for (int j = tid; j < w; j += blockDim.x) sm[(size_t)j * R + kl] = prow[j];
+      if (tid == 0) orig[kl] = (int)prow[w];
+    }
+    if (own_p && prow_g != k) {
+      for (int j = tid; j < w; j += blockDim.x) sm[(size_t)j * R + pl] = krow[j];
+      if (tid == 0) orig[pl] = (int)krow[w];
+    }
+    // a positioned pivot was recorded by the fallback that placed it
+    if (cta == 0 && tid == 0 && !positioned) p.ipiv[k] = (int)prow_g;
+    __syncthreads();
+
+    // 6. scale the multipliers and update the rest of the panel
+    {
+      const double inv = 1.0 / prow[s];
+      const int rstart = max(0, kl + 1);
+      double* colc = sm + (size_t)s * R;
+      for (int r = rstart + tid; r < rows_here; r += blockDim.x) {
+        const double l = colc[r] * inv;
+        colc[r] = l;
+        for (int j = s + 1; j < w; ++j) sm[(size_t)j * R + r] -= l * prow[j];
+      }
+    }
+    __syncthreads();
+  }
+
+  // Write the slice back.
+  for (int c = 0; c < w; ++c) {
+    double* dst = p.a + idx(row0, p.begin + c, p.lda);
+    for (int r = tid; r < rows_here; r += blockDim.x) dst[r] = sm[(size_t)c * R + r];
+  }
+  if (aborted) return;
+
+  // Swap list: block rows [begin, end) record their source row; rows below
+  // `end` that received another row append (dst, src) pairs.
+  for (int r = tid; r < rows_here; r += blockDim.x) {
+    const long long g = row0 + r;
+    const int src = orig[r];
+    if (g < p.end) {
+      p.swap_block[g - p.begin] = src;
+      if (src != (int)g) atomicAdd(&p.state->block_changed, 1);
+    } else if (src != (int)g) {
+      const int slot = atomicAdd(&p.state->swap_count, 1);
+      p.swap_extra[2 * slot + 0] = (int)g;
+      p.swap_extra[2 * slot + 1] = src;
+    }
+  }
+}
+
+size_t panel_smem_bytes(int w, int rows_per_cta) {
+  return (size_t)w * rows_per_cta * sizeof(double) + 2 * (size_t)(w + 1) * sizeof(double) +
+         (size_t)((rows_per_cta + 3) & ~3) * sizeof(int);
+}
+
+}  // namespace dp

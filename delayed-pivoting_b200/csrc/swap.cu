@@ -1,0 +1,158 @@
+// Row and column permutation kernels of the delayed-pivoting LU.
+//
+// The reference swaps a full row (n elements, stride lda) and, on a fallback,
+// a full column (m elements) at every step (delayed_lu/delayed_dgetrf.cpp:202-209,
+// delayed_lu_cuda/delayed_dgetrf_cuda.cu:304-317).  Here the panel kernel
+// swaps rows only inside the panel columns and writes the composite
+// permutation of the whole panel as a list of (destination, source) rows;
+// laswp_kernel then moves, per column outside the panel, only the rows that
+// changed, once per panel: each warp owns one column, gathers every source
+// row into registers and scatters them to their destinations.  The block
+// part of the list (destinations begin..end-1) is contiguous, so those writes
+// are coalesced.  Full-row / full-column swaps of a fallback step are
+// separate grid-stride kernels.
+#include "dp_device.cuh"
+#include "dp_kernels.h"
+
+namespace dp {
+
+namespace {
+
+constexpr int kLaswpThreads = 256;
+constexpr int kMaxSwapEntries = 512;  // 2 * maximum panel width
+constexpr int kPerLane = kMaxSwapEntries / 32;
+
+__global__ void __launch_bounds__(kLaswpThreads)
+laswp_kernel(double* a, long long lda, int begin, int nblock, const int* swap_block,
+             const int* swap_extra, const State* state, int c0, int c1, int c2, int c3) {
+  __shared__ int s_dst[kMaxSwapEntries];
+  __shared__ int s_src[kMaxSwapEntries];
+  __shared__ int s_count;
+  const int tid = threadIdx.x;
+  const int nextra = min(state->swap_count, kMaxSwapEntries - nblock);
+  if (tid == 0) s_count = 0;
+  __syncthreads();
+  // keep only rows whose content changed (warp-aggregated compaction)
+  for (int base = 0; base < nblock + nextra; base += blockDim.x) {
+    const int i = base + tid;
+    int d = 0, sr = 0;
+    bool keep = false;
+    if (i < nblock) {
+      d = begin + i;
+      sr = swap_block[i];
+      keep = sr != d;
+    } else if (i < nblock + nextra) {
+      d = swap_extra[2 * (i - nblock)];
+      sr = swap_extra[2 * (i - nblock) + 1];
+      keep = sr != d;
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, keep);
+    int wbase = 0;
+    if ((tid & 31) == 0 && mask) wbase = atomicAdd(&s_count, __popc(mask));
+    wbase = __shfl_sync(0xffffffffu, wbase, 0);
+    if (keep) {
+      const int pos = wbase + __popc(mask & ((1u << (tid & 31)) - 1u));
+      s_dst[pos] = d;
+      s_src[pos] = sr;
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  const int total = s_count;
+  if (total == 0) return;
+
+  const int lane = tid & 31;
+  const int warps = blockDim.x >> 5;
+  const long long n1 = c1 - c0, ncols = n1 + (c3 - c2);
+  for (long long cid = (long long)blockIdx.x * warps + (tid >> 5); cid < ncols;
+       cid += (long long)gridDim.x * warps) {
+    const long long col = cid < n1 ? c0 + cid : c2 + (cid - n1);
+    double* ac = a + idx(0, col, lda);
+    double v[kPerLane];
+#pragma unroll
+    for (int j = 0; j < kPerLane; ++j) {
+      const int i = lane + 32 * j;
+      if (i < total) v[j] = ac[s_src[i]];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < kPerLane; ++j) {
+      const int i = lane + 32 * j;
+      if (i < total) ac[s_dst[i]] = v[j];
+    }
+    __syncwarp();
+  }
+}
+
+__global__ void swap_row_kernel(double* a, long long lda, int n, int r1, int r2) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    const double t = a[idx(r1, j, lda)];
+    a[idx(r1, j, lda)] = a[idx(r2, j, lda)];
+    a[idx(r2, j, lda)] = t;
+  }
+}
+
+__global__ void swap_col_kernel(double* a, long long lda, int m, int c1, int c2) {
+  double* x = a + idx(0, c1, lda);
+  double* y = a + idx(0, c2, lda);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double t = x[i];
+    x[i] = y[i];
+    y[i] = t;
+  }
+}
+
+__global__ void identity_records_kernel(int* ipiv, int* jpiv, int count) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    ipiv[i] = i;
+    jpiv[i] = i;
+  }
+}
+
+__global__ void set_record_kernel(int* ipiv, int* jpiv, int k, int p, int q) {
+  ipiv[k] = p;
+  jpiv[k] = q;
+}
+
+int grid_for(long long work, int threads, int cap) {
+  long long g = (work + threads - 1) / threads;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (int)g;
+}
+
+}  // namespace
+
+void launch_laswp(double* a, long long lda, int begin, int nblock, const int* swap_block,
+                  const int* swap_extra, const State* state, int c0, int c1, int c2, int c3,
+                  cudaStream_t s) {
+  const long long ncols = (long long)(c1 - c0) + (c3 - c2);
+  if (ncols <= 0 || nblock <= 0) return;
+  const int warps = kLaswpThreads / 32;
+  const int grid = grid_for(ncols, warps, 148 * 16);
+  laswp_kernel<<<grid, kLaswpThreads, 0, s>>>(a, lda, begin, nblock, swap_block, swap_extra,
+                                              state, c0, c1, c2, c3);
+}
+
+void launch_swap_row(double* a, long long lda, int n, int r1, int r2, cudaStream_t s) {
+  if (r1 == r2 || n <= 0) return;
+  swap_row_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(a, lda, n, r1, r2);
+}
+
+void launch_swap_col(double* a, long long lda, int m, int c1, int c2, cudaStream_t s) {
+  if (c1 == c2 || m <= 0) return;
+  swap_col_kernel<<<grid_for(m, 256, 148 * 8), 256, 0, s>>>(a, lda, m, c1, c2);
+}
+
+void launch_set_record(int* ipiv, int* jpiv, int k, int p, int q, cudaStream_t s) {
+  set_record_kernel<<<1, 1, 0, s>>>(ipiv, jpiv, k, p, q);
+}
+
+void launch_identity_records(int* ipiv, int* jpiv, int count, cudaStream_t s) {
+  if (count <= 0) return;
+  identity_records_kernel<<<grid_for(count, 256, 148 * 4), 256, 0, s>>>(ipiv, jpiv, count);
+}
+
+}  // namespace dp

@@ -1,0 +1,161 @@
+"""ctypes bindings of the C ABI (include/delayed_pivoting_b200.h)."""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent.parent
+_LIB_DIR = _PKG / "lib"
+
+SUCCESS, INVALID_ARGUMENT, ALLOCATION_FAILED, CUDA_FAILURE, LIBRARY_FAILURE, DEVICE_TIMEOUT = range(6)
+POLICY_FULL_PIVOT, POLICY_NONZERO_COLUMN = 0, 1
+
+_lib = None
+_gen = None
+
+
+class Options(ctypes.Structure):
+    """dp_options: panel width, acceptance threshold, fallback policy."""
+
+    _fields_ = [
+        ("nb", ctypes.c_int),
+        ("threshold", ctypes.c_double),
+        ("policy", ctypes.c_int),
+        ("panel_rows", ctypes.c_int),
+        ("reserved", ctypes.c_int * 4),
+    ]
+
+
+def library_path() -> Path:
+    return _LIB_DIR / "libdelayed_lu_b200.so"
+
+
+def lib() -> ctypes.CDLL:
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        path = library_path()
+        if not path.exists():
+            raise RuntimeError(f"CUDA library not built: {path} (run __graft_entry__.build())")
+        L = ctypes.CDLL(str(path))
+        ip = ctypes.POINTER(ctypes.c_int)
+        for name in ("dp_getrf_device", "dp_getrf_host", "dp_getrf_native_device",
+                     "dp_getrf_native_host", "dp_getrf_hybrid_device", "dp_getrf_hybrid_host"):
+            f = getattr(L, name)
+            f.restype = ctypes.c_int
+            f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ip, ip, ip,
+                          ctypes.c_void_p]
+        L.dp_getrf_device_ex.restype = ctypes.c_int
+        L.dp_getrf_device_ex.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                         ip, ip, ip, ctypes.c_void_p, ctypes.POINTER(Options)]
+        L.dp_status_string.restype = ctypes.c_char_p
+        L.dp_status_string.argtypes = [ctypes.c_int]
+        L.dp_options_init.restype = None
+        L.dp_options_init.argtypes = [ctypes.POINTER(Options)]
+        _lib = L
+    return _lib
+
+
+def matgen() -> ctypes.CDLL:
+    global _gen
+    if _gen is None:
+        path = _LIB_DIR / "libdp_matgen.so"
+        if not path.exists():
+            raise RuntimeError(f"generator library not built: {path}")
+        G = ctypes.CDLL(str(path))
+        G.dpgen_mt64_nth.restype = ctypes.c_uint64
+        G.dpgen_mt64_nth.argtypes = [ctypes.c_uint64, ctypes.c_int]
+        G.dpgen_normal_matrix.restype = None
+        G.dpgen_normal_matrix.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                          ctypes.c_longlong, ctypes.c_uint64]
+        G.dpgen_normal_vector.restype = None
+        G.dpgen_normal_vector.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_uint64]
+        G.dpgen_plant_columns.restype = ctypes.c_int
+        G.dpgen_plant_columns.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                          ctypes.c_longlong, ctypes.c_uint64, ctypes.c_int,
+                                          ctypes.c_double, ctypes.c_int, ctypes.c_void_p,
+                                          ctypes.c_void_p]
+        G.dpgen_uniform.restype = None
+        G.dpgen_uniform.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_uint64]
+        _gen = G
+    return _gen
+
+
+def _iptr(arr):
+    if arr is None:
+        return None
+    assert arr.dtype == np.int32 and arr.flags.c_contiguous
+    return arr.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def _dptr(x):
+    """Device pointer of a torch tensor, or an int address, or None."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    return x.data_ptr()
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def _call(name, m, n, a_ptr, lda, ipiv, jpiv, stream):
+    info = ctypes.c_int(-1)
+    st = getattr(lib(), name)(m, n, a_ptr, lda, _iptr(ipiv), _iptr(jpiv), ctypes.byref(info),
+                              _stream(stream))
+    return st, info.value
+
+
+def delayed_getrf_cuda_device(m, n, d_a, lda, ipiv, jpiv, stream=None):
+    """delayed_dgetrf_cuda.hpp:24 — d_a device memory (torch tensor / address),
+    ipiv/jpiv host int32 arrays of min(m,n).  Returns (status, info)."""
+    return _call("dp_getrf_device", m, n, _dptr(d_a), lda, ipiv, jpiv, stream)
+
+
+def delayed_getrf_cuda_host(m, n, a, lda, ipiv, jpiv, stream=None):
+    """delayed_dgetrf_cuda.hpp:35 — a is a host float64 array (Fortran order,
+    overwritten in place).  Returns (status, info)."""
+    ptr = None if a is None else a.ctypes.data
+    return _call("dp_getrf_host", m, n, ptr, lda, ipiv, jpiv, stream)
+
+
+def delayed_getrf_cuda_native_device(m, n, d_a, lda, ipiv, jpiv, stream=None):
+    return _call("dp_getrf_native_device", m, n, _dptr(d_a), lda, ipiv, jpiv, stream)
+
+
+def delayed_getrf_cuda_native_host(m, n, a, lda, ipiv, jpiv, stream=None):
+    return _call("dp_getrf_native_host", m, n, None if a is None else a.ctypes.data, lda, ipiv,
+                 jpiv, stream)
+
+
+def delayed_getrf_cuda_hybrid_device(m, n, d_a, lda, ipiv, jpiv, stream=None):
+    return _call("dp_getrf_hybrid_device", m, n, _dptr(d_a), lda, ipiv, jpiv, stream)
+
+
+def delayed_getrf_cuda_hybrid_host(m, n, a, lda, ipiv, jpiv, stream=None):
+    return _call("dp_getrf_hybrid_host", m, n, None if a is None else a.ctypes.data, lda, ipiv,
+                 jpiv, stream)
+
+
+def delayed_getrf_cuda_status_string(status: int) -> str:
+    return lib().dp_status_string(int(status)).decode()
+
+
+def getrf_device_ex(m, n, d_a, lda, ipiv, jpiv, stream=None, nb=64, threshold=0.0,
+                    policy=POLICY_FULL_PIVOT, panel_rows=0):
+    """dp_getrf_device_ex with explicit options.  Returns (status, info)."""
+    opt = Options()
+    lib().dp_options_init(ctypes.byref(opt))
+    opt.nb, opt.threshold, opt.policy, opt.panel_rows = nb, threshold, policy, panel_rows
+    info = ctypes.c_int(-1)
+    st = lib().dp_getrf_device_ex(m, n, _dptr(d_a), lda, _iptr(ipiv), _iptr(jpiv),
+                                  ctypes.byref(info), _stream(stream), ctypes.byref(opt))
+    return st, info.value

@@ -1,0 +1,106 @@
+/* C ABI of the B200 delayed-pivoting LU (libdelayed_lu_b200.so).
+ *
+ * Plain pointers and sizes only; `stream` is a cudaStream_t passed as void*
+ * (NULL = the legacy default stream).  Return values are status codes:
+ *   0 DP_SUCCESS, 1 DP_INVALID_ARGUMENT, 2 DP_ALLOCATION_FAILED,
+ *   3 DP_CUDA_FAILURE, 4 DP_LIBRARY_FAILURE (the reference's cublas_failure),
+ *   5 DP_DEVICE_TIMEOUT (a bounded device wait gave up).
+ * The codes equal the reference's DelayedGetrfCudaStatus values
+ * (delayed_lu_cuda/delayed_dgetrf_cuda.hpp:7-13) plus one.
+ *
+ * Matrix and record conventions are the reference's
+ * (delayed_lu_cuda/delayed_dgetrf_cuda.hpp:15-26): column-major, 0-based,
+ * in-place compact L\U, ipiv/jpiv are 0-based swap histories of min(m,n)
+ * entries in HOST memory, info = min(m,n) or the first delayed step, -1 on
+ * any failure.  Every entry point synchronises `stream` before returning.
+ */
+#ifndef DELAYED_PIVOTING_B200_H
+#define DELAYED_PIVOTING_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  DP_SUCCESS = 0,
+  DP_INVALID_ARGUMENT = 1,
+  DP_ALLOCATION_FAILED = 2,
+  DP_CUDA_FAILURE = 3,
+  DP_LIBRARY_FAILURE = 4,
+  DP_DEVICE_TIMEOUT = 5
+};
+
+enum { DP_POLICY_FULL_PIVOT = 0, DP_POLICY_NONZERO_COLUMN = 1 };
+
+/* Tuning and semantics knobs; dp_options_init() fills the defaults that
+ * reproduce the reference exactly (threshold 0, full-pivot fallback). */
+typedef struct dp_options {
+  int nb;            /* panel width (the reference fixes 64); 0 = automatic */
+  double threshold;  /* accept a pivot iff |alpha| > threshold; 0 = reference */
+  int policy;        /* DP_POLICY_FULL_PIVOT (delayed_getrf) or
+                        DP_POLICY_NONZERO_COLUMN (delayed_getrf_column) */
+  int panel_rows;    /* target rows per CTA in the panel kernel; 0 = automatic */
+  int reserved[4];
+} dp_options;
+
+void dp_options_init(dp_options *opt);
+
+/* Replaces delayed_getrf_cuda_device (delayed_lu_cuda/delayed_dgetrf_cuda.hpp:24-26,
+ * delayed_dgetrf_cuda.cu:403-447).  d_a is device memory. */
+int dp_getrf_device(int m, int n, double *d_a, int lda, int *ipiv, int *jpiv, int *info,
+                    void *stream);
+
+/* Replaces delayed_getrf_cuda_host (delayed_dgetrf_cuda.hpp:35-37,
+ * delayed_dgetrf_cuda.cu:449-488).  a is host memory. */
+int dp_getrf_host(int m, int n, double *a, int lda, int *ipiv, int *jpiv, int *info,
+                  void *stream);
+
+/* delayed_dgetrf_cuda.hpp:40-46 (native_*) and :55-61 (hybrid_*, which here
+ * run the same all-device path). */
+int dp_getrf_native_device(int m, int n, double *d_a, int lda, int *ipiv, int *jpiv, int *info,
+                           void *stream);
+int dp_getrf_native_host(int m, int n, double *a, int lda, int *ipiv, int *jpiv, int *info,
+                         void *stream);
+int dp_getrf_hybrid_device(int m, int n, double *d_a, int lda, int *ipiv, int *jpiv, int *info,
+                           void *stream);
+int dp_getrf_hybrid_host(int m, int n, double *a, int lda, int *ipiv, int *jpiv, int *info,
+                         void *stream);
+
+/* dp_getrf_device with explicit options (opt == NULL: defaults).  Also the
+ * column-fallback policy of delayed_lu/delayed_dgetrf_column.hpp:18. */
+int dp_getrf_device_ex(int m, int n, double *d_a, int lda, int *ipiv, int *jpiv, int *info,
+                       void *stream, const dp_options *opt);
+
+/* Per-kernel-family device timing (no reference counterpart; the reference
+ * only times whole calls with std::chrono, delayed_lu_cuda/benchmark.cu:54-57).
+ * When enabled, every call records CUDA events around each launch group on
+ * its stream and accumulates device milliseconds, launches and algorithmic
+ * flops / bytes per family. */
+enum {
+  DP_KFAM_PANEL = 0, /* panel factorisation (search, swap, scale, rank-1) */
+  DP_KFAM_LASWP = 1, /* row permutation of the columns outside the panel */
+  DP_KFAM_TRSM = 2,  /* U12 = L11^-1 A12 */
+  DP_KFAM_GEMM = 3,  /* A22 -= L21 U12 (FP64 DMMA) */
+  DP_KFAM_SEARCH = 4,/* fallback search over the active submatrix */
+  DP_KFAM_SWAP = 5,  /* fallback full-row / full-column swaps and records */
+  DP_KFAM_OTHER = 6, /* record initialisation */
+  DP_KFAM_COUNT = 8
+};
+typedef struct dp_kernel_stats {
+  double ms[8];
+  double flops[8];
+  double bytes[8];
+  long long launches[8];
+  long long calls;
+} dp_kernel_stats;
+void dp_stats_enable(int on);
+void dp_stats_reset(void);
+void dp_stats_get(dp_kernel_stats *out);
+
+/* delayed_dgetrf_cuda.hpp:63 (delayed_getrf_cuda_status_string). */
+const char *dp_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

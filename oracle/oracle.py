@@ -1,0 +1,185 @@
+"""Python access to the two CPU checkers of the delayed-pivoting LU.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU leg of bench.py, never by the product library.
+
+* ``oracle_getrf`` - the plain-C restatement (delayed_getrf_oracle.c) of
+  delayed_lu/delayed_dgetrf.cpp:129-251 and delayed_dgetrf_column.cpp:99-211,
+  with a panel width and an acceptance threshold.
+* ``ref_getrf`` / ``ref_getrf_column`` / ``ref_lapack_getrf`` - the reference's
+  own unmodified CPU sources compiled against SciPy's bundled OpenBLAS into
+  ``_ref/libref_delayed_lu.so`` by the Makefile beside this file.
+* ``residual`` - ||P A Q - Lbar Ubar||_F and ||A||_F of a compact factor, the
+  reconstruction check of delayed_lu_cuda/example.cu:24-80.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "liboracle_dp.so"
+REF_SO = HERE / "_ref" / "libref_delayed_lu.so"
+
+_or = None
+_ref = None
+
+
+def build(ref: bool = True) -> None:
+    """Compiles the oracle (and, when the reference tree exists, the reference)."""
+    targets = ["oracle"]
+    if ref and Path(os.environ.get("DP_REFERENCE", "/root/reference")).exists():
+        targets.append("ref")
+    env = dict(os.environ)
+    if "DP_REFERENCE" in os.environ:
+        env["REF"] = os.environ["DP_REFERENCE"]
+    subprocess.run(["make", "-s", "-C", str(HERE)] + targets, check=True, env=env)
+
+
+def _ip():
+    return ctypes.POINTER(ctypes.c_int)
+
+
+def oracle_lib() -> ctypes.CDLL:
+    global _or
+    if _or is None:
+        if not ORACLE_SO.exists():
+            raise RuntimeError(f"oracle not built: {ORACLE_SO}")
+        L = ctypes.CDLL(str(ORACLE_SO))
+        L.oracle_delayed_getrf.restype = ctypes.c_int
+        L.oracle_delayed_getrf.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                           ctypes.c_int, _ip(), _ip(), _ip(), ctypes.c_int,
+                                           ctypes.c_double, ctypes.c_int]
+        L.oracle_residual.restype = None
+        L.oracle_residual.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                      ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _ip(), _ip(),
+                                      ctypes.c_void_p, _ip(), _ip(), ctypes.c_void_p]
+        L.oracle_max_threads.restype = ctypes.c_int
+        _or = L
+    return _or
+
+
+def ref_available() -> bool:
+    return REF_SO.exists()
+
+
+def ref_lib() -> ctypes.CDLL:
+    global _ref
+    if _ref is None:
+        if not REF_SO.exists():
+            raise RuntimeError(f"reference CPU build missing: {REF_SO}")
+        L = ctypes.CDLL(str(REF_SO))
+        for name in ("ref_delayed_getrf", "ref_delayed_getrf_column"):
+            f = getattr(L, name)
+            f.restype = None
+            f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, _ip(), _ip(),
+                          _ip()]
+        L.ref_lapack_getrf.restype = None
+        L.ref_lapack_getrf.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                       _ip(), _ip()]
+        L.ref_set_threads.restype = None
+        L.ref_set_threads.argtypes = [ctypes.c_int]
+        L.ref_get_threads.restype = ctypes.c_int
+        _ref = L
+    return _ref
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def _check(a):
+    assert a.dtype == np.float64 and a.flags.f_contiguous
+
+
+def oracle_getrf(a: np.ndarray, m: int | None = None, n: int | None = None, nb: int = 64,
+                 threshold: float = 0.0, policy: int = 0):
+    """Factors `a` (Fortran float64, lda = a.shape[0]) in place.
+    Returns (ipiv, jpiv, info)."""
+    _check(a)
+    lda = a.shape[0]
+    m = lda if m is None else m
+    n = a.shape[1] if n is None else n
+    piv = max(min(m, n), 1)
+    ipiv = np.zeros(piv, dtype=np.int32)
+    jpiv = np.zeros(piv, dtype=np.int32)
+    info = ctypes.c_int(-1)
+    oracle_lib().oracle_delayed_getrf(m, n, a.ctypes.data, lda, _p(ipiv), _p(jpiv),
+                                      ctypes.byref(info), nb, threshold, policy)
+    k = min(m, n)
+    return ipiv[:k], jpiv[:k], info.value
+
+
+def _ref_call(name, a, m, n, threads):
+    _check(a)
+    lda = a.shape[0]
+    m = lda if m is None else m
+    n = a.shape[1] if n is None else n
+    L = ref_lib()
+    if threads is not None:
+        L.ref_set_threads(int(threads))
+    piv = max(min(m, n), 1)
+    ipiv = np.zeros(piv, dtype=np.int32)
+    jpiv = np.zeros(piv, dtype=np.int32)
+    info = ctypes.c_int(-1)
+    getattr(L, name)(m, n, a.ctypes.data, lda, _p(ipiv), _p(jpiv), ctypes.byref(info))
+    k = min(m, n)
+    return ipiv[:k], jpiv[:k], info.value
+
+
+def ref_getrf(a, m=None, n=None, threads=None):
+    """The reference's delayed_getrf (delayed_lu/delayed_dgetrf.cpp:129)."""
+    return _ref_call("ref_delayed_getrf", a, m, n, threads)
+
+
+def ref_getrf_column(a, m=None, n=None, threads=None):
+    """The reference's delayed_getrf_column (delayed_lu/delayed_dgetrf_column.cpp:99)."""
+    return _ref_call("ref_delayed_getrf_column", a, m, n, threads)
+
+
+def ref_lapack_getrf(a, m=None, n=None, threads=None):
+    """LAPACK dgetrf through the reference's wrapper (delayed_lu/lapack_dgetrf.cpp)."""
+    _check(a)
+    lda = a.shape[0]
+    m = lda if m is None else m
+    n = a.shape[1] if n is None else n
+    L = ref_lib()
+    if threads is not None:
+        L.ref_set_threads(int(threads))
+    piv = max(min(m, n), 1)
+    ipiv = np.zeros(piv, dtype=np.int32)
+    info = ctypes.c_int(-1)
+    L.ref_lapack_getrf(m, n, a.ctypes.data, lda, _p(ipiv), ctypes.byref(info))
+    return ipiv[:min(m, n)], info.value
+
+
+def residual(orig: np.ndarray, fac: np.ndarray, m: int, n: int, info: int, ipiv, jpiv):
+    """Returns (||P A Q - Lbar Ubar||_F, ||A||_F)."""
+    _check(orig)
+    _check(fac)
+    L = oracle_lib()
+    k = max(min(m, n), 1)
+    ip = np.zeros(k, dtype=np.int32)
+    jp = np.zeros(k, dtype=np.int32)
+    ip[:len(ipiv)] = ipiv
+    jp[:len(jpiv)] = jpiv
+    ro = np.zeros(max(m, 1), dtype=np.int32)
+    co = np.zeros(max(n, 1), dtype=np.int32)
+    work = np.zeros(max(m, 1) * L.oracle_max_threads(), dtype=np.float64)
+    out = np.zeros(2, dtype=np.float64)
+    L.oracle_residual(m, n, orig.ctypes.data, orig.shape[0], fac.ctypes.data, fac.shape[0],
+                      max(info, 0), _p(ip), _p(jp), out.ctypes.data, _p(ro), _p(co),
+                      work.ctypes.data)
+    return float(out[0]), float(out[1])
+
+
+def scaled_residual(orig, fac, m, n, info, ipiv, jpiv) -> float:
+    """||PAQ - LU||_F / (||A||_F * max(m,n) * u), the acceptance metric (<= 10)."""
+    r, an = residual(orig, fac, m, n, info, ipiv, jpiv)
+    if an == 0.0:
+        return 0.0 if r == 0.0 else float("inf")
+    return r / (an * max(m, n) * np.finfo(np.float64).eps / 2)

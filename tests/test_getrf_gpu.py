@@ -1,0 +1,190 @@
+"""GPU parity tests of the delayed-pivoting LU through the C ABI.
+
+Records (ipiv, jpiv, info) must equal the reference's bit for bit (golden
+fixtures from its own CPU code, tests/golden/); the factor must satisfy
+||PAQ - LU||_F / (||A||_F * max(m,n) * u) <= 10.  Inputs that differ from the
+fixtures (threshold > 0, other panel widths) are checked against the oracle
+(oracle/delayed_getrf_oracle.c) on the same seeded input."""
+import numpy as np
+import pytest
+
+import golden_cases as gc
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def run_device(a, m, n, **opts):
+    """Factors a (host Fortran array) on the GPU through dp_getrf_device[_ex];
+    returns (factor (host), ipiv, jpiv, info, status)."""
+    import delayed_pivoting as dp
+
+    torch = _torch()
+    lda = a.shape[0]
+    d = torch.from_numpy(a.T.copy()).cuda()  # (n, lda) row-major == column-major lda x n
+    k = max(min(m, n), 1)
+    ipiv = np.full(k, -7, dtype=np.int32)
+    jpiv = np.full(k, -7, dtype=np.int32)
+    if opts:
+        st, info = dp.getrf_device_ex(m, n, d, lda, ipiv, jpiv, **opts)
+    else:
+        st, info = dp.delayed_getrf_cuda_device(m, n, d, lda, ipiv, jpiv)
+    torch.cuda.synchronize()
+    fac = np.asfortranarray(d.cpu().numpy().T)
+    kk = min(m, n)
+    return fac, ipiv[:kk], jpiv[:kk], info, st
+
+
+@pytest.mark.parametrize("name", gc.names(max_elems=4096 * 4096))
+def test_records_match_reference(built, name):
+    import oracle as orc
+
+    a, case = gc.load(name)
+    m, n = case["m"], case["n"]
+    opts = {"policy": case["policy"]} if case["policy"] else {}
+    fac, ipiv, jpiv, info, st = run_device(a, m, n, **opts)
+    assert st == 0
+    assert info == case["info"]
+    np.testing.assert_array_equal(ipiv, case["ipiv"])
+    np.testing.assert_array_equal(jpiv, case["jpiv"])
+    assert orc.scaled_residual(a, fac, m, n, info, ipiv, jpiv) <= 10.0
+    if case["lda"] > m:  # padding rows below m are never touched
+        np.testing.assert_array_equal(fac[m:, :], a[m:, :])
+
+
+def test_delayed_block_is_exactly_zero(built):
+    a, case = gc.load("config1_n1024")
+    fac, ipiv, jpiv, info, st = run_device(a, 1024, 1024)
+    assert st == 0 and info == 1020
+    assert np.all(fac[info:, info:] == 0.0)
+
+
+@pytest.mark.parametrize("nb", [1, 8, 32, 100, 128])
+def test_panel_width_does_not_change_records(built, nb):
+    import oracle as orc
+
+    a, case = gc.load("square_2000_zero20")
+    fac, ipiv, jpiv, info, st = run_device(a, 2000, 2000, nb=nb)
+    assert st == 0 and info == case["info"]
+    np.testing.assert_array_equal(ipiv, case["ipiv"])
+    np.testing.assert_array_equal(jpiv, case["jpiv"])
+    assert orc.scaled_residual(a, fac, 2000, 2000, info, ipiv, jpiv) <= 10.0
+
+
+@pytest.mark.parametrize("rows", [1, 7, 64, 1000])
+def test_panel_cta_split_does_not_change_records(built, rows):
+    a, case = gc.load("square_517_lda520")
+    _, ipiv, jpiv, info, st = run_device(a, 517, 517, panel_rows=rows)
+    assert st == 0 and info == case["info"]
+    np.testing.assert_array_equal(ipiv, case["ipiv"])
+    np.testing.assert_array_equal(jpiv, case["jpiv"])
+
+
+@pytest.mark.parametrize("thr", [1e-14, 1e-9])
+def test_threshold_matches_oracle(built, thr):
+    import oracle as orc
+
+    a, _ = gc.load("config1_n1024")
+    o = a.copy(order="F")
+    oi, oj, oinfo = orc.oracle_getrf(o, threshold=thr)
+    fac, ipiv, jpiv, info, st = run_device(a, 1024, 1024, threshold=thr)
+    assert st == 0 and info == oinfo == 1004
+    np.testing.assert_array_equal(ipiv, oi)
+    np.testing.assert_array_equal(jpiv, oj)
+    assert np.abs(fac[info:, info:]).max() <= thr
+
+
+@pytest.mark.parametrize("name", ["ref_dense_4x4", "ref_far_pivot_70", "tall_300x200",
+                                  "wide_150x260"])
+@pytest.mark.parametrize("entry", ["delayed_getrf_cuda_host", "delayed_getrf_cuda_native_host",
+                                   "delayed_getrf_cuda_hybrid_host"])
+def test_host_entry_points(built, name, entry):
+    import delayed_pivoting as dp
+    import oracle as orc
+
+    _torch()
+    a, case = gc.load(name)
+    m, n = case["m"], case["n"]
+    f = a.copy(order="F")
+    k = min(m, n)
+    ipiv = np.zeros(k, dtype=np.int32)
+    jpiv = np.zeros(k, dtype=np.int32)
+    st, info = getattr(dp, entry)(m, n, f, case["lda"], ipiv, jpiv)
+    assert st == 0 and info == case["info"]
+    np.testing.assert_array_equal(ipiv, case["ipiv"])
+    np.testing.assert_array_equal(jpiv, case["jpiv"])
+    assert orc.scaled_residual(a, f, m, n, info, ipiv, jpiv) <= 10.0
+
+
+def test_device_aliases_and_user_stream(built):
+    import delayed_pivoting as dp
+
+    torch = _torch()
+    a, case = gc.load("square_517_lda520")
+    s = torch.cuda.Stream()
+    for entry in ("delayed_getrf_cuda_native_device", "delayed_getrf_cuda_hybrid_device"):
+        d = torch.from_numpy(a.T.copy()).cuda()
+        ipiv = np.zeros(517, dtype=np.int32)
+        jpiv = np.zeros(517, dtype=np.int32)
+        torch.cuda.synchronize()
+        st, info = getattr(dp, entry)(517, 517, d, 520, ipiv, jpiv, stream=s)
+        assert st == 0 and info == case["info"]
+        np.testing.assert_array_equal(ipiv, case["ipiv"])
+        np.testing.assert_array_equal(jpiv, case["jpiv"])
+
+
+def test_repeat_calls_are_deterministic(built):
+    a, _ = gc.load("square_2000_zero20")
+    f1 = run_device(a, 2000, 2000)[0]
+    f2 = run_device(a, 2000, 2000)[0]
+    np.testing.assert_array_equal(f1, f2)
+
+
+@pytest.mark.slow
+def test_config2_n16384_records_bit_identical(built):
+    """n = 16384, 16 tiny + 3 zero columns: records equal the reference's;
+    the residual is checked on the GPU (float64 products in torch)."""
+    import delayed_pivoting as dp
+
+    torch = _torch()
+    if "config2_n16384" not in gc.names():
+        pytest.skip("n=16384 fixture not generated")
+    a, case = gc.load("config2_n16384")
+    n = 16384
+    d = torch.from_numpy(a.T.copy()).cuda()
+    orig = d.clone()
+    ipiv = np.zeros(n, dtype=np.int32)
+    jpiv = np.zeros(n, dtype=np.int32)
+    st, info = dp.delayed_getrf_cuda_device(n, n, d, n, ipiv, jpiv)
+    torch.cuda.synchronize()
+    assert st == 0 and info == case["info"]
+    np.testing.assert_array_equal(ipiv, case["ipiv"])
+    np.testing.assert_array_equal(jpiv, case["jpiv"])
+    assert scaled_residual_gpu(torch, orig, d, n, info, ipiv, jpiv) <= 10.0
+
+
+def scaled_residual_gpu(torch, orig_t, fac_t, n, info, ipiv, jpiv):
+    """Square case: tensors are (n, n) holding the column-major matrix transposed."""
+    F = fac_t.T  # column-major view -> actual matrix
+    A = orig_t.T
+    row = np.arange(n)
+    col = np.arange(n)
+    for k in range(info):
+        row[[k, ipiv[k]]] = row[[ipiv[k], k]]
+        col[[k, jpiv[k]]] = col[[jpiv[k], k]]
+    PAQ = A[torch.from_numpy(row).cuda()][:, torch.from_numpy(col).cuda()]
+    L = torch.tril(F, -1)
+    L[:, info:] = 0
+    L += torch.eye(n, dtype=F.dtype, device=F.device)
+    U = torch.triu(F)
+    U[info:, :] = 0
+    U[info:, info:] = F[info:, info:]
+    R = PAQ - L @ U
+    return float(torch.linalg.norm(R) / (torch.linalg.norm(A) * n * 2.0**-53))
