@@ -237,9 +237,11 @@ def main():
             raise RuntimeError(dp.delayed_getrf_cuda_status_string(st))
         return e0, e1, info
 
+    L.dp_stats_enable(1)  # warm-up also warms the library's event pool
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    L.dp_stats_enable(0)
     if dist:
         dist.barrier()
 

@@ -38,7 +38,9 @@ void launch_laswp(double* a, long long lda, int begin, int nblock, const int* sw
                   const int* swap_extra, const State* state, int c0, int c1, int c2, int c3,
                   cudaStream_t s);
 
-// B(w x nc) <- L^{-1} B, L unit lower (w x w) at a(r0, r0), B at a(r0, c0).
+// B(w x nc) <- L^{-1} B, L unit lower (w x w) at a(r0, r0), B at a(r0, c0);
+// w <= trsm_max_width().
+int trsm_max_width();
 void launch_trsm_unit_lower(double* a, long long lda, int r0, int w, int c0, int nc,
                             cudaStream_t s);
 

@@ -3,31 +3,24 @@
 // This is the O(n^3) work of the LU: finish_panel's dgemm
 // (delayed_lu/delayed_dgetrf.cpp:80-83, delayed_lu_cuda/delayed_dgetrf_cuda.cu:205-209)
 // and the far-column update of materialize_partial_panel (:120-123).  The
-// inner dimension K is the panel width (<= 256).
+// inner dimension K is the (outer) panel width.
 //
 // sm_100a has no FP64 kind of tcgen05.mma; the FP64 tensor path is
 // mma.sync.m16n8k4.f64 (measured at ~37 TFLOP/s on B200, the same rate as
-// DFMA).  CTA tile 128 x 128, 8 warps as 2 x 4, warp tile 64 x 32 (4 x 4
-// MMAs per k-step), K streamed in chunks of 32 through a 3-stage cp.async
-// pipeline into padded shared tiles (A k-major with stride 136, B n-major
-// with stride 36: both give conflict-free fragment loads).  The C tile is
-// prefetched into L2 when the CTA starts, so the read-modify-write in the
-// epilogue does not wait on HBM.  Accumulation is C - sum_k(a*b) with the
-// sum formed in FP64 by the tensor core.
+// DFMA).  A CTA computes a BM x BN tile with WARPS_M x WARPS_N warps, each
+// warp a (BM/WARPS_M) x (BN/WARPS_N) tile of 16x8 MMAs; K is streamed in
+// chunks of BK through a STAGES-deep cp.async pipeline into padded shared
+// tiles (A k-major with stride BM + 4, B n-major with stride BK + 4: both
+// give conflict-free fragment loads); fragments are double-buffered in
+// registers so shared-memory latency hides behind the previous k-step's MMAs.  The C tile is prefetched into L2 when
+// the CTA starts so the read-modify-write of the epilogue hits L2.
+// Accumulation is C - sum_k(a*b), the sum formed in FP64 by the tensor core.
 #include "dp_device.cuh"
 #include "dp_kernels.h"
 
 namespace dp {
 
-namespace {
-
-constexpr int BM = 128, BN = 128, BK = 32, STAGES = 3;
-constexpr int LDA_S = BM + 8;  // doubles; == 8 (mod 16)
-constexpr int LDB_S = BK + 4;  // doubles; == 4 (mod 16)
-constexpr int kGemmThreads = 256;
-constexpr int A_STAGE = BK * LDA_S;  // doubles
-constexpr int B_STAGE = BN * LDB_S;
-constexpr size_t kGemmSmem = (size_t)STAGES * (A_STAGE + B_STAGE) * sizeof(double);
+namespace gemm {
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
   const unsigned saddr = (unsigned)__cvta_generic_to_shared(smem);
@@ -49,131 +42,173 @@ __device__ __forceinline__ void mma_f64_16x8x4(double (&c)[4], double a0, double
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
-__global__ void __launch_bounds__(kGemmThreads, 1)
+template <int BM_, int BN_, int BK_, int STAGES_, int WARPS_M_, int WARPS_N_, int MINB_>
+struct Cfg {
+  static constexpr int BM = BM_, BN = BN_, BK = BK_, STAGES = STAGES_;
+  static constexpr int WARPS_M = WARPS_M_, WARPS_N = WARPS_N_, MINB = MINB_;
+  static constexpr int THREADS = 32 * WARPS_M * WARPS_N;
+  static constexpr int WTM = BM / WARPS_M, WTN = BN / WARPS_N;  // warp tile
+  static constexpr int MI = WTM / 16, NI = WTN / 8;
+  // A fragments are read by half-warps of (g = 0..3, t = 0..3) at t*LDA_S + g:
+  // LDA_S == 4 (mod 16) doubles puts the 16 lanes on 16 distinct 8-byte banks.
+  static constexpr int LDA_S = BM + 4;
+  static constexpr int LDB_S = BK + 4;  // == 4 (mod 16) doubles
+  static constexpr int A_STAGE = BK * LDA_S;
+  static constexpr int B_STAGE = BN * LDB_S;
+  static constexpr size_t SMEM = (size_t)STAGES * (A_STAGE + B_STAGE) * sizeof(double);
+  static_assert(BM % 16 == 0 && BN % 8 == 0 && WTM % 16 == 0 && WTN % 8 == 0, "tile");
+  static_assert((BM * BK) % THREADS == 0 && (BN * BK) % THREADS == 0, "loader");
+  static_assert(LDA_S % 16 == 4 && LDB_S % 16 == 4, "bank layout");
+};
+
+template <class C>
+__global__ void __launch_bounds__(C::THREADS, C::MINB)
 dgemm_minus_kernel(int M, int N, int K, const double* __restrict__ A, long long lda,
-                   const double* __restrict__ B, long long ldb, double* C, long long ldc) {
+                   const double* __restrict__ B, long long ldb, double* Cm, long long ldc) {
   extern __shared__ __align__(16) double gsm[];
-  double* As = gsm;                      // [STAGES][BK][LDA_S]
-  double* Bs = gsm + STAGES * A_STAGE;   // [STAGES][BN][LDB_S]
+  double* As = gsm;                         // [STAGES][BK][LDA_S]
+  double* Bs = gsm + C::STAGES * C::A_STAGE;  // [STAGES][BN][LDB_S]
 
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
-  const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warps
+  const int wm = warp / C::WARPS_N, wn = warp % C::WARPS_N;
   const int g = lane >> 2, t = lane & 3;
-  const long long m0 = (long long)blockIdx.x * BM;
-  const long long n0 = (long long)blockIdx.y * BN;
+  const long long m0 = (long long)blockIdx.x * C::BM;
+  const long long n0 = (long long)blockIdx.y * C::BN;
 
   // Prefetch this CTA's C tile into L2 (128-byte lines, in-bounds only).
   {
-    const int rows = (int)min((long long)BM, M - m0);
-    const int cols = (int)min((long long)BN, N - n0);
+    const int rows = (int)min((long long)C::BM, M - m0);
+    const int cols = (int)min((long long)C::BN, N - n0);
     const int lines_per_col = (rows * 8 + 127) / 128 + 1;
-    for (int e = tid; e < cols * lines_per_col; e += kGemmThreads) {
+    for (int e = tid; e < cols * lines_per_col; e += C::THREADS) {
       const int c = e / lines_per_col, l = e % lines_per_col;
       const int r = min(rows - 1, l * 16);
-      const double* p = C + idx(m0 + r, n0 + c, ldc);
+      const double* p = Cm + idx(m0 + r, n0 + c, ldc);
       asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
     }
   }
 
-  const int ktiles = (K + BK - 1) / BK;
+  const int ktiles = (K + C::BK - 1) / C::BK;
 
   auto load_stage = [&](int stage, int kt) {
-    double* as = As + stage * A_STAGE;
-    double* bs = Bs + stage * B_STAGE;
-    const int k0 = kt * BK;
+    double* as = As + stage * C::A_STAGE;
+    double* bs = Bs + stage * C::B_STAGE;
+    const int k0 = kt * C::BK;
 #pragma unroll
-    for (int i = 0; i < (BM * BK) / kGemmThreads; ++i) {
-      const int e = tid + i * kGemmThreads;
-      const int r = e % BM, kk = e / BM;
+    for (int i = 0; i < (C::BM * C::BK) / C::THREADS; ++i) {
+      const int e = tid + i * C::THREADS;
+      const int r = e % C::BM, kk = e / C::BM;
       const bool ok = (m0 + r < M) && (k0 + kk < K);
       const double* src = ok ? A + idx(m0 + r, k0 + kk, lda) : A;
-      cp_async8(as + kk * LDA_S + r, src, ok);
+      cp_async8(as + kk * C::LDA_S + r, src, ok);
     }
 #pragma unroll
-    for (int i = 0; i < (BN * BK) / kGemmThreads; ++i) {
-      const int e = tid + i * kGemmThreads;
-      const int kk = e % BK, c = e / BK;
+    for (int i = 0; i < (C::BN * C::BK) / C::THREADS; ++i) {
+      const int e = tid + i * C::THREADS;
+      const int kk = e % C::BK, c = e / C::BK;
       const bool ok = (n0 + c < N) && (k0 + kk < K);
       const double* src = ok ? B + idx(k0 + kk, n0 + c, ldb) : B;
-      cp_async8(bs + c * LDB_S + kk, src, ok);
+      cp_async8(bs + c * C::LDB_S + kk, src, ok);
     }
   };
 
-  double acc[4][4][4];
+  double acc[C::MI][C::NI][4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < C::MI; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < C::NI; ++j)
 #pragma unroll
       for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
 
 #pragma unroll
-  for (int s = 0; s < STAGES - 1; ++s) {
+  for (int s = 0; s < C::STAGES - 1; ++s) {
     if (s < ktiles) load_stage(s, s);
     cp_async_commit();
   }
 
   for (int kt = 0; kt < ktiles; ++kt) {
-    cp_async_wait<STAGES - 2>();
+    cp_async_wait<C::STAGES - 2>();
     __syncthreads();
     {
-      const int nk = kt + STAGES - 1;
-      if (nk < ktiles) load_stage(nk % STAGES, nk);
+      const int nk = kt + C::STAGES - 1;
+      if (nk < ktiles) load_stage(nk % C::STAGES, nk);
       cp_async_commit();
     }
-    const double* as = As + (kt % STAGES) * A_STAGE;
-    const double* bs = Bs + (kt % STAGES) * B_STAGE;
+    const double* as = As + (kt % C::STAGES) * C::A_STAGE;
+    const double* bs = Bs + (kt % C::STAGES) * C::B_STAGE;
+    double af[2][C::MI][2], bf[2][C::NI];
+    auto load_frag = [&](int buf, int kk) {
 #pragma unroll
-    for (int kk = 0; kk < BK; kk += 4) {
-      double af[4][2], bf[4];
-#pragma unroll
-      for (int mi = 0; mi < 4; ++mi) {
-        const double* ap = as + (kk + t) * LDA_S + wm * 64 + mi * 16 + g;
-        af[mi][0] = ap[0];
-        af[mi][1] = ap[8];
+      for (int mi = 0; mi < C::MI; ++mi) {
+        const double* ap = as + (kk + t) * C::LDA_S + wm * C::WTM + mi * 16 + g;
+        af[buf][mi][0] = ap[0];
+        af[buf][mi][1] = ap[8];
       }
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni) bf[ni] = bs[(wn * 32 + ni * 8 + g) * LDB_S + kk + t];
+      for (int ni = 0; ni < C::NI; ++ni)
+        bf[buf][ni] = bs[(wn * C::WTN + ni * 8 + g) * C::LDB_S + kk + t];
+    };
+    load_frag(0, 0);
 #pragma unroll
-      for (int mi = 0; mi < 4; ++mi)
+    for (int kk = 0; kk < C::BK; kk += 4) {
+      const int cur = (kk >> 2) & 1;
+      if (kk + 4 < C::BK) load_frag(cur ^ 1, kk + 4);
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni) mma_f64_16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+      for (int mi = 0; mi < C::MI; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < C::NI; ++ni)
+          mma_f64_16x8x4(acc[mi][ni], af[cur][mi][0], af[cur][mi][1], bf[cur][ni]);
     }
   }
   cp_async_wait<0>();
 
-  // Epilogue: C -= acc.
+  // Epilogue: C -= acc, one 16-row block at a time with all its loads issued
+  // before the first store.
 #pragma unroll
-  for (int mi = 0; mi < 4; ++mi) {
+  for (int mi = 0; mi < C::MI; ++mi) {
+    double old[C::NI][4];
 #pragma unroll
-    for (int ni = 0; ni < 4; ++ni) {
+    for (int ni = 0; ni < C::NI; ++ni)
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
-        const long long r = m0 + wm * 64 + mi * 16 + g + 8 * (v >> 1);
-        const long long c = n0 + wn * 32 + ni * 8 + 2 * t + (v & 1);
-        if (r < M && c < N) {
-          double* cp = C + idx(r, c, ldc);
-          *cp = *cp - acc[mi][ni][v];
-        }
+        const long long r = m0 + wm * C::WTM + mi * 16 + g + 8 * (v >> 1);
+        const long long c = n0 + wn * C::WTN + ni * 8 + 2 * t + (v & 1);
+        old[ni][v] = (r < M && c < N) ? Cm[idx(r, c, ldc)] : 0.0;
       }
-    }
+#pragma unroll
+    for (int ni = 0; ni < C::NI; ++ni)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const long long r = m0 + wm * C::WTM + mi * 16 + g + 8 * (v >> 1);
+        const long long c = n0 + wn * C::WTN + ni * 8 + 2 * t + (v & 1);
+        if (r < M && c < N) Cm[idx(r, c, ldc)] = old[ni][v] - acc[mi][ni][v];
+      }
   }
 }
 
-}  // namespace
+template <class C>
+void launch(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
+            double* Cm, long long ldc, cudaStream_t s) {
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(dgemm_minus_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)C::SMEM);
+    configured = true;
+  }
+  dim3 grid((M + C::BM - 1) / C::BM, (N + C::BN - 1) / C::BN);
+  dgemm_minus_kernel<C><<<grid, C::THREADS, C::SMEM, s>>>(M, N, K, A, lda, B, ldb, Cm, ldc);
+}
+
+// Production configuration: 128 x 128 tiles, 8 warps of 64 x 32.
+using Big = Cfg<128, 128, 32, 3, 2, 4, 1>;
+
+}  // namespace gemm
 
 void launch_gemm_minus(int M, int N, int K, const double* A, long long lda, const double* B,
                        long long ldb, double* C, long long ldc, cudaStream_t s) {
   if (M <= 0 || N <= 0 || K <= 0) return;
-  static bool configured = false;
-  if (!configured) {
-    cudaFuncSetAttribute(dgemm_minus_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)kGemmSmem);
-    configured = true;
-  }
-  dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
-  dgemm_minus_kernel<<<grid, kGemmThreads, kGemmSmem, s>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  gemm::launch<gemm::Big>(M, N, K, A, lda, B, ldb, C, ldc, s);
 }
 
 }  // namespace dp

@@ -15,6 +15,8 @@
 //                   fallback search -> delay (info = k) or swap row/column and
 //                   restart the panel at k with the pivot in place.
 #include <algorithm>
+#include <chrono>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <limits>
@@ -31,6 +33,7 @@ namespace dp {
 namespace {
 
 constexpr int kDefaultNb = 64;
+constexpr int kDefaultNbOuter = 256;
 constexpr int kMaxPanelWidth = 128;   // TRSM stages L11 (w x w) in shared memory
 constexpr int kDefaultPanelRows = 256;
 constexpr int kMaxSearchBlocks = 1024;
@@ -65,6 +68,7 @@ int device_info(DeviceInfo& out) {
 
 struct Options {
   int nb = kDefaultNb;
+  int nb_outer = kDefaultNbOuter;
   double threshold = 0.0;
   int policy = DP_POLICY_FULL_PIVOT;
   int panel_rows = kDefaultPanelRows;
@@ -141,9 +145,35 @@ bool plan_panel(int rows, int& w, int target_rows, const DeviceInfo& di, int& G,
     if ((call) != cudaSuccess) return kCudaFailure; \
   } while (0)
 
+// Host-side phase trace (environment variable DP_TRACE=1): accumulated wall
+// time spent waiting in read_state versus issuing work, printed per call.
+struct HostTrace {
+  bool on = false;
+  double wait_s = 0.0, total_s = 0.0;
+  long long waits = 0;
+  std::chrono::steady_clock::time_point t0;
+  HostTrace() {
+    const char* e = std::getenv("DP_TRACE");
+    on = e && e[0] == '1';
+    t0 = std::chrono::steady_clock::now();
+  }
+  ~HostTrace() {
+    if (!on) return;
+    total_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::fprintf(stderr, "[dp trace] call %.3f ms, %lld state reads waited %.3f ms\n",
+                 total_s * 1e3, waits, wait_s * 1e3);
+  }
+};
+thread_local HostTrace* g_trace = nullptr;
+
 int read_state(State& hs, const Workspace& ws, cudaStream_t st) {
+  const auto t = std::chrono::steady_clock::now();
   DP_CHECK_CUDA(cudaMemcpyAsync(&hs, ws.state, sizeof(State), cudaMemcpyDeviceToHost, st));
   DP_CHECK_CUDA(cudaStreamSynchronize(st));
+  if (g_trace && g_trace->on) {
+    g_trace->wait_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
+    g_trace->waits += 1;
+  }
   return kOk;
 }
 
@@ -153,6 +183,28 @@ int read_state(State& hs, const Workspace& ws, cudaStream_t st) {
 std::mutex g_stats_mutex;
 dp_kernel_stats g_stats;
 bool g_stats_on = false;
+
+// Events are recycled across calls (creating them per launch costs more
+// host time than the launches themselves).  Guarded by g_stats_mutex.
+std::vector<cudaEvent_t> g_event_pool;
+std::mutex g_pool_mutex;
+
+cudaEvent_t event_get() {
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  if (!g_event_pool.empty()) {
+    cudaEvent_t e = g_event_pool.back();
+    g_event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+void event_put(cudaEvent_t e) {
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  g_event_pool.push_back(e);
+}
 
 struct Recorder {
   struct Mark {
@@ -172,8 +224,8 @@ struct Recorder {
   void begin(int fam) {
     if (!on) return;
     Mark mk{fam, nullptr, nullptr, 0.0, 0.0, 0};
-    cudaEventCreate(&mk.e0);
-    cudaEventCreate(&mk.e1);
+    mk.e0 = event_get();
+    mk.e1 = event_get();
     cudaEventRecord(mk.e0, st);
     marks.push_back(mk);
     cur = (int)marks.size() - 1;
@@ -199,8 +251,8 @@ struct Recorder {
         g_stats.bytes[mk.fam] += mk.bytes;
         g_stats.launches[mk.fam] += mk.launches;
       }
-      cudaEventDestroy(mk.e0);
-      cudaEventDestroy(mk.e1);
+      event_put(mk.e0);
+      event_put(mk.e1);
     }
     if (ok) g_stats.calls += 1;
     marks.clear();
@@ -216,26 +268,61 @@ double panel_flops(int m, int begin, int w) {
   return f;
 }
 
-// U12 <- L11^{-1} A12 over columns [far, n), then A(r_gemm:m, far:n) -=
-// L(r_gemm:m, begin:begin+w) * U12 (finish_panel when r_gemm == far == end,
-// materialize_partial_panel when r_gemm == k, far == panel end).
-void trsm_and_gemm(double* a, long long lda, int m, int n, int begin, int w, int r_gemm, int far,
-                   cudaStream_t st, Recorder& rec) {
-  const int nc = n - far;
-  if (w <= 0 || nc <= 0) return;
-  if (w > 1) {
-    rec.begin(DP_KFAM_TRSM);
-    launch_trsm_unit_lower(a, lda, begin, w, far, nc, st);
-    rec.end((double)w * (w - 1) * nc, 8.0 * (0.5 * w * w + 2.0 * w * nc), 1);
+// Blocked forward substitution U <- L^{-1} A for rows [r0, r0 + W) and
+// columns [c0, c0 + nc), L unit lower at a(r0, r0); diagonal blocks of at
+// most trsm_max_width() are solved by the TRSM kernel, the blocks below them
+// by the GEMM kernel.
+void trsm_blocked(double* a, long long lda, int r0, int W, int c0, int nc, cudaStream_t st,
+                  Recorder& rec) {
+  if (W <= 1 || nc <= 0) return;
+  const int tw = trsm_max_width();
+  for (int b = 0; b < W; b += tw) {
+    const int wb = std::min(tw, W - b);
+    if (wb > 1) {
+      rec.begin(DP_KFAM_TRSM);
+      launch_trsm_unit_lower(a, lda, r0 + b, wb, c0, nc, st);
+      rec.end((double)wb * (wb - 1) * nc, 8.0 * (0.5 * wb * wb + 2.0 * wb * nc), 1);
+    }
+    const int rows_below = W - b - wb;
+    if (rows_below > 0) {
+      rec.begin(DP_KFAM_GEMM);
+      launch_gemm_minus(rows_below, nc, wb, a + idx(r0 + b + wb, r0 + b, lda), lda,
+                        a + idx(r0 + b, c0, lda), lda, a + idx(r0 + b + wb, c0, lda), lda, st);
+      rec.end(2.0 * rows_below * (double)nc * wb,
+              8.0 * ((double)rows_below * wb + (double)wb * nc + 2.0 * rows_below * (double)nc), 1);
+    }
   }
+}
+
+// Brings columns [c0, n_end) up to date with the eliminated steps
+// [s0, s0 + W): blocked TRSM on rows [s0, s0 + W), then
+// A(r_gemm:m, c0:n_end) -= L(r_gemm:m, s0:s0+W) * U(s0:s0+W, c0:n_end).
+void update_columns(double* a, long long lda, int m, int s0, int W, int r_gemm, int c0, int n_end,
+                    cudaStream_t st, Recorder& rec) {
+  const int nc = n_end - c0;
+  if (W <= 0 || nc <= 0) return;
+  trsm_blocked(a, lda, s0, W, c0, nc, st, rec);
   const int M = m - r_gemm;
   if (M <= 0) return;
   rec.begin(DP_KFAM_GEMM);
-  launch_gemm_minus(M, nc, w, a + idx(r_gemm, begin, lda), lda, a + idx(begin, far, lda), lda,
-                    a + idx(r_gemm, far, lda), lda, st);
-  rec.end(2.0 * M * (double)nc * w, 8.0 * ((double)M * w + (double)w * nc + 2.0 * M * (double)nc), 1);
+  launch_gemm_minus(M, nc, W, a + idx(r_gemm, s0, lda), lda, a + idx(s0, c0, lda), lda,
+                    a + idx(r_gemm, c0, lda), lda, st);
+  rec.end(2.0 * M * (double)nc * W, 8.0 * ((double)M * W + (double)W * nc + 2.0 * M * (double)nc), 1);
 }
 
+// Two-level blocked delayed LU.  An outer block [B, E) of width NB is
+// factored as a sequence of inner panels [b, e) of width nb (the panel
+// kernel); after each inner panel its row swaps are applied to every column
+// outside it and the rest of the outer block [e, E) is updated (rank nb);
+// the columns right of the outer block receive one rank-NB update when the
+// block completes.  When a panel stops at step k (no acceptable column
+// pivot) every column right of the stopped panel is brought up to date for
+// the steps [B, k) (delayed_dgetrf.cpp:183-186 materialize), the fallback
+// search runs on the true Schur complement A(k:m, k:n), and the factorisation
+// either delays from k (info = k) or swaps the chosen pivot to (k, k) and
+// restarts a new outer block at k with that pivot positioned
+// (delayed_dgetrf.cpp:188-218).  Block sizes only change rounding, never the
+// pivot decisions.
 int factorize(int m, int n, double* a, long long lda, const Options& o, Workspace& ws,
               const DeviceInfo& di, cudaStream_t st, int& info, Recorder& rec) {
   const int pivots = std::min(m, n);
@@ -244,66 +331,80 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
   rec.end(0.0, 8.0 * pivots, 1);
   DP_CHECK_CUDA(cudaGetLastError());
   info = pivots;
-  int begin = 0, parity = 0;
+  int B = 0, parity = 0;
   bool positioned = false;
   State hs;
-  while (begin < pivots) {
-    int w = std::min(std::min(o.nb, ws.w_max), pivots - begin);
-    int G = 1, R = 1;
-    if (!plan_panel(m - begin, w, o.panel_rows, di, G, R)) return kInvalidArgument;
-    const int end = begin + w;
+  const int NB = std::max(o.nb_outer, o.nb);
+  while (B < pivots) {
+    const int E = std::min(pivots, B + NB);
+    int b = B, e = B, stop = -1;
+    while (b < E) {
+      int w = std::min(std::min(o.nb, ws.w_max), E - b);
+      int G = 1, R = 1;
+      if (!plan_panel(m - b, w, o.panel_rows, di, G, R)) return kInvalidArgument;
+      e = b + w;
 
-    PanelParams pp;
-    pp.a = a;
-    pp.lda = lda;
-    pp.m = m;
-    pp.begin = begin;
-    pp.end = end;
-    pp.rows_per_cta = R;
-    pp.positioned = positioned ? 1 : 0;
-    pp.parity = parity;
-    pp.max_ctas = ws.max_ctas;
-    pp.w_max = ws.w_max;
-    pp.threshold = o.threshold;
-    pp.ipiv = ws.d_ipiv;
-    pp.state = ws.state;
-    pp.slots = ws.slots;
-    pp.xdata = ws.xdata;
-    pp.rowk = ws.rowk;
-    pp.swap_block = ws.swap_block;
-    pp.swap_extra = ws.swap_extra;
-    void* args[] = {&pp};
-    rec.begin(DP_KFAM_PANEL);
-    DP_CHECK_CUDA(cudaLaunchCooperativeKernel((const void*)panel_factor_kernel, G,
-                                              kPanelThreadsHost, args, panel_smem_bytes(w, R), st));
-    rec.end(panel_flops(m, begin, w), 16.0 * (double)(m - begin) * w, 1);
-    parity ^= 1;
-    if (int e = read_state(hs, ws, st)) return e;
-    if (hs.status != kOk) return hs.status;
-
-    const int stop = hs.stop_k;
-    rec.begin(DP_KFAM_LASWP);
-    launch_laswp(a, lda, begin, w, ws.swap_block, ws.swap_extra, ws.state, 0, begin, end, n, st);
-    rec.end(0.0, 16.0 * (double)(hs.block_changed + hs.swap_count) * (double)(n - w), 1);
-    if (stop < 0) {
-      trsm_and_gemm(a, lda, m, n, begin, w, end, end, st, rec);
-      DP_CHECK_CUDA(cudaGetLastError());
-      begin = end;
+      PanelParams pp;
+      pp.a = a;
+      pp.lda = lda;
+      pp.m = m;
+      pp.begin = b;
+      pp.end = e;
+      pp.rows_per_cta = R;
+      pp.positioned = positioned ? 1 : 0;
+      pp.parity = parity;
+      pp.max_ctas = ws.max_ctas;
+      pp.w_max = ws.w_max;
+      pp.threshold = o.threshold;
+      pp.ipiv = ws.d_ipiv;
+      pp.state = ws.state;
+      pp.slots = ws.slots;
+      pp.xdata = ws.xdata;
+      pp.rowk = ws.rowk;
+      pp.swap_block = ws.swap_block;
+      pp.swap_extra = ws.swap_extra;
+      void* args[] = {&pp};
+      rec.begin(DP_KFAM_PANEL);
+      DP_CHECK_CUDA(cudaLaunchCooperativeKernel((const void*)panel_factor_kernel, G,
+                                                kPanelThreadsHost, args, panel_smem_bytes(w, R),
+                                                st));
+      rec.end(panel_flops(m, b, w), 16.0 * (double)(m - b) * w, 1);
       positioned = false;
+      parity ^= 1;
+      if (int err = read_state(hs, ws, st)) return err;
+      if (hs.status != kOk) return hs.status;
+
+      rec.begin(DP_KFAM_LASWP);
+      launch_laswp(a, lda, b, w, ws.swap_block, ws.swap_extra, ws.state, 0, b, e, n, st);
+      rec.end(0.0, 16.0 * (double)(hs.block_changed + hs.swap_count) * (double)(n - w), 1);
+      if (hs.stop_k >= 0) {
+        stop = hs.stop_k;
+        break;
+      }
+      update_columns(a, lda, m, b, w, e, e, E, st, rec);  // rest of the outer block
+      DP_CHECK_CUDA(cudaGetLastError());
+      b = e;
+    }
+    if (stop < 0) {
+      update_columns(a, lda, m, B, E - B, E, E, n, st, rec);  // right of the outer block
+      DP_CHECK_CUDA(cudaGetLastError());
+      B = E;
       continue;
     }
 
-    // Stopped at k: dgetrf.cpp:182-218.
+    // Stopped at k inside panel [b, e): materialize, then search.
     const int k = stop;
-    if (k > begin) trsm_and_gemm(a, lda, m, n, begin, k - begin, k, end, st, rec);
+    update_columns(a, lda, m, b, k - b, k, e, E, st, rec);  // rest of the outer block
+    update_columns(a, lda, m, B, k - B, k, E, n, st, rec);  // right of the outer block
     rec.begin(DP_KFAM_SEARCH);
     if (o.policy == DP_POLICY_NONZERO_COLUMN)
       launch_search_nonzero_column(a, lda, m, n, k, o.threshold, ws.state, st);
     else
       launch_search_active(a, lda, m, n, k, ws.state, ws.cands, kMaxSearchBlocks, st);
-    rec.end(0.0, 8.0 * (double)(m - k) * (double)(n - k), o.policy == DP_POLICY_NONZERO_COLUMN ? 2 : 1);
+    rec.end(0.0, 8.0 * (double)(m - k) * (double)(n - k),
+            o.policy == DP_POLICY_NONZERO_COLUMN ? 2 : 1);
     DP_CHECK_CUDA(cudaGetLastError());
-    if (int e = read_state(hs, ws, st)) return e;
+    if (int err = read_state(hs, ws, st)) return err;
     if (hs.status != kOk) return hs.status;
     const Cand c = hs.fallback;
     if (!(c.val > o.threshold)) {
@@ -317,7 +418,7 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
     rec.end(0.0, 32.0 * ((c.row != k ? (double)n : 0.0) + (c.col != k ? (double)m : 0.0)),
             1 + (c.row != k) + (c.col != k));
     DP_CHECK_CUDA(cudaGetLastError());
-    begin = k;
+    B = k;
     positioned = true;
   }
   return kOk;
@@ -347,7 +448,9 @@ bool resolve_options(const dp_options* in, Options& o) {
   if (in->nb < 0 || in->panel_rows < 0) return false;
   if (!(in->threshold >= 0.0)) return false;  // rejects NaN and negatives
   if (in->policy != DP_POLICY_FULL_PIVOT && in->policy != DP_POLICY_NONZERO_COLUMN) return false;
+  if (in->nb_outer < 0) return false;
   o.nb = in->nb ? std::min(in->nb, kMaxPanelWidth) : kDefaultNb;
+  o.nb_outer = in->nb_outer ? in->nb_outer : std::max(kDefaultNbOuter, o.nb);
   o.threshold = in->threshold;
   o.policy = in->policy;
   o.panel_rows = in->panel_rows ? in->panel_rows : kDefaultPanelRows;
@@ -386,6 +489,8 @@ int getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* 
   int status = kOk;
   if (cudaMemsetAsync(base, 0, bytes, st) != cudaSuccess) status = kCudaFailure;
   int inf = pivots;
+  HostTrace trace;
+  g_trace = &trace;
   Recorder rec(st);
   if (status == kOk) status = factorize(m, n, d_a, lda, o, ws, di, st, inf, rec);
   if (status == kOk) {
@@ -398,6 +503,7 @@ int getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* 
   cudaFreeAsync(base, st);
   if (cudaStreamSynchronize(st) != cudaSuccess && status == kOk) status = kCudaFailure;
   rec.flush(status == kOk);
+  g_trace = nullptr;
   if (status != kOk) {
     cudaGetLastError();
     *info = -1;

@@ -113,6 +113,22 @@ panel_factor_kernel(PanelParams p) {
   const int lane = tid & 31, warp = tid >> 5;
   bool aborted = false;
 
+  // Local candidate of column 0 (later columns are found inside the rank-1
+  // update of the previous step).  Strict '>' from an initial magnitude of
+  // 0: zeros and NaN never become candidates; the first of equal magnitudes
+  // stays (reference: idamax / delayed_dgetrf_cuda.cu:13-20).
+  Best mine{0.0, -1, 0};
+  {
+    const int kl0 = (int)((long long)p.begin - row0);
+    for (int r = max(0, kl0) + tid; r < rows_here; r += blockDim.x) {
+      const double v = fabs(sm[r]);
+      if (v > mine.val) {
+        mine.val = v;
+        mine.row = r;
+      }
+    }
+  }
+
   for (int s = 0; s < w; ++s) {
     const long long k = (long long)p.begin + s;
     const int q = s & (kSlots - 1);
@@ -121,64 +137,44 @@ panel_factor_kernel(PanelParams p) {
     const int kl = (int)(k - row0);  // local index of row k (valid if 0 <= kl < rows_here)
     const bool own_k = kl >= 0 && kl < rows_here;
 
-    // 1. local candidate over column s, rows >= k
-    Best mine;
-    mine.val = 0.0;
-    mine.row = -1;
-    mine.pad = 0;
+    // 1. CTA candidate for column s.
     if (positioned) {
-      if (own_k && tid == 0) {
-        mine.val = __longlong_as_double(0x7ff0000000000000ll);
-        mine.row = kl;
-      }
-    } else {
-      // strict '>' from an initial magnitude of 0: zeros and NaN never
-      // become candidates; the first of equal magnitudes stays.
-      const int rstart = max(0, kl);
-      const double* col = sm + (size_t)s * R;
-      for (int r = rstart + tid; r < rows_here; r += blockDim.x) {
-        const double v = fabs(col[r]);
-        if (v > mine.val) {
-          mine.val = v;
-          mine.row = r;
-        }
-      }
+      mine = Best{0.0, -1, 0};
+      if (own_k && tid == 0) mine = Best{__longlong_as_double(0x7ff0000000000000ll), kl, 0};
     }
     mine = warp_best(mine);
     if (lane == 0) red[warp] = mine;
     __syncthreads();
-    if (warp == 0) {
-      Best v = lane < (blockDim.x >> 5) ? red[lane] : Best{0.0, -1, 0};
-      v = warp_best(v);
-      if (lane == 0) red[0] = v;
-    }
-    __syncthreads();
-    const Best cb = red[0];
 
-    // 2. publish the candidate row (and row k if this CTA owns it)
-    double* xd = xdata + ((size_t)q * p.max_ctas + cta) * xs;
-    if (cb.row >= 0) {
-      for (int j = tid; j < w; j += blockDim.x) __stcg(xd + j, sm[(size_t)j * R + cb.row]);
-      if (tid == 0) __stcg(xd + w, (double)orig[cb.row]);
-    }
-    if (own_k) {
-      double* rk = rowk + (size_t)q * xs;
-      for (int j = tid; j < w; j += blockDim.x) __stcg(rk + j, sm[(size_t)j * R + kl]);
-      if (tid == 0) __stcg(rk + w, (double)orig[kl]);
-    }
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) {
-      const unsigned long long vbits =
-          cb.row >= 0 ? (unsigned long long)__double_as_longlong(cb.val) : 0ull;
-      const unsigned long long grow = cb.row >= 0 ? (unsigned long long)(row0 + cb.row) : 0x7fffffffull;
-      unsigned long long* mys = slots + ((size_t)q * p.max_ctas + cta) * 2;
-      st_volatile_u64(mys + 1, (grow << 1) | tb);
-      st_volatile_u64(mys + 0, (vbits << 1) | tb);
-    }
-
-    // 3. warp 0 gathers all G candidates (bounded wait) and picks the winner
+    // 2-4. Warp 0: publish, gather all G candidates (bounded wait), fetch the
+    // pivot row.  One warp, one fence, no CTA barrier on the critical path.
     if (warp == 0) {
+      Best cb = lane < (blockDim.x >> 5) ? red[lane] : Best{0.0, -1, 0};
+      cb = warp_best(cb);
+      cb.val = __shfl_sync(0xffffffffu, cb.val, 0);
+      cb.row = __shfl_sync(0xffffffffu, cb.row, 0);
+      double* xd = xdata + ((size_t)q * p.max_ctas + cta) * xs;
+      if (cb.row >= 0) {
+        for (int j = lane; j < w; j += 32) __stcg(xd + j, sm[(size_t)j * R + cb.row]);
+        if (lane == 0) __stcg(xd + w, (double)orig[cb.row]);
+      }
+      if (own_k) {
+        double* rk = rowk + (size_t)q * xs;
+        for (int j = lane; j < w; j += 32) __stcg(rk + j, sm[(size_t)j * R + kl]);
+        if (lane == 0) __stcg(rk + w, (double)orig[kl]);
+      }
+      fence_acq_rel_gpu();
+      __syncwarp();
+      if (lane == 0) {
+        const unsigned long long vbits =
+            cb.row >= 0 ? (unsigned long long)__double_as_longlong(cb.val) : 0ull;
+        const unsigned long long grow =
+            cb.row >= 0 ? (unsigned long long)(row0 + cb.row) : 0x7fffffffull;
+        unsigned long long* mys = slots + ((size_t)q * p.max_ctas + cta) * 2;
+        st_volatile_u64(mys + 1, (grow << 1) | tb);
+        st_volatile_u64(mys + 0, (vbits << 1) | tb);
+      }
+
       unsigned long long best_bits = 0ull;
       long long best_row = 0x7fffffffll;
       bool have = false;
@@ -192,7 +188,7 @@ panel_factor_kernel(PanelParams p) {
           kv = ld_volatile_u64(sl + 0);
           kr = ld_volatile_u64(sl + 1);
           if ((kv & 1ull) == tb && (kr & 1ull) == tb) break;
-          if (((++spins) & 1023u) == 0u) {
+          if (((++spins) & 255u) == 0u) {
             if (globaltimer_ns() - t0 > kSpinLimitNs || ld_volatile_i32(&p.state->status) != kOk) {
               timeout = true;
               break;
@@ -221,18 +217,31 @@ panel_factor_kernel(PanelParams p) {
           have = true;
         }
       }
-      __threadfence();
+      best_bits = __shfl_sync(0xffffffffu, best_bits, 0);
+      best_row = __shfl_sync(0xffffffffu, best_row, 0);
+      have = __shfl_sync(0xffffffffu, (int)have, 0) != 0;
+      fence_acq_rel_gpu();
+      const double bv = __longlong_as_double((long long)best_bits);
+      const bool stop = !positioned && !(have && bv > p.threshold);
       if (lane == 0) {
-        if (any_timeout) {
-          atomicCAS(&p.state->status, kOk, kDeviceTimeout);
-          s_flag[3] = 1;
-        } else {
-          s_flag[3] = 0;
-        }
-        const double bv = __longlong_as_double((long long)best_bits);
+        if (any_timeout) atomicCAS(&p.state->status, kOk, kDeviceTimeout);
+        s_flag[3] = any_timeout ? 1 : 0;
         s_flag[0] = (int)best_row;
-        s_flag[1] = (!positioned && !(have && bv > p.threshold)) ? 1 : 0;
-        s_flag[2] = (int)((best_row - p.begin) / R);
+        s_flag[1] = stop ? 1 : 0;
+        if (!any_timeout && !stop && cta == 0 && !positioned) p.ipiv[k] = (int)best_row;
+        if (!any_timeout && stop && cta == 0) p.state->stop_k = (int)k;
+      }
+      if (!any_timeout && !stop) {
+        // L2-only loads (ld.cg): the same slot was read four steps ago and a
+        // stale L1 line must not be served.
+        const int wcta = (int)((best_row - p.begin) / R);
+        const double* src = xdata + ((size_t)q * p.max_ctas + wcta) * xs;
+        for (int j = lane; j <= w; j += 32) prow[j] = __ldcg(src + j);
+        const int pl = (int)(best_row - row0);
+        if (pl >= 0 && pl < rows_here && best_row != k) {
+          const double* rk = rowk + (size_t)q * xs;
+          for (int j = lane; j <= w; j += 32) krow[j] = __ldcg(rk + j);
+        }
       }
     }
     __syncthreads();
@@ -240,55 +249,45 @@ panel_factor_kernel(PanelParams p) {
       aborted = true;
       break;
     }
-    if (s_flag[1]) {
-      // no acceptable pivot in this column: stop at step k
-      if (cta == 0 && tid == 0) p.state->stop_k = (int)k;
-      break;
-    }
+    if (s_flag[1]) break;  // no acceptable pivot in this column: stop at step k
+
+    // 5-6. Swap rows k and p inside the panel, scale the multipliers, update
+    // the rest of the panel, and find the next column's local candidate.
+    // Each row is swapped by the thread that then updates it, so no barrier
+    // separates the swap from the update.
     const long long prow_g = s_flag[0];
-    const int wcta = s_flag[2];
     const int pl = (int)(prow_g - row0);
-    const bool own_p = pl >= 0 && pl < rows_here;
-
-    // 4. fetch the pivot row (and old row k for the owner of the pivot row)
-    {
-      // L2-only loads (ld.cg): the same slot was read four steps ago and a
-      // stale L1 line must not be served.
-      const double* src = xdata + ((size_t)q * p.max_ctas + wcta) * xs;
-      for (int j = tid; j <= w; j += blockDim.x) prow[j] = __ldcg(src + j);
-      if (own_p && prow_g != k) {
-        const double* rk = rowk + (size_t)q * xs;
-        for (int j = tid; j <= w; j += blockDim.x) krow[j] = __ldcg(rk + j);
+    const bool swap_p = pl >= 0 && pl < rows_here && prow_g != k;
+    const double inv = 1.0 / prow[s];
+    mine = Best{0.0, -1, 0};
+    for (int r = max(0, kl) + tid; r < rows_here; r += blockDim.x) {
+      if (r == kl) {  // row k receives the pivot row; it is final from now on
+        for (int j = 0; j < w; ++j) sm[(size_t)j * R + r] = prow[j];
+        orig[r] = (int)prow[w];
+        continue;
+      }
+      if (swap_p && r == pl) {
+        for (int j = 0; j < w; ++j) sm[(size_t)j * R + r] = krow[j];
+        orig[r] = (int)krow[w];
+      }
+      const double l = sm[(size_t)s * R + r] * inv;
+      sm[(size_t)s * R + r] = l;
+      if (s + 1 < w) {
+        const double v = sm[(size_t)(s + 1) * R + r] - l * prow[s + 1];
+        sm[(size_t)(s + 1) * R + r] = v;
+        const double av = fabs(v);
+        if (av > mine.val) {
+          mine.val = av;
+          mine.row = r;
+        }
+        for (int j = s + 2; j < w; ++j) sm[(size_t)j * R + r] -= l * prow[j];
       }
     }
-    __syncthreads();
-
-    // 5. swap rows k and p inside the panel columns
-    if (own_k) {
-      for (int j = tid; j < w; j += blockDim.x) sm[(size_t)j * R + kl] = prow[j];
-      if (tid == 0) orig[kl] = (int)prow[w];
-    }
-    if (own_p && prow_g != k) {
-      for (int j = tid; j < w; j += blockDim.x) sm[(size_t)j * R + pl] = krow[j];
-      if (tid == 0) orig[pl] = (int)krow[w];
-    }
-    // a positioned pivot was recorded by the fallback that placed it
-    if (cta == 0 && tid == 0 && !positioned) p.ipiv[k] = (int)prow_g;
-    __syncthreads();
-
-    // 6. scale the multipliers and update the rest of the panel
-    {
-      const double inv = 1.0 / prow[s];
-      const int rstart = max(0, kl + 1);
-      double* colc = sm + (size_t)s * R;
-      for (int r = rstart + tid; r < rows_here; r += blockDim.x) {
-        const double l = colc[r] * inv;
-        colc[r] = l;
-        for (int j = s + 1; j < w; ++j) sm[(size_t)j * R + r] -= l * prow[j];
-      }
-    }
-    __syncthreads();
   }
+
+  // The last step's swaps and updates were made by other threads than the
+  // ones that write the rows back.
+  __syncthreads();
 
   // Write the slice back.
   for (int c = 0; c < w; ++c) {

@@ -24,7 +24,8 @@ class Options(ctypes.Structure):
         ("threshold", ctypes.c_double),
         ("policy", ctypes.c_int),
         ("panel_rows", ctypes.c_int),
-        ("reserved", ctypes.c_int * 4),
+        ("nb_outer", ctypes.c_int),
+        ("reserved", ctypes.c_int * 3),
     ]
 
 
@@ -150,11 +151,12 @@ def delayed_getrf_cuda_status_string(status: int) -> str:
 
 
 def getrf_device_ex(m, n, d_a, lda, ipiv, jpiv, stream=None, nb=64, threshold=0.0,
-                    policy=POLICY_FULL_PIVOT, panel_rows=0):
+                    policy=POLICY_FULL_PIVOT, panel_rows=0, nb_outer=0):
     """dp_getrf_device_ex with explicit options.  Returns (status, info)."""
     opt = Options()
     lib().dp_options_init(ctypes.byref(opt))
     opt.nb, opt.threshold, opt.policy, opt.panel_rows = nb, threshold, policy, panel_rows
+    opt.nb_outer = nb_outer
     info = ctypes.c_int(-1)
     st = lib().dp_getrf_device_ex(m, n, _dptr(d_a), lda, _iptr(ipiv), _iptr(jpiv),
                                   ctypes.byref(info), _stream(stream), ctypes.byref(opt))

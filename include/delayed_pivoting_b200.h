@@ -40,7 +40,8 @@ typedef struct dp_options {
   int policy;        /* DP_POLICY_FULL_PIVOT (delayed_getrf) or
                         DP_POLICY_NONZERO_COLUMN (delayed_getrf_column) */
   int panel_rows;    /* target rows per CTA in the panel kernel; 0 = automatic */
-  int reserved[4];
+  int nb_outer;      /* outer block width of the trailing update; 0 = automatic */
+  int reserved[3];
 } dp_options;
 
 void dp_options_init(dp_options *opt);
