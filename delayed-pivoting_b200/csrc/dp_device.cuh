@@ -76,6 +76,19 @@ __device__ __forceinline__ void st_volatile_u64(unsigned long long* p, unsigned 
   asm volatile("st.volatile.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// 16-byte volatile vector access: both words of a tagged candidate travel in
+// one request (each word carries its own tag, so a torn read is detected).
+// GPU-scope relaxed accesses (system-scope volatile would also order against
+// the host and peers, which these device-local flags do not need).
+__device__ __forceinline__ void ld_volatile_v2u64(const unsigned long long* p,
+                                                  unsigned long long& a, unsigned long long& b) {
+  asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p) : "memory");
+}
+__device__ __forceinline__ void st_volatile_v2u64(unsigned long long* p, unsigned long long a,
+                                                  unsigned long long b) {
+  asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(a), "l"(b) : "memory");
+}
+
 // Release / acquire fence at GPU scope (cumulative: orders this thread's
 // earlier writes, and those it has observed, before its later writes).
 __device__ __forceinline__ void fence_acq_rel_gpu() {

@@ -21,7 +21,7 @@ struct PanelParams {
   double threshold;
   int* ipiv;          // device swap history (global step index)
   State* state;
-  unsigned long long* slots;  // [2][4][max_ctas][2] tagged words
+  unsigned long long* slots;  // mailboxes [2][4][max_ctas reader][max_ctas writer][2 words]
   double* xdata;              // [4][max_ctas][w_max + 1]
   double* rowk;               // [4][w_max + 1]
   int* swap_block;            // [end - begin]: source row of block row begin + i
@@ -29,6 +29,11 @@ struct PanelParams {
 };
 
 __global__ void panel_factor_kernel(PanelParams p);
+// Cluster variant: one thread-block cluster of C <= 16 CTAs holds the panel
+// in distributed shared memory (launched with a cluster dimension).
+__global__ void panel_cluster_kernel(PanelParams p);
+size_t panel_cluster_smem_bytes(int w, int rows_per_cta);
+int panel_cluster_threads();
 constexpr int kPanelThreadsHost = 256;
 size_t panel_smem_bytes(int w, int rows_per_cta);
 

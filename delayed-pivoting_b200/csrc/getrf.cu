@@ -41,6 +41,7 @@ constexpr int kMaxSearchBlocks = 1024;
 struct DeviceInfo {
   int sms = 0;
   int smem_optin = 0;
+  int max_cluster = 0;  // largest cluster the cluster panel kernel may use (0: none)
   bool ready = false;
 };
 
@@ -60,6 +61,31 @@ int device_info(DeviceInfo& out) {
     if (cudaFuncSetAttribute(panel_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              d.smem_optin - 1024) != cudaSuccess)
       return kCudaFailure;
+    d.max_cluster = 0;
+    if (cudaFuncSetAttribute(panel_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             d.smem_optin - 1024) == cudaSuccess) {
+      cudaFuncSetAttribute(panel_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      for (int c : {16, 8}) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = c;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(c);
+        cfg.blockDim = dim3(panel_cluster_threads());
+        cfg.dynamicSmemBytes = (size_t)d.smem_optin - 1024;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, panel_cluster_kernel, &cfg) == cudaSuccess &&
+            clusters >= 1) {
+          d.max_cluster = c;
+          break;
+        }
+      }
+      cudaGetLastError();
+    }
     d.ready = true;
   }
   out = d;
@@ -67,6 +93,7 @@ int device_info(DeviceInfo& out) {
 }
 
 struct Options {
+  int panel_kernel = 0;  // 0 automatic (cluster when it fits), 1 cluster, 2 multi-CTA grid
   int nb = kDefaultNb;
   int nb_outer = kDefaultNbOuter;
   double threshold = 0.0;
@@ -105,7 +132,8 @@ size_t layout_workspace(Workspace& ws, char* base, int pivots, int max_ctas, int
   ws.state = reinterpret_cast<State*>(take(sizeof(State)));
   ws.d_ipiv = reinterpret_cast<int*>(take(sizeof(int) * (size_t)std::max(pivots, 1)));
   ws.d_jpiv = reinterpret_cast<int*>(take(sizeof(int) * (size_t)std::max(pivots, 1)));
-  ws.slots = reinterpret_cast<unsigned long long*>(take(sizeof(unsigned long long) * 2 * 4 * max_ctas * 2));
+  ws.slots = reinterpret_cast<unsigned long long*>(
+      take(sizeof(unsigned long long) * 2 * 4 * (size_t)max_ctas * max_ctas * 2));
   ws.xdata = reinterpret_cast<double*>(take(sizeof(double) * 4 * (size_t)max_ctas * (w_max + 1)));
   ws.rowk = reinterpret_cast<double*>(take(sizeof(double) * 4 * (size_t)(w_max + 1)));
   ws.swap_block = reinterpret_cast<int*>(take(sizeof(int) * (size_t)w_max));
@@ -121,7 +149,8 @@ size_t layout_workspace(Workspace& ws, char* base, int pivots, int max_ctas, int
 bool plan_panel(int rows, int& w, int target_rows, const DeviceInfo& di, int& G, int& R) {
   const size_t budget = (size_t)di.smem_optin - 1024;
   while (w >= 1) {
-    const size_t fixed = 2 * (size_t)(w + 1) * sizeof(double) + 64;
+    // pivot / old-row buffers, one padding row of the odd column stride, slack
+    const size_t fixed = 2 * (size_t)(w + 1) * sizeof(double) + (size_t)w * sizeof(double) + 64;
     const long long max_r = (long long)((budget - fixed) / ((size_t)w * sizeof(double) + sizeof(int)));
     long long g = (rows + (long long)target_rows - 1) / target_rows;
     g = std::max(1LL, std::min<long long>(g, di.sms));
@@ -138,6 +167,21 @@ bool plan_panel(int rows, int& w, int target_rows, const DeviceInfo& di, int& G,
     w /= 2;
   }
   return false;
+}
+
+// Cluster panel: C CTAs (one cluster) of R rows each; the R x w slice per
+// CTA must fit in shared memory.  Returns false when even an 8-wide panel
+// does not fit (very tall panels then use panel_factor_kernel).
+bool plan_cluster(int rows, int& w, const DeviceInfo& di, int& C, int& R) {
+  if (di.max_cluster <= 0) return false;
+  const size_t budget = (size_t)di.smem_optin - 1024 - 512;
+  C = (int)std::min<long long>(di.max_cluster, std::max(1LL, ((long long)rows + 255) / 256));
+  R = (rows + C - 1) / C;
+  int wf = w;
+  while (wf >= 1 && panel_cluster_smem_bytes(wf, R) > budget) --wf;
+  if (wf < std::min(w, 8)) return false;
+  if (wf < w) w = wf >= 16 ? (wf & ~7) : wf;
+  return true;
 }
 
 #define DP_CHECK_CUDA(call)                       \
@@ -341,7 +385,8 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
     while (b < E) {
       int w = std::min(std::min(o.nb, ws.w_max), E - b);
       int G = 1, R = 1;
-      if (!plan_panel(m - b, w, o.panel_rows, di, G, R)) return kInvalidArgument;
+      const bool use_cluster = o.panel_kernel != 2 && plan_cluster(m - b, w, di, G, R);
+      if (!use_cluster && !plan_panel(m - b, w, o.panel_rows, di, G, R)) return kInvalidArgument;
       e = b + w;
 
       PanelParams pp;
@@ -363,14 +408,30 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       pp.rowk = ws.rowk;
       pp.swap_block = ws.swap_block;
       pp.swap_extra = ws.swap_extra;
-      void* args[] = {&pp};
       rec.begin(DP_KFAM_PANEL);
-      DP_CHECK_CUDA(cudaLaunchCooperativeKernel((const void*)panel_factor_kernel, G,
-                                                kPanelThreadsHost, args, panel_smem_bytes(w, R),
-                                                st));
+      if (use_cluster) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = G;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(G);
+        cfg.blockDim = dim3(panel_cluster_threads());
+        cfg.dynamicSmemBytes = panel_cluster_smem_bytes(w, R);
+        cfg.stream = st;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        DP_CHECK_CUDA(cudaLaunchKernelEx(&cfg, panel_cluster_kernel, pp));
+      } else {
+        void* args[] = {&pp};
+        DP_CHECK_CUDA(cudaLaunchCooperativeKernel((const void*)panel_factor_kernel, G,
+                                                  kPanelThreadsHost, args, panel_smem_bytes(w, R),
+                                                  st));
+        parity ^= 1;
+      }
       rec.end(panel_flops(m, b, w), 16.0 * (double)(m - b) * w, 1);
       positioned = false;
-      parity ^= 1;
       if (int err = read_state(hs, ws, st)) return err;
       if (hs.status != kOk) return hs.status;
 
@@ -454,6 +515,8 @@ bool resolve_options(const dp_options* in, Options& o) {
   o.threshold = in->threshold;
   o.policy = in->policy;
   o.panel_rows = in->panel_rows ? in->panel_rows : kDefaultPanelRows;
+  if (in->panel_kernel < 0 || in->panel_kernel > 2) return false;
+  o.panel_kernel = in->panel_kernel;
   return true;
 }
 

@@ -30,6 +30,13 @@ namespace {
 
 constexpr int kPanelThreads = 256;
 constexpr int kSlots = 4;  // exchange slots, indexed by step mod 4
+constexpr int kMaxSlotsPerLane = 5;  // ceil(max CTAs (<= 160) / 32)
+// Mailboxes: mbox[parity][q][reader][writer] holds the writer's tagged
+// candidate (2 words, 16 bytes).  Every CTA pushes its candidate into every
+// reader's mailbox and polls only its own, contiguous mailbox, so each line
+// has exactly one reader and no CTA spins on a line another CTA is writing
+// for everyone (which delayed the writers' stores by microseconds).
+constexpr int kMboxWords = 2;
 
 struct __align__(16) Best {
   double val;
@@ -59,6 +66,20 @@ __device__ __forceinline__ Best warp_best(Best v) {
   return v;
 }
 
+// row[j * stride] = src[j] for j < w, loads of a batch before its stores.
+__device__ __forceinline__ void copy_row(double* __restrict__ row, const double* __restrict__ src,
+                                         int w, int stride) {
+  int j = 0;
+  for (; j + 8 <= w; j += 8) {
+    double x[8];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) x[b] = src[j + b];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) row[(size_t)(j + b) * stride] = x[b];
+  }
+  for (; j < w; ++j) row[(size_t)j * stride] = src[j];
+}
+
 }  // namespace
 
 __global__ void __launch_bounds__(kPanelThreads, 1)
@@ -71,27 +92,29 @@ panel_factor_kernel(PanelParams p) {
   const int tid = threadIdx.x;
   const long long row0 = (long long)p.begin + (long long)cta * R;  // global row of local row 0
   const int rows_here = (int)min((long long)R, (long long)p.m - row0);
+  const int RP = R | 1;  // odd column stride: a row read across columns hits distinct banks
 
-  double* sm = reinterpret_cast<double*>(smem_raw);   // [w][R]
-  double* prow = sm + (size_t)w * R;                  // [w + 1] pivot row (+orig)
+  double* sm = reinterpret_cast<double*>(smem_raw);   // [w][RP]
+  double* prow = sm + (size_t)w * RP;                 // [w + 1] pivot row (+orig)
   double* krow = prow + (w + 1);                      // [w + 1] old row k (+orig)
   int* orig = reinterpret_cast<int*>(krow + (w + 1));  // [R] source row of each local row
   __shared__ Best red[kPanelThreads / 32];
   __shared__ int s_flag[4];  // 0: winner row (global), 1: stop, 2: winner cta, 3: abort
 
-  unsigned long long* slots = p.slots + (size_t)(p.parity & 1) * kSlots * p.max_ctas * 2;
+  const size_t mbox_q = (size_t)p.max_ctas * p.max_ctas * kMboxWords;  // words per (parity, q)
+  unsigned long long* mbox = p.slots + (size_t)(p.parity & 1) * kSlots * mbox_q;
   double* xdata = p.xdata;  // [kSlots][max_ctas][w_max + 1]
   double* rowk = p.rowk;    // [kSlots][w_max + 1]
   const int xs = p.w_max + 1;
 
-  // Zero this CTA's share (slots cta, cta + G, ...) of the other slot buffer,
-  // which the next launch uses; no CTA of this launch reads it.
+  // Zero the mailboxes of readers cta, cta + G, ... in the other parity
+  // buffer, which the next launch uses; no CTA of this launch touches it.
   {
-    unsigned long long* other = p.slots + (size_t)((p.parity + 1) & 1) * kSlots * p.max_ctas * 2;
-    for (int c = cta; c < p.max_ctas; c += G) {
-      for (int i = tid; i < kSlots * 2; i += blockDim.x) {
-        const int q = i >> 1, word = i & 1;
-        other[((size_t)q * p.max_ctas + c) * 2 + word] = 0ull;
+    unsigned long long* other = p.slots + (size_t)((p.parity + 1) & 1) * kSlots * mbox_q;
+    for (int rd = cta; rd < p.max_ctas; rd += G) {
+      for (int q = 0; q < kSlots; ++q) {
+        unsigned long long* box = other + q * mbox_q + (size_t)rd * p.max_ctas * kMboxWords;
+        for (int i = tid; i < p.max_ctas * kMboxWords; i += blockDim.x) box[i] = 0ull;
       }
     }
   }
@@ -105,7 +128,7 @@ panel_factor_kernel(PanelParams p) {
   // Load the panel slice.
   for (int c = 0; c < w; ++c) {
     const double* src = p.a + idx(row0, p.begin + c, p.lda);
-    for (int r = tid; r < rows_here; r += blockDim.x) sm[(size_t)c * R + r] = src[r];
+    for (int r = tid; r < rows_here; r += blockDim.x) sm[(size_t)c * RP + r] = src[r];
   }
   for (int r = tid; r < rows_here; r += blockDim.x) orig[r] = (int)(row0 + r);
   __syncthreads();
@@ -155,54 +178,69 @@ panel_factor_kernel(PanelParams p) {
       cb.row = __shfl_sync(0xffffffffu, cb.row, 0);
       double* xd = xdata + ((size_t)q * p.max_ctas + cta) * xs;
       if (cb.row >= 0) {
-        for (int j = lane; j < w; j += 32) __stcg(xd + j, sm[(size_t)j * R + cb.row]);
+        for (int j = lane; j < w; j += 32) __stcg(xd + j, sm[(size_t)j * RP + cb.row]);
         if (lane == 0) __stcg(xd + w, (double)orig[cb.row]);
       }
       if (own_k) {
         double* rk = rowk + (size_t)q * xs;
-        for (int j = lane; j < w; j += 32) __stcg(rk + j, sm[(size_t)j * R + kl]);
+        for (int j = lane; j < w; j += 32) __stcg(rk + j, sm[(size_t)j * RP + kl]);
         if (lane == 0) __stcg(rk + w, (double)orig[kl]);
       }
       fence_acq_rel_gpu();
       __syncwarp();
-      if (lane == 0) {
+      {
         const unsigned long long vbits =
             cb.row >= 0 ? (unsigned long long)__double_as_longlong(cb.val) : 0ull;
         const unsigned long long grow =
             cb.row >= 0 ? (unsigned long long)(row0 + cb.row) : 0x7fffffffull;
-        unsigned long long* mys = slots + ((size_t)q * p.max_ctas + cta) * 2;
-        st_volatile_u64(mys + 1, (grow << 1) | tb);
-        st_volatile_u64(mys + 0, (vbits << 1) | tb);
+        unsigned long long* boxes = mbox + q * mbox_q + (size_t)cta * kMboxWords;
+        for (int rd = lane; rd < G; rd += 32)
+          st_volatile_v2u64(boxes + (size_t)rd * p.max_ctas * kMboxWords, (vbits << 1) | tb,
+                            (grow << 1) | tb);
       }
 
+      // Each lane owns mailbox entries lane, lane + 32, ... (at most
+      // kMaxSlotsPerLane) and re-reads all of its pending ones per round, so
+      // a round costs one L2 round trip however many entries are late.
       unsigned long long best_bits = 0ull;
       long long best_row = 0x7fffffffll;
       bool have = false;
       const unsigned long long t0 = globaltimer_ns();
       bool timeout = false;
-      for (int i = lane; i < G; i += 32) {
-        const unsigned long long* sl = slots + ((size_t)q * p.max_ctas + i) * 2;
-        unsigned long long kv, kr;
-        unsigned int spins = 0;
-        while (true) {
-          kv = ld_volatile_u64(sl + 0);
-          kr = ld_volatile_u64(sl + 1);
-          if ((kv & 1ull) == tb && (kr & 1ull) == tb) break;
-          if (((++spins) & 255u) == 0u) {
-            if (globaltimer_ns() - t0 > kSpinLimitNs || ld_volatile_i32(&p.state->status) != kOk) {
-              timeout = true;
-              break;
+      unsigned pending = 0;
+#pragma unroll
+      for (int u = 0; u < kMaxSlotsPerLane; ++u)
+        if (lane + 32 * u < G) pending |= 1u << u;
+      unsigned int rounds = 0;
+      while (pending) {
+        unsigned long long kv[kMaxSlotsPerLane], kr[kMaxSlotsPerLane];
+#pragma unroll
+        for (int u = 0; u < kMaxSlotsPerLane; ++u) {
+          if (pending & (1u << u)) {
+            const unsigned long long* sl =
+                mbox + q * mbox_q + ((size_t)cta * p.max_ctas + lane + 32 * u) * kMboxWords;
+            ld_volatile_v2u64(sl, kv[u], kr[u]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kMaxSlotsPerLane; ++u) {
+          if ((pending & (1u << u)) && (kv[u] & 1ull) == tb && (kr[u] & 1ull) == tb) {
+            pending &= ~(1u << u);
+            const unsigned long long vb = kv[u] >> 1;
+            const long long rr = (long long)(kr[u] >> 1);
+            if (rr != 0x7fffffffll &&
+                (!have || vb > best_bits || (vb == best_bits && rr < best_row))) {
+              best_bits = vb;
+              best_row = rr;
+              have = true;
             }
           }
         }
-        if (timeout) break;
-        const unsigned long long vb = kv >> 1;
-        const long long rr = (long long)(kr >> 1);
-        if (rr == 0x7fffffffll) continue;
-        if (!have || vb > best_bits || (vb == best_bits && rr < best_row)) {
-          best_bits = vb;
-          best_row = rr;
-          have = true;
+        if (pending && ((++rounds) & 63u) == 0u) {
+          if (globaltimer_ns() - t0 > kSpinLimitNs || ld_volatile_i32(&p.state->status) != kOk) {
+            timeout = true;
+            break;
+          }
         }
       }
       const bool any_timeout = __any_sync(0xffffffffu, timeout);
@@ -260,27 +298,42 @@ panel_factor_kernel(PanelParams p) {
     const bool swap_p = pl >= 0 && pl < rows_here && prow_g != k;
     const double inv = 1.0 / prow[s];
     mine = Best{0.0, -1, 0};
+    const double* __restrict__ pr = prow;
     for (int r = max(0, kl) + tid; r < rows_here; r += blockDim.x) {
+      double* __restrict__ row = sm + r;  // element (r, j) at row[j * RP]
       if (r == kl) {  // row k receives the pivot row; it is final from now on
-        for (int j = 0; j < w; ++j) sm[(size_t)j * R + r] = prow[j];
-        orig[r] = (int)prow[w];
+        copy_row(row, pr, w, RP);
+        orig[r] = (int)pr[w];
         continue;
       }
       if (swap_p && r == pl) {
-        for (int j = 0; j < w; ++j) sm[(size_t)j * R + r] = krow[j];
+        copy_row(row, krow, w, RP);
         orig[r] = (int)krow[w];
       }
-      const double l = sm[(size_t)s * R + r] * inv;
-      sm[(size_t)s * R + r] = l;
+      const double l = row[(size_t)s * RP] * inv;
+      row[(size_t)s * RP] = l;
       if (s + 1 < w) {
-        const double v = sm[(size_t)(s + 1) * R + r] - l * prow[s + 1];
-        sm[(size_t)(s + 1) * R + r] = v;
+        const double v = row[(size_t)(s + 1) * RP] - l * pr[s + 1];
+        row[(size_t)(s + 1) * RP] = v;
         const double av = fabs(v);
         if (av > mine.val) {
           mine.val = av;
           mine.row = r;
         }
-        for (int j = s + 2; j < w; ++j) sm[(size_t)j * R + r] -= l * prow[j];
+        // Remaining columns in batches of 8: all loads of a batch are
+        // issued before its stores.
+        int j = s + 2;
+        for (; j + 8 <= w; j += 8) {
+          double x[8], u[8];
+#pragma unroll
+          for (int b = 0; b < 8; ++b) {
+            u[b] = pr[j + b];
+            x[b] = row[(size_t)(j + b) * RP];
+          }
+#pragma unroll
+          for (int b = 0; b < 8; ++b) row[(size_t)(j + b) * RP] = x[b] - l * u[b];
+        }
+        for (; j < w; ++j) row[(size_t)j * RP] -= l * pr[j];
       }
     }
   }
@@ -292,7 +345,7 @@ panel_factor_kernel(PanelParams p) {
   // Write the slice back.
   for (int c = 0; c < w; ++c) {
     double* dst = p.a + idx(row0, p.begin + c, p.lda);
-    for (int r = tid; r < rows_here; r += blockDim.x) dst[r] = sm[(size_t)c * R + r];
+    for (int r = tid; r < rows_here; r += blockDim.x) dst[r] = sm[(size_t)c * RP + r];
   }
   if (aborted) return;
 
@@ -313,7 +366,8 @@ panel_factor_kernel(PanelParams p) {
 }
 
 size_t panel_smem_bytes(int w, int rows_per_cta) {
-  return (size_t)w * rows_per_cta * sizeof(double) + 2 * (size_t)(w + 1) * sizeof(double) +
+  const size_t rp = (size_t)(rows_per_cta | 1);
+  return (size_t)w * rp * sizeof(double) + 2 * (size_t)(w + 1) * sizeof(double) +
          (size_t)((rows_per_cta + 3) & ~3) * sizeof(int);
 }
 

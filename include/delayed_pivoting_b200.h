@@ -41,7 +41,8 @@ typedef struct dp_options {
                         DP_POLICY_NONZERO_COLUMN (delayed_getrf_column) */
   int panel_rows;    /* target rows per CTA in the panel kernel; 0 = automatic */
   int nb_outer;      /* outer block width of the trailing update; 0 = automatic */
-  int reserved[3];
+  int panel_kernel;  /* 0 automatic (cluster panel when it fits), 1 cluster, 2 grid-wide */
+  int reserved[2];
 } dp_options;
 
 void dp_options_init(dp_options *opt);
