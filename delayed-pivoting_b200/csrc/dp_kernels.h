@@ -54,6 +54,14 @@ void launch_trsm_unit_lower(double* a, long long lda, int r0, int w, int c0, int
 void launch_gemm_minus(int M, int N, int K, const double* A, long long lda, const double* B,
                        long long ldb, double* C, long long ldc, cudaStream_t s);
 
+// C(M x N) -= A(M x K) * B(K x N) on the tensor cores (BF16 hi/lo split,
+// three products, FP32 accumulation in TMEM); scratch of
+// mixed_scratch_bytes(M, N, K) bytes.  Returns a status code.
+size_t mixed_scratch_bytes(int max_rows, int max_cols, int max_k);
+int launch_gemm_minus_mixed(int M, int N, int K, const double* A, long long lda, const double* B,
+                            long long ldb, double* C, long long ldc, void* scratch, int* status,
+                            cudaStream_t s);
+
 // Full-pivot search over a(k:m, k:n); result in state->fallback.
 void launch_search_active(const double* a, long long lda, int m, int n, int k, State* state,
                           Cand* block_cands, int max_blocks, cudaStream_t s);

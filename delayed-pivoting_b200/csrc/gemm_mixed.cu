@@ -1,0 +1,372 @@
+// Mixed-precision Schur-complement update on the 5th-generation tensor cores:
+//   C(M x N, FP64) -= A(M x K, FP64) * B(K x N, FP64)
+// with the product formed from a BF16 hi/lo split of A and B as
+//   Ah*Bh + Ah*Bl + Al*Bh          (three tcgen05.mma kind::f16 products)
+// accumulated in FP32 in tensor memory, then subtracted from C in FP64.
+// This replaces the FP64 trailing update (delayed_lu/delayed_dgetrf.cpp:80-83)
+// in the mixed-precision factorisation; pivot search, delay / fallback
+// decisions and the panel stay in FP64.  Relative error of one update is about
+// 2^-16 (the dropped Al*Bl term and the BF16 rounding of the low parts) plus
+// FP32 accumulation; FP64 iterative refinement recovers full accuracy.
+//
+// Pipeline (one CTA per 128 x 128 tile of C, 4 warps):
+//   split_*_kernel  FP64 column-major -> BF16 hi / lo, K-major, K padded to 64
+//   TMA             128 x 64 BF16 boxes with 128-byte swizzle into a 2-stage
+//                   ring, completion through mbarrier transaction counts
+//   tcgen05.mma     issued by one thread: 4 K-steps of 16 x 3 products per
+//                   stage into a 128 x 128 FP32 accumulator (128 TMEM columns)
+//   tcgen05.commit  frees a stage / signals the epilogue
+//   epilogue        tcgen05.ld (32 lanes x 16 columns per warp and call),
+//                   C -= acc in FP64, coalesced along the column
+// Every mbarrier wait is bounded; on timeout the kernel records
+// kDeviceTimeout, skips the epilogue and still frees its tensor memory.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <mutex>
+
+#include "dp_device.cuh"
+#include "dp_kernels.h"
+
+namespace dp {
+
+namespace mixed {
+
+constexpr int BM = 128, BN = 128, BK = 64;  // BK: BF16 elements per 128-byte swizzle row
+constexpr int kThreads = 128;
+constexpr int kTileBytes = BM * BK * 2;     // 16 KB per operand tile (BN == BM)
+constexpr int kStageBytes = 4 * kTileBytes; // Ah, Al, Bh, Bl
+constexpr int kStages = 2;
+constexpr size_t kSmem = (size_t)kStages * kStageBytes + 1024;  // + alignment slack
+constexpr unsigned kTmemCols = BN;
+
+// ---------------------------------------------------------------- split ----
+__device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  hi = __double2bfloat16(x);
+  lo = __double2bfloat16(x - (double)__bfloat162float(hi));
+}
+
+// A (M x K, column-major, lda) -> Ah, Al as [M][Kp] (K contiguous).  32x32
+// tiles transposed through shared memory so both sides stay coalesced.
+__global__ void split_a_kernel(const double* __restrict__ A, long long lda, int M, int K, int Kp,
+                               __nv_bfloat16* __restrict__ Ah, __nv_bfloat16* __restrict__ Al) {
+  __shared__ double t[32][33];
+  const int m0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  for (int i = ty; i < 32; i += 8) {
+    const int m = m0 + tx, k = k0 + i;
+    t[i][tx] = (m < M && k < K) ? A[idx(m, k, lda)] : 0.0;
+  }
+  __syncthreads();
+  for (int i = ty; i < 32; i += 8) {
+    const int m = m0 + i, k = k0 + tx;
+    if (m < M && k < Kp) {
+      __nv_bfloat16 h, l;
+      split_bf16(t[tx][i], h, l);
+      Ah[(size_t)m * Kp + k] = h;
+      Al[(size_t)m * Kp + k] = l;
+    }
+  }
+}
+
+// B (K x N, column-major, ldb) -> Bh, Bl as [N][Kp] (K contiguous).
+__global__ void split_b_kernel(const double* __restrict__ B, long long ldb, int K, int N, int Kp,
+                               __nv_bfloat16* __restrict__ Bh, __nv_bfloat16* __restrict__ Bl) {
+  const long long total = (long long)N * Kp;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int n = (int)(e / Kp), k = (int)(e - (long long)n * Kp);
+    const double x = k < K ? B[idx(k, n, ldb)] : 0.0;
+    __nv_bfloat16 h, l;
+    split_bf16(x, h, l);
+    Bh[e] = h;
+    Bl[e] = l;
+  }
+}
+
+// ------------------------------------------------------ PTX wrappers ----
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// Bounded wait for the phase with the given parity; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  const uint32_t addr = smem_u32(bar);
+  const unsigned long long t0 = globaltimer_ns();
+  for (unsigned it = 0;; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if ((it & 255u) == 255u && globaltimer_ns() - t0 > kSpinLimitNs) return false;
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tm, uint64_t* bar, int x,
+                                            int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+// Shared-memory matrix descriptor of a K-major, 128-byte-swizzled operand
+// tile (8-row x 128-byte swizzle atoms, atoms 1024 bytes apart).
+__device__ __forceinline__ uint64_t umma_desc_k_sw128(const void* tile) {
+  const uint64_t addr = smem_u32(tile);
+  uint64_t d = 0;
+  d |= (addr >> 4) & 0x3FFFull;          // start address (16-byte units)
+  d |= 1ull << 16;                        // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;       // stride byte offset: next 8-row group
+  d |= 1ull << 46;                        // descriptor version (sm_100)
+  d |= 2ull << 61;                        // layout: 128-byte swizzle
+  return d;
+}
+
+// kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both
+// K-major, M = 128, N = 128.
+__host__ __device__ constexpr uint32_t idesc_bf16_f32(int m, int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                         uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15},"
+      " [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// -------------------------------------------------------------- GEMM ----
+__global__ void __launch_bounds__(kThreads, 1)
+gemm_bf16x3_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
+                   const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl,
+                   int M, int N, int kchunks, double* C, long long ldc, int* status) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages], done_bar;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int failed;
+  unsigned char* smem =
+      reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_base_sh)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 32) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(&done_bar, 1);
+    failed = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base_sh;
+
+  if (tid == 0) {
+    auto load_chunk = [&](int c, int s) {
+      unsigned char* st = smem + (size_t)s * kStageBytes;
+      mbar_expect_tx(&full_bar[s], kStageBytes);
+      tma_load_2d(st + 0 * kTileBytes, &tmAh, &full_bar[s], c * BK, m0);
+      tma_load_2d(st + 1 * kTileBytes, &tmAl, &full_bar[s], c * BK, m0);
+      tma_load_2d(st + 2 * kTileBytes, &tmBh, &full_bar[s], c * BK, n0);
+      tma_load_2d(st + 3 * kTileBytes, &tmBl, &full_bar[s], c * BK, n0);
+    };
+    const uint32_t idesc = idesc_bf16_f32(BM, BN);
+    for (int c = 0; c < kchunks && c < kStages; ++c) load_chunk(c, c);
+    bool ok = true;
+    for (int c = 0; c < kchunks && ok; ++c) {
+      const int s = c % kStages;
+      const unsigned ph = (unsigned)((c / kStages) & 1);
+      if (!mbar_wait(&full_bar[s], ph)) {
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      unsigned char* st = smem + (size_t)s * kStageBytes;
+#pragma unroll
+      for (int kk = 0; kk < BK / 16; ++kk) {
+        const uint64_t ah = umma_desc_k_sw128(st + 0 * kTileBytes + kk * 32);
+        const uint64_t al = umma_desc_k_sw128(st + 1 * kTileBytes + kk * 32);
+        const uint64_t bh = umma_desc_k_sw128(st + 2 * kTileBytes + kk * 32);
+        const uint64_t bl = umma_desc_k_sw128(st + 3 * kTileBytes + kk * 32);
+        umma_f16(tmem, ah, bh, idesc, (c > 0 || kk > 0) ? 1u : 0u);
+        umma_f16(tmem, ah, bl, idesc, 1u);
+        umma_f16(tmem, al, bh, idesc, 1u);
+      }
+      umma_commit(&empty_bar[s]);
+      if (c + kStages < kchunks) {
+        if (!mbar_wait(&empty_bar[s], ph)) {
+          ok = false;
+          break;
+        }
+        load_chunk(c + kStages, s);
+      }
+    }
+    if (!ok) {
+      failed = 1;
+      atomicCAS(status, kOk, kDeviceTimeout);
+    }
+    umma_commit(&done_bar);  // arrives once every issued MMA has completed
+  }
+  __syncwarp();
+  const bool done_ok = mbar_wait(&done_bar, 0);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (done_ok && !failed) {
+    const int row = m0 + warp * 32 + lane;
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+    for (int cc = 0; cc < BN / 16; ++cc) {
+      uint32_t r[16];
+      tmem_ld16(lane_base + (uint32_t)(cc * 16), r);
+      if (row < M) {
+        double old[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int col = n0 + cc * 16 + j;
+          old[j] = col < N ? C[idx(row, col, ldc)] : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int col = n0 + cc * 16 + j;
+          if (col < N) C[idx(row, col, ldc)] = old[j] - (double)__uint_as_float(r[j]);
+        }
+      }
+    }
+  } else if (!done_ok && tid == 0) {
+    atomicCAS(status, kOk, kDeviceTimeout);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols)
+                 : "memory");
+  }
+}
+
+// ------------------------------------------------------ host helpers ----
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+// 2-D BF16 tensor [rows][kp] (kp contiguous), box 64 x 128, 128-byte swizzle.
+bool make_map(CUtensorMap* tm, void* base, int rows, int kp) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)kp * 2};
+  cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)BM};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace mixed
+
+size_t mixed_scratch_bytes(int max_rows, int max_cols, int max_k) {
+  const size_t kp = (size_t)((max_k + mixed::BK - 1) / mixed::BK) * mixed::BK;
+  return 2 * ((size_t)max_rows + (size_t)max_cols) * kp * sizeof(__nv_bfloat16) + 4096;
+}
+
+// C(M x N) -= A(M x K) * B(K x N) through the BF16x3 tensor-core path.
+// scratch must hold mixed_scratch_bytes(M, N, K) bytes (256-byte aligned).
+int launch_gemm_minus_mixed(int M, int N, int K, const double* A, long long lda, const double* B,
+                            long long ldb, double* C, long long ldc, void* scratch, int* status,
+                            cudaStream_t s) {
+  using namespace mixed;
+  if (M <= 0 || N <= 0 || K <= 0) return kOk;
+  static bool configured = false;
+  if (!configured) {
+    if (cudaFuncSetAttribute(gemm_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kSmem) != cudaSuccess)
+      return kCudaFailure;
+    configured = true;
+  }
+  const int kp = (K + BK - 1) / BK * BK;
+  auto* ah = reinterpret_cast<__nv_bfloat16*>(scratch);
+  auto* al = ah + (size_t)M * kp;
+  auto* bh = al + (size_t)M * kp;
+  auto* bl = bh + (size_t)N * kp;
+  split_a_kernel<<<dim3((M + 31) / 32, (kp + 31) / 32), dim3(32, 8), 0, s>>>(A, lda, M, K, kp, ah,
+                                                                            al);
+  {
+    const long long total = (long long)N * kp;
+    long long grid = (total + 255) / 256;
+    if (grid > 148 * 16) grid = 148 * 16;
+    split_b_kernel<<<(int)grid, 256, 0, s>>>(B, ldb, K, N, kp, bh, bl);
+  }
+  CUtensorMap tah, tal, tbh, tbl;
+  if (!make_map(&tah, ah, M, kp) || !make_map(&tal, al, M, kp) || !make_map(&tbh, bh, N, kp) ||
+      !make_map(&tbl, bl, N, kp))
+    return kLibraryFailure;
+  dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
+  gemm_bf16x3_kernel<<<grid, kThreads, kSmem, s>>>(tah, tal, tbh, tbl, M, N, kp / BK, C, ldc,
+                                                   status);
+  return cudaGetLastError() == cudaSuccess ? kOk : kCudaFailure;
+}
+
+}  // namespace dp
