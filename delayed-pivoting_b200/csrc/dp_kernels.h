@@ -48,6 +48,11 @@ void launch_laswp(double* a, long long lda, int begin, int nblock, const int* sw
 int trsm_max_width();
 void launch_trsm_unit_lower(double* a, long long lda, int r0, int w, int c0, int nc,
                             cudaStream_t s);
+// Same with separate operands; and B <- U^{-1} B for upper U with diagonal.
+void launch_trsm_lower_unit(const double* L, long long ldl, double* B, long long ldb, int w, int nc,
+                            cudaStream_t s);
+void launch_trsm_upper(const double* U, long long ldu, double* B, long long ldb, int w, int nc,
+                       cudaStream_t s);
 
 // C(M x N) -= A(M x K) * B(K x N); all three inside the same column-major
 // matrix (or any column-major operands).

@@ -93,6 +93,7 @@ int device_info(DeviceInfo& out) {
 }
 
 struct Options {
+  int precision = DP_PRECISION_FP64;
   int panel_kernel = 0;  // 0 automatic (cluster when it fits), 1 cluster, 2 multi-CTA grid
   int nb = kDefaultNb;
   int nb_outer = kDefaultNbOuter;
@@ -113,6 +114,7 @@ struct Workspace {
   int* swap_block = nullptr;
   int* swap_extra = nullptr;
   Cand* cands = nullptr;
+  void* mixed = nullptr;  // BF16 operand scratch of the tensor-core update (mixed precision)
   int max_ctas = 0;
   int w_max = 0;
 };
@@ -120,7 +122,8 @@ struct Workspace {
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 // Lays the workspace out from `base` (nullptr: only computes the size).
-size_t layout_workspace(Workspace& ws, char* base, int pivots, int max_ctas, int w_max) {
+size_t layout_workspace(Workspace& ws, char* base, int pivots, int max_ctas, int w_max,
+                        size_t mixed_bytes) {
   size_t off = 0;
   auto take = [&](size_t bytes) {
     const size_t at = off;
@@ -139,6 +142,7 @@ size_t layout_workspace(Workspace& ws, char* base, int pivots, int max_ctas, int
   ws.swap_block = reinterpret_cast<int*>(take(sizeof(int) * (size_t)w_max));
   ws.swap_extra = reinterpret_cast<int*>(take(sizeof(int) * 2 * (size_t)w_max));
   ws.cands = reinterpret_cast<Cand*>(take(sizeof(Cand) * kMaxSearchBlocks));
+  ws.mixed = mixed_bytes ? reinterpret_cast<void*>(take(mixed_bytes)) : nullptr;
   ws.base = base;
   ws.bytes = off;
   return off;
@@ -341,17 +345,31 @@ void trsm_blocked(double* a, long long lda, int r0, int W, int c0, int nc, cudaS
 // Brings columns [c0, n_end) up to date with the eliminated steps
 // [s0, s0 + W): blocked TRSM on rows [s0, s0 + W), then
 // A(r_gemm:m, c0:n_end) -= L(r_gemm:m, s0:s0+W) * U(s0:s0+W, c0:n_end).
-void update_columns(double* a, long long lda, int m, int s0, int W, int r_gemm, int c0, int n_end,
-                    cudaStream_t st, Recorder& rec) {
+// When `mixed_ws` is set the rank-W update runs on the tensor cores (BF16x3,
+// FP32 accumulation); the TRSM always runs in FP64.
+int update_columns(double* a, long long lda, int m, int s0, int W, int r_gemm, int c0, int n_end,
+                   cudaStream_t st, Recorder& rec, void* mixed_ws = nullptr,
+                   int* status = nullptr) {
   const int nc = n_end - c0;
-  if (W <= 0 || nc <= 0) return;
+  if (W <= 0 || nc <= 0) return kOk;
   trsm_blocked(a, lda, s0, W, c0, nc, st, rec);
   const int M = m - r_gemm;
-  if (M <= 0) return;
+  if (M <= 0) return kOk;
+  const double fl = 2.0 * M * (double)nc * W;
+  const double by = 8.0 * ((double)M * W + (double)W * nc + 2.0 * M * (double)nc);
+  if (mixed_ws) {
+    rec.begin(DP_KFAM_GEMM_MIXED);
+    const int e = launch_gemm_minus_mixed(M, nc, W, a + idx(r_gemm, s0, lda), lda,
+                                          a + idx(s0, c0, lda), lda, a + idx(r_gemm, c0, lda), lda,
+                                          mixed_ws, status, st);
+    rec.end(fl, by, 3);
+    return e;
+  }
   rec.begin(DP_KFAM_GEMM);
   launch_gemm_minus(M, nc, W, a + idx(r_gemm, s0, lda), lda, a + idx(s0, c0, lda), lda,
                     a + idx(r_gemm, c0, lda), lda, st);
-  rec.end(2.0 * M * (double)nc * W, 8.0 * ((double)M * W + (double)W * nc + 2.0 * M * (double)nc), 1);
+  rec.end(fl, by, 1);
+  return kOk;
 }
 
 // Two-level blocked delayed LU.  An outer block [B, E) of width NB is
@@ -446,8 +464,12 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       DP_CHECK_CUDA(cudaGetLastError());
       b = e;
     }
+    void* mixed_ws = o.precision == DP_PRECISION_MIXED_BF16X3 ? ws.mixed : nullptr;
     if (stop < 0) {
-      update_columns(a, lda, m, B, E - B, E, E, n, st, rec);  // right of the outer block
+      // right of the outer block: the O(n^3) update
+      if (int err = update_columns(a, lda, m, B, E - B, E, E, n, st, rec, mixed_ws,
+                                   &ws.state->status))
+        return err;
       DP_CHECK_CUDA(cudaGetLastError());
       B = E;
       continue;
@@ -456,7 +478,9 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
     // Stopped at k inside panel [b, e): materialize, then search.
     const int k = stop;
     update_columns(a, lda, m, b, k - b, k, e, E, st, rec);  // rest of the outer block
-    update_columns(a, lda, m, B, k - B, k, E, n, st, rec);  // right of the outer block
+    if (int err = update_columns(a, lda, m, B, k - B, k, E, n, st, rec, mixed_ws,
+                                 &ws.state->status))  // right of the outer block
+      return err;
     rec.begin(DP_KFAM_SEARCH);
     if (o.policy == DP_POLICY_NONZERO_COLUMN)
       launch_search_nonzero_column(a, lda, m, n, k, o.threshold, ws.state, st);
@@ -517,6 +541,9 @@ bool resolve_options(const dp_options* in, Options& o) {
   o.panel_rows = in->panel_rows ? in->panel_rows : kDefaultPanelRows;
   if (in->panel_kernel < 0 || in->panel_kernel > 2) return false;
   o.panel_kernel = in->panel_kernel;
+  if (in->precision != DP_PRECISION_FP64 && in->precision != DP_PRECISION_MIXED_BF16X3)
+    return false;
+  o.precision = in->precision;
   return true;
 }
 
@@ -541,16 +568,20 @@ int getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* 
   }
   Workspace ws;
   const int w_max = kMaxPanelWidth;
-  const size_t bytes = layout_workspace(ws, nullptr, pivots, di.sms, w_max);
+  const size_t mixed_bytes = o.precision == DP_PRECISION_MIXED_BF16X3
+                                 ? mixed_scratch_bytes(m, n, std::max(o.nb_outer, o.nb))
+                                 : 0;
+  const size_t bytes = layout_workspace(ws, nullptr, pivots, di.sms, w_max, mixed_bytes);
   char* base = nullptr;
   if (cudaMallocAsync(reinterpret_cast<void**>(&base), bytes, st) != cudaSuccess) {
     cudaGetLastError();
     *info = -1;
     return kAllocationFailed;
   }
-  layout_workspace(ws, base, pivots, di.sms, w_max);
+  layout_workspace(ws, base, pivots, di.sms, w_max, mixed_bytes);
   int status = kOk;
-  if (cudaMemsetAsync(base, 0, bytes, st) != cudaSuccess) status = kCudaFailure;
+  // the BF16 scratch is fully written before use; clear only the rest
+  if (cudaMemsetAsync(base, 0, bytes - mixed_bytes, st) != cudaSuccess) status = kCudaFailure;
   int inf = pivots;
   HostTrace trace;
   g_trace = &trace;

@@ -1,0 +1,363 @@
+// Solve and iterative refinement on top of the delayed-pivoting LU.
+//
+// The reference stops at the factorisation (no getrs, no refinement).  The
+// factorisation P*A*Q = L*U it produces (delayed_lu_cuda/delayed_dgetrf_cuda.hpp:15-21:
+// ipiv / jpiv are swap histories replayed in order, example.cu:61-68) gives
+//   A x = b  <=>  L U y = P b,  x = Q y.
+// getrs: gather b through the row order of ipiv, forward substitution with
+// the unit-lower L and back substitution with U (64-row diagonal blocks on
+// the TRSM kernels, the off-diagonal blocks as FP64 DMMA GEMM updates),
+// scatter y through the column order of jpiv.
+// gesv_ir: factor (mixed precision: BF16x3 tensor-core trailing update, or
+// plain FP64), solve, then refine in FP64: r = b - A x on the FP64 GEMM,
+// backward error max_c ||r_c||_inf / (||A||_inf ||x_c||_inf + ||b_c||_inf),
+// correction through the same factors.  A refinement that stops improving
+// (error not halved) or does not reach the tolerance within max_iter steps
+// triggers a plain FP64 re-factorisation.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "delayed_pivoting_b200.h"
+#include "dp_device.cuh"
+#include "dp_kernels.h"
+
+namespace dp {
+
+int getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* info,
+                 cudaStream_t st, const dp_options* opt);
+
+namespace {
+
+__global__ void gather_rows_kernel(const double* __restrict__ in, long long ldi, double* out,
+                                   long long ldo, const int* __restrict__ perm, int n, int nrhs) {
+  const long long total = (long long)n * nrhs;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % n), c = (int)(e / n);
+    out[idx(i, c, ldo)] = in[idx(perm[i], c, ldi)];
+  }
+}
+
+__global__ void scatter_rows_kernel(const double* __restrict__ in, long long ldi, double* out,
+                                    long long ldo, const int* __restrict__ perm, int n, int nrhs) {
+  const long long total = (long long)n * nrhs;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % n), c = (int)(e / n);
+    out[idx(perm[i], c, ldo)] = in[idx(i, c, ldi)];
+  }
+}
+
+__global__ void copy_kernel(const double* __restrict__ in, long long ldi, double* out, long long ldo,
+                            int n, int nrhs) {
+  const long long total = (long long)n * nrhs;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % n), c = (int)(e / n);
+    out[idx(i, c, ldo)] = in[idx(i, c, ldi)];
+  }
+}
+
+__global__ void axpy_kernel(const double* __restrict__ d, long long ldd, double* x, long long ldx,
+                            int n, int nrhs) {
+  const long long total = (long long)n * nrhs;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % n), c = (int)(e / n);
+    x[idx(i, c, ldx)] += d[idx(i, c, ldd)];
+  }
+}
+
+__device__ __forceinline__ void atomic_max_pos(double* addr, double v) {
+  // non-negative doubles order like their bit patterns
+  atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+// out[c] = max_i |X(i, c)| (out must be zero on entry); NaN is reported as +inf.
+__global__ void colmax_kernel(const double* __restrict__ X, long long ldx, int n, int nrhs,
+                              double* out) {
+  const int c = blockIdx.y;
+  double m = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = fabs(X[idx(i, c, ldx)]);
+    m = (v == v) ? fmax(m, v) : __longlong_as_double(0x7ff0000000000000ll);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) atomic_max_pos(out + c, m);
+}
+
+// rowsum[i] = sum_j |A(i, j)| over the n x n matrix (threads over rows, so
+// each column is read coalesced); out[0] = max_i rowsum (atomic).
+__global__ void row_abs_sum_kernel(const double* __restrict__ A, long long lda, int n, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double s = 0.0;
+  if (i < n)
+    for (int j = 0; j < n; ++j) s += fabs(A[idx(i, j, lda)]);
+  if (i < n) atomic_max_pos(out, s == s ? s : __longlong_as_double(0x7ff0000000000000ll));
+}
+
+int grid_of(long long work) {
+  long long g = (work + 255) / 256;
+  return (int)std::max(1LL, std::min(g, 148LL * 16));
+}
+
+}  // namespace
+
+// L y = b (unit lower, n x n at lu) in place on B (n x nrhs).
+void forward_solve(const double* lu, long long ldlu, int n, double* B, long long ldb, int nrhs,
+                   cudaStream_t st) {
+  const int tw = trsm_max_width();
+  for (int b = 0; b < n; b += tw) {
+    const int w = std::min(tw, n - b);
+    launch_trsm_lower_unit(lu + idx(b, b, ldlu), ldlu, B + b, ldb, w, nrhs, st);
+    if (b + w < n)
+      launch_gemm_minus(n - b - w, nrhs, w, lu + idx(b + w, b, ldlu), ldlu, B + b, ldb, B + b + w,
+                        ldb, st);
+  }
+}
+
+// U x = y (upper with diagonal, n x n at lu) in place on B (n x nrhs).
+void backward_solve(const double* lu, long long ldlu, int n, double* B, long long ldb, int nrhs,
+                    cudaStream_t st) {
+  const int tw = trsm_max_width();
+  const int nblocks = (n + tw - 1) / tw;
+  for (int bi = nblocks - 1; bi >= 0; --bi) {
+    const int b = bi * tw;
+    const int w = std::min(tw, n - b);
+    launch_trsm_upper(lu + idx(b, b, ldlu), ldlu, B + b, ldb, w, nrhs, st);
+    if (b > 0) launch_gemm_minus(b, nrhs, w, lu + idx(0, b, ldlu), ldlu, B + b, ldb, B, ldb, st);
+  }
+}
+
+int getrs_device(int n, int nrhs, const double* lu, int ldlu, const int* ipiv, const int* jpiv,
+                 double* B, int ldb, cudaStream_t st) {
+  if (n < 0 || nrhs < 0 || ldlu < std::max(1, n) || ldb < std::max(1, n)) return kInvalidArgument;
+  if (n == 0 || nrhs == 0) return kOk;
+  if (!lu || !B || !ipiv || !jpiv) return kInvalidArgument;
+  std::vector<int> row(n), col(n);
+  for (int i = 0; i < n; ++i) row[i] = col[i] = i;
+  for (int k = 0; k < n; ++k) {
+    if (ipiv[k] < k || ipiv[k] >= n || jpiv[k] < k || jpiv[k] >= n) return kInvalidArgument;
+    std::swap(row[k], row[ipiv[k]]);
+    std::swap(col[k], col[jpiv[k]]);
+  }
+  int* d_perm = nullptr;
+  double* tmp = nullptr;
+  if (cudaMallocAsync(reinterpret_cast<void**>(&d_perm), sizeof(int) * 2 * (size_t)n, st) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return kAllocationFailed;
+  }
+  if (cudaMallocAsync(reinterpret_cast<void**>(&tmp), sizeof(double) * (size_t)n * nrhs, st) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    cudaFreeAsync(d_perm, st);
+    return kAllocationFailed;
+  }
+  int status = kOk;
+  if (cudaMemcpyAsync(d_perm, row.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(d_perm + n, col.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st) !=
+          cudaSuccess)
+    status = kCudaFailure;
+  if (status == kOk) {
+    const long long total = (long long)n * nrhs;
+    gather_rows_kernel<<<grid_of(total), 256, 0, st>>>(B, ldb, tmp, n, d_perm, n, nrhs);
+    forward_solve(lu, ldlu, n, tmp, n, nrhs, st);
+    backward_solve(lu, ldlu, n, tmp, n, nrhs, st);
+    scatter_rows_kernel<<<grid_of(total), 256, 0, st>>>(tmp, n, B, ldb, d_perm + n, n, nrhs);
+    if (cudaGetLastError() != cudaSuccess) status = kCudaFailure;
+  }
+  cudaFreeAsync(tmp, st);
+  cudaFreeAsync(d_perm, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && status == kOk) status = kCudaFailure;
+  return status;
+}
+
+namespace {
+
+// max over columns of ||R_c|| / (normA ||X_c|| + ||B_c||), all infinity norms.
+int backward_error(const double* A, int lda, int n, const double* B, int ldb, const double* X,
+                   int ldx, int nrhs, double* R, double* norms, double normA,
+                   const std::vector<double>& normB, double& berr, cudaStream_t st) {
+  const long long total = (long long)n * nrhs;
+  copy_kernel<<<grid_of(total), 256, 0, st>>>(B, ldb, R, n, n, nrhs);
+  launch_gemm_minus(n, nrhs, n, A, lda, X, ldx, R, n, st);
+  if (cudaMemsetAsync(norms, 0, sizeof(double) * 2 * nrhs, st) != cudaSuccess) return kCudaFailure;
+  dim3 g((unsigned)std::min(64, (n + 255) / 256), (unsigned)nrhs);
+  colmax_kernel<<<g, 256, 0, st>>>(R, n, n, nrhs, norms);
+  colmax_kernel<<<g, 256, 0, st>>>(X, ldx, n, nrhs, norms + nrhs);
+  std::vector<double> h(2 * (size_t)nrhs);
+  if (cudaMemcpyAsync(h.data(), norms, sizeof(double) * 2 * nrhs, cudaMemcpyDeviceToHost, st) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return kCudaFailure;
+  berr = 0.0;
+  for (int c = 0; c < nrhs; ++c) {
+    const double den = normA * h[nrhs + c] + normB[c];
+    const double e = den > 0.0 ? h[c] / den : (h[c] > 0.0 ? INFINITY : 0.0);
+    berr = std::max(berr, std::isnan(e) ? INFINITY : e);
+  }
+  return kOk;
+}
+
+}  // namespace
+
+int gesv_ir_device(int n, int nrhs, const double* A, int lda, double* B, int ldb, int precision,
+                   int max_iter, double tol, dp_ir_result* res, cudaStream_t st) {
+  if (!res) return kInvalidArgument;
+  std::memset(res, 0, sizeof(*res));
+  res->info = -1;
+  res->backward_error = INFINITY;
+  if (n < 0 || nrhs < 0 || lda < std::max(1, n) || ldb < std::max(1, n) || max_iter < 0 ||
+      !(tol >= 0.0) || (precision != DP_PRECISION_FP64 && precision != DP_PRECISION_MIXED_BF16X3))
+    return kInvalidArgument;
+  if (n == 0 || nrhs == 0) {
+    res->info = n;
+    res->backward_error = 0.0;
+    res->converged = 1;
+    return kOk;
+  }
+  if (!A || !B) return kInvalidArgument;
+
+  const size_t nn = (size_t)n * n, nr = (size_t)n * nrhs;
+  double *lu = nullptr, *X = nullptr, *R = nullptr, *norms = nullptr;
+  auto release = [&] {
+    if (lu) cudaFreeAsync(lu, st);
+    if (X) cudaFreeAsync(X, st);
+    if (R) cudaFreeAsync(R, st);
+    if (norms) cudaFreeAsync(norms, st);
+    cudaStreamSynchronize(st);
+  };
+  if (cudaMallocAsync(reinterpret_cast<void**>(&lu), nn * sizeof(double), st) != cudaSuccess ||
+      cudaMallocAsync(reinterpret_cast<void**>(&X), nr * sizeof(double), st) != cudaSuccess ||
+      cudaMallocAsync(reinterpret_cast<void**>(&R), nr * sizeof(double), st) != cudaSuccess ||
+      cudaMallocAsync(reinterpret_cast<void**>(&norms), (2 * (size_t)nrhs + 1) * sizeof(double),
+                      st) != cudaSuccess) {
+    cudaGetLastError();
+    release();
+    return kAllocationFailed;
+  }
+  std::vector<int> ipiv(n), jpiv(n);
+  std::vector<double> normB(nrhs);
+  double normA = 0.0;
+  int status = kOk;
+
+  // ||A||_inf and ||B_c||_inf
+  if (cudaMemsetAsync(norms, 0, (2 * (size_t)nrhs + 1) * sizeof(double), st) != cudaSuccess)
+    status = kCudaFailure;
+  if (status == kOk) {
+    row_abs_sum_kernel<<<(n + 255) / 256, 256, 0, st>>>(A, lda, n, norms + 2 * nrhs);
+    dim3 g((unsigned)std::min(64, (n + 255) / 256), (unsigned)nrhs);
+    colmax_kernel<<<g, 256, 0, st>>>(B, ldb, n, nrhs, norms);
+    std::vector<double> h(2 * (size_t)nrhs + 1);
+    if (cudaMemcpyAsync(h.data(), norms, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      status = kCudaFailure;
+    else {
+      normA = h[2 * nrhs];
+      for (int c = 0; c < nrhs; ++c) normB[c] = h[c];
+    }
+  }
+
+  auto factor_and_solve = [&](int prec) -> int {
+    const long long total = (long long)nn;
+    copy_kernel<<<grid_of(total), 256, 0, st>>>(A, lda, lu, n, n, n);
+    dp_options opt;
+    dp_options_init(&opt);
+    opt.precision = prec;
+    int info = -1;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, st);
+    int s = getrf_device(n, n, lu, n, ipiv.data(), jpiv.data(), &info, st, &opt);
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    res->factor_ms += ms;
+    res->info = info;
+    if (s != kOk) return s;
+    if (info < n) return kOk;  // singular: no solution
+    copy_kernel<<<grid_of((long long)nr), 256, 0, st>>>(B, ldb, X, n, n, nrhs);
+    return getrs_device(n, nrhs, lu, n, ipiv.data(), jpiv.data(), X, n, st);
+  };
+
+  // refinement loop; returns status, sets converged
+  auto refine = [&](int iters_left, bool& converged, bool& stalled) -> int {
+    converged = stalled = false;
+    double prev = INFINITY;
+    for (int it = 0;; ++it) {
+      double berr = INFINITY;
+      int s = backward_error(A, lda, n, B, ldb, X, n, nrhs, R, norms, normA, normB, berr, st);
+      if (s != kOk) return s;
+      res->backward_error = berr;
+      if (berr <= tol) {
+        converged = true;
+        return kOk;
+      }
+      if (it >= iters_left) return kOk;
+      if (it > 0 && !(berr <= 0.5 * prev)) {
+        stalled = true;
+        return kOk;
+      }
+      prev = berr;
+      s = getrs_device(n, nrhs, lu, n, ipiv.data(), jpiv.data(), R, n, st);
+      if (s != kOk) return s;
+      axpy_kernel<<<grid_of((long long)nr), 256, 0, st>>>(R, n, X, n, n, nrhs);
+      res->iterations += 1;
+    }
+  };
+
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  cudaEventRecord(t0, st);
+  if (status == kOk) status = factor_and_solve(precision);
+  bool converged = false, stalled = false;
+  if (status == kOk && res->info == n) status = refine(max_iter, converged, stalled);
+  if (status == kOk && precision != DP_PRECISION_FP64 && !converged) {
+    // refinement on the mixed-precision factors stalled (or the mixed
+    // factorisation delayed): re-factor on the plain FP64 path
+    res->refactored = 1;
+    status = factor_and_solve(DP_PRECISION_FP64);
+    if (status == kOk && res->info == n) status = refine(max_iter, converged, stalled);
+  }
+  cudaEventRecord(t1, st);
+  cudaEventSynchronize(t1);
+  float tot = 0.f;
+  cudaEventElapsedTime(&tot, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  res->total_ms = tot;
+  res->converged = converged ? 1 : 0;
+  if (status == kOk && res->info == n)
+    copy_kernel<<<grid_of((long long)nr), 256, 0, st>>>(X, n, B, ldb, n, nrhs);
+  release();
+  return status;
+}
+
+}  // namespace dp
+
+extern "C" {
+
+int dp_getrs_device(int n, int nrhs, const double* d_lu, int ldlu, const int* ipiv,
+                    const int* jpiv, double* d_b, int ldb, void* stream) {
+  return dp::getrs_device(n, nrhs, d_lu, ldlu, ipiv, jpiv, d_b, ldb,
+                          static_cast<cudaStream_t>(stream));
+}
+
+int dp_gesv_ir_device(int n, int nrhs, const double* d_a, int lda, double* d_b, int ldb,
+                      int precision, int max_iter, double tol, dp_ir_result* result, void* stream) {
+  return dp::gesv_ir_device(n, nrhs, d_a, lda, d_b, ldb, precision, max_iter, tol, result,
+                            static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

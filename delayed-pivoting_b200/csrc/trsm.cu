@@ -1,18 +1,17 @@
-// Unit-lower triangular solve of the panel's block row:
-//   U12 <- L11^{-1} A12
-// (delayed_lu/delayed_dgetrf.cpp:72-74 `cblas_dtrsm(Left, Lower, NoTrans,
-// Unit)`; also the first half of materialize_partial_panel, :111-114).
+// Triangular solves with a diagonal block of at most 64 rows:
+//   lower, unit diagonal:   B <- L^{-1} B   (the panel's block row, U12 = L11^{-1} A12,
+//                           delayed_lu/delayed_dgetrf.cpp:72-74; also the first half of
+//                           materialize_partial_panel, :111-114; and the forward
+//                           substitution of the solve)
+//   upper, non-unit:        B <- U^{-1} B   (back substitution of the solve)
+// Wider blocks are split by the host into 64-wide solves and GEMM updates.
 //
-// Diagonal blocks are at most 64 wide (wider blocks are split by the host
-// into 64-wide solves and GEMM updates).  A CTA owns 64 columns of A12 and
-// two threads own each column, one per 32-row half, with their half in 32
-// registers and the forward substitution fully unrolled:
-//   phase 1: rows 0..31  <- L(0:32, 0:32)^{-1} rows 0..31
-//   phase 2: rows 32..63 <- L(32:64, 32:64)^{-1} (rows 32..63 - L(32:64, 0:32) rows 0..31)
-// L11 sits in shared memory (every load of it is a broadcast); the tile is
-// staged through shared memory so global loads and stores stay coalesced.
-// Rows / columns of L11 beyond w are zero, so narrower blocks run the same
-// code.
+// A CTA owns 64 columns of B; two threads own each column, one per 32-row
+// half, holding their half in 32 registers with the substitution fully
+// unrolled.  The triangle sits in shared memory (every load of it is a
+// broadcast); the tile is staged through shared memory so the global loads
+// and stores stay coalesced.  Rows / columns beyond w are an identity block,
+// so narrower blocks run the same code.
 #include "dp_device.cuh"
 #include "dp_kernels.h"
 
@@ -25,25 +24,42 @@ constexpr int kHalf = 32;
 constexpr int kTrsmCols = 64;  // columns per CTA
 constexpr int kTrsmThreads = 2 * kTrsmCols;
 constexpr int kStage = kTrsmW + 1;  // odd stride: conflict-free per-thread column access
-constexpr size_t kTrsmSmem = (size_t)(kTrsmW * kTrsmW + kTrsmCols * kStage) * sizeof(double);
+constexpr size_t kTrsmSmem =
+    (size_t)(kTrsmW * kTrsmW + kTrsmW + kTrsmCols * kStage) * sizeof(double);
 
+__device__ __forceinline__ void stage_in(const double* B, long long ldb, int w, int ncols,
+                                         double* Bt) {
+  for (int e = threadIdx.x; e < w * ncols; e += kTrsmThreads) {
+    const int i = e % w, c = e / w;
+    Bt[c * kStage + i] = B[idx(i, c, ldb)];
+  }
+}
+
+__device__ __forceinline__ void stage_out(double* B, long long ldb, int w, int ncols,
+                                          const double* Bt) {
+  for (int e = threadIdx.x; e < w * ncols; e += kTrsmThreads) {
+    const int i = e % w, cc = e / w;
+    B[idx(i, cc, ldb)] = Bt[cc * kStage + i];
+  }
+}
+
+// B (w x nc) <- L^{-1} B, L unit lower (w x w).
 __global__ void __launch_bounds__(kTrsmThreads)
-trsm_unit_lower_kernel(double* a, long long lda, int r0, int w, int c0, int nc) {
+trsm_lower_unit_kernel(const double* __restrict__ L, long long ldl, double* B, long long ldb, int w,
+                       int nc) {
   extern __shared__ __align__(16) double tsm[];
-  double* Ls = tsm;                   // Ls[p * 64 + i] = L(i, p), zero outside the strict lower part
-  double* Bt = tsm + kTrsmW * kTrsmW;  // Bt[c * 65 + i] = A12(i, c)
+  double* Ls = tsm;                    // Ls[p * 64 + i] = L(i, p), zero outside the strict lower part
+  double* Bt = tsm + kTrsmW * kTrsmW + kTrsmW;  // Bt[c * 65 + i] = B(i, c)
   const int tid = threadIdx.x;
-  const int col0 = c0 + blockIdx.x * kTrsmCols;
-  const int ncols = min(kTrsmCols, c0 + nc - col0);
+  const int col0 = blockIdx.x * kTrsmCols;
+  const int ncols = min(kTrsmCols, nc - col0);
+  B += idx(0, col0, ldb);
 
   for (int e = tid; e < kTrsmW * kTrsmW; e += kTrsmThreads) {
     const int i = e % kTrsmW, pcol = e / kTrsmW;
-    Ls[e] = (i > pcol && i < w) ? a[idx(r0 + i, r0 + pcol, lda)] : 0.0;
+    Ls[e] = (i > pcol && i < w) ? L[idx(i, pcol, ldl)] : 0.0;
   }
-  for (int e = tid; e < w * ncols; e += kTrsmThreads) {
-    const int i = e % w, c = e / w;
-    Bt[c * kStage + i] = a[idx(r0 + i, col0 + c, lda)];
-  }
+  stage_in(B, ldb, w, ncols, Bt);
   __syncthreads();
 
   const int c = tid % kTrsmCols;
@@ -83,27 +99,108 @@ trsm_unit_lower_kernel(double* a, long long lda, int r0, int w, int c0, int nc) 
       if (kHalf + i < w) bc[kHalf + i] = x[i];
   }
   __syncthreads();
-  for (int e = tid; e < w * ncols; e += kTrsmThreads) {
-    const int i = e % w, cc = e / w;
-    a[idx(r0 + i, col0 + cc, lda)] = Bt[cc * kStage + i];
+  stage_out(B, ldb, w, ncols, Bt);
+}
+
+// B (w x nc) <- U^{-1} B, U upper with its diagonal (w x w).
+__global__ void __launch_bounds__(kTrsmThreads)
+trsm_upper_kernel(const double* __restrict__ U, long long ldu, double* B, long long ldb, int w,
+                  int nc) {
+  extern __shared__ __align__(16) double tsm[];
+  double* Us = tsm;                     // Us[p * 64 + i] = U(i, p) for i < p, zero elsewhere
+  double* dg = tsm + kTrsmW * kTrsmW;   // diagonal, 1 beyond w
+  double* Bt = dg + kTrsmW;
+  const int tid = threadIdx.x;
+  const int col0 = blockIdx.x * kTrsmCols;
+  const int ncols = min(kTrsmCols, nc - col0);
+  B += idx(0, col0, ldb);
+
+  for (int e = tid; e < kTrsmW * kTrsmW; e += kTrsmThreads) {
+    const int i = e % kTrsmW, pcol = e / kTrsmW;
+    Us[e] = (i < pcol && pcol < w) ? U[idx(i, pcol, ldu)] : 0.0;
   }
+  for (int i = tid; i < kTrsmW; i += kTrsmThreads) dg[i] = i < w ? U[idx(i, i, ldu)] : 1.0;
+  stage_in(B, ldb, w, ncols, Bt);
+  __syncthreads();
+
+  const int c = tid % kTrsmCols;
+  const bool top = tid < kTrsmCols;  // warps 0-1: rows 0..31, warps 2-3: rows 32..63
+  double* bc = Bt + c * kStage;
+  if (!top && c < ncols && w > kHalf) {
+    double x[kHalf];
+#pragma unroll
+    for (int i = 0; i < kHalf; ++i) x[i] = kHalf + i < w ? bc[kHalf + i] : 0.0;
+#pragma unroll
+    for (int p = kHalf - 1; p >= 0; --p) {
+      x[p] /= dg[kHalf + p];
+#pragma unroll
+      for (int i = 0; i < p; ++i) x[i] -= Us[(kHalf + p) * kTrsmW + kHalf + i] * x[p];
+    }
+#pragma unroll
+    for (int i = 0; i < kHalf; ++i)
+      if (kHalf + i < w) bc[kHalf + i] = x[i];
+  }
+  __syncthreads();
+  if (top && c < ncols) {
+    double x[kHalf];
+#pragma unroll
+    for (int i = 0; i < kHalf; ++i) x[i] = i < w ? bc[i] : 0.0;
+    if (w > kHalf) {
+#pragma unroll 4
+      for (int p = 0; p < kHalf; ++p) {
+        const double xp = bc[kHalf + p];
+#pragma unroll
+        for (int i = 0; i < kHalf; ++i) x[i] -= Us[(kHalf + p) * kTrsmW + i] * xp;
+      }
+    }
+#pragma unroll
+    for (int p = kHalf - 1; p >= 0; --p) {
+      x[p] /= dg[p];
+#pragma unroll
+      for (int i = 0; i < p; ++i) x[i] -= Us[p * kTrsmW + i] * x[p];
+    }
+#pragma unroll
+    for (int i = 0; i < kHalf; ++i)
+      if (i < w) bc[i] = x[i];
+  }
+  __syncthreads();
+  stage_out(B, ldb, w, ncols, Bt);
+}
+
+bool g_configured = false;
+
+void configure() {
+  if (g_configured) return;
+  cudaFuncSetAttribute(trsm_lower_unit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)kTrsmSmem);
+  cudaFuncSetAttribute(trsm_upper_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)kTrsmSmem);
+  g_configured = true;
 }
 
 }  // namespace
 
 int trsm_max_width() { return kTrsmW; }
 
-void launch_trsm_unit_lower(double* a, long long lda, int r0, int w, int c0, int nc,
+void launch_trsm_lower_unit(const double* L, long long ldl, double* B, long long ldb, int w, int nc,
                             cudaStream_t s) {
   if (w <= 1 || nc <= 0) return;  // w == 1: unit diagonal, nothing to solve
-  static bool configured = false;
-  if (!configured) {
-    cudaFuncSetAttribute(trsm_unit_lower_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)kTrsmSmem);
-    configured = true;
-  }
+  configure();
   const int grid = (nc + kTrsmCols - 1) / kTrsmCols;
-  trsm_unit_lower_kernel<<<grid, kTrsmThreads, kTrsmSmem, s>>>(a, lda, r0, w, c0, nc);
+  trsm_lower_unit_kernel<<<grid, kTrsmThreads, kTrsmSmem, s>>>(L, ldl, B, ldb, w, nc);
+}
+
+void launch_trsm_upper(const double* U, long long ldu, double* B, long long ldb, int w, int nc,
+                       cudaStream_t s) {
+  if (w <= 0 || nc <= 0) return;
+  configure();
+  const int grid = (nc + kTrsmCols - 1) / kTrsmCols;
+  trsm_upper_kernel<<<grid, kTrsmThreads, kTrsmSmem, s>>>(U, ldu, B, ldb, w, nc);
+}
+
+void launch_trsm_unit_lower(double* a, long long lda, int r0, int w, int c0, int nc,
+                            cudaStream_t s) {
+  launch_trsm_lower_unit(a + idx(r0, r0, lda), lda, a + idx(r0, c0, lda), lda, w, nc, s);
 }
 
 }  // namespace dp

@@ -11,6 +11,7 @@ _LIB_DIR = _PKG / "lib"
 
 SUCCESS, INVALID_ARGUMENT, ALLOCATION_FAILED, CUDA_FAILURE, LIBRARY_FAILURE, DEVICE_TIMEOUT = range(6)
 POLICY_FULL_PIVOT, POLICY_NONZERO_COLUMN = 0, 1
+PRECISION_FP64, PRECISION_MIXED_BF16X3 = 0, 1
 
 _lib = None
 _gen = None
@@ -26,7 +27,22 @@ class Options(ctypes.Structure):
         ("panel_rows", ctypes.c_int),
         ("nb_outer", ctypes.c_int),
         ("panel_kernel", ctypes.c_int),
-        ("reserved", ctypes.c_int * 2),
+        ("precision", ctypes.c_int),
+        ("reserved", ctypes.c_int * 1),
+    ]
+
+
+class IRResult(ctypes.Structure):
+    """dp_ir_result of dp_gesv_ir_device."""
+
+    _fields_ = [
+        ("info", ctypes.c_int),
+        ("iterations", ctypes.c_int),
+        ("refactored", ctypes.c_int),
+        ("converged", ctypes.c_int),
+        ("backward_error", ctypes.c_double),
+        ("factor_ms", ctypes.c_double),
+        ("total_ms", ctypes.c_double),
     ]
 
 
@@ -52,6 +68,17 @@ def lib() -> ctypes.CDLL:
         L.dp_getrf_device_ex.restype = ctypes.c_int
         L.dp_getrf_device_ex.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
                                          ip, ip, ip, ctypes.c_void_p, ctypes.POINTER(Options)]
+        L.dp_getrs_device.restype = ctypes.c_int
+        L.dp_getrs_device.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                      ip, ip, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.dp_gesv_ir_device.restype = ctypes.c_int
+        L.dp_gesv_ir_device.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                        ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_double, ctypes.POINTER(IRResult), ctypes.c_void_p]
+        L.dp_stats_enable.restype = None
+        L.dp_stats_enable.argtypes = [ctypes.c_int]
+        L.dp_stats_reset.restype = None
+        L.dp_stats_reset.argtypes = []
         L.dp_status_string.restype = ctypes.c_char_p
         L.dp_status_string.argtypes = [ctypes.c_int]
         L.dp_options_init.restype = None
@@ -152,14 +179,32 @@ def delayed_getrf_cuda_status_string(status: int) -> str:
 
 
 def getrf_device_ex(m, n, d_a, lda, ipiv, jpiv, stream=None, nb=64, threshold=0.0,
-                    policy=POLICY_FULL_PIVOT, panel_rows=0, nb_outer=0, panel_kernel=0):
+                    policy=POLICY_FULL_PIVOT, panel_rows=0, nb_outer=0, panel_kernel=0,
+                    precision=PRECISION_FP64):
     """dp_getrf_device_ex with explicit options.  Returns (status, info)."""
     opt = Options()
     lib().dp_options_init(ctypes.byref(opt))
     opt.nb, opt.threshold, opt.policy, opt.panel_rows = nb, threshold, policy, panel_rows
     opt.nb_outer = nb_outer
     opt.panel_kernel = panel_kernel
+    opt.precision = precision
     info = ctypes.c_int(-1)
     st = lib().dp_getrf_device_ex(m, n, _dptr(d_a), lda, _iptr(ipiv), _iptr(jpiv),
                                   ctypes.byref(info), _stream(stream), ctypes.byref(opt))
     return st, info.value
+
+
+def getrs_device(n, nrhs, d_lu, ldlu, ipiv, jpiv, d_b, ldb, stream=None):
+    """dp_getrs_device: solve with the factors of getrf; d_b overwritten."""
+    return lib().dp_getrs_device(n, nrhs, _dptr(d_lu), ldlu, _iptr(ipiv), _iptr(jpiv),
+                                 _dptr(d_b), ldb, _stream(stream))
+
+
+def gesv_ir_device(n, nrhs, d_a, lda, d_b, ldb, precision=PRECISION_MIXED_BF16X3, max_iter=10,
+                   tol=1e-14, stream=None):
+    """dp_gesv_ir_device: mixed-precision LU + FP64 iterative refinement.
+    Returns (status, IRResult)."""
+    res = IRResult()
+    st = lib().dp_gesv_ir_device(n, nrhs, _dptr(d_a), lda, _dptr(d_b), ldb, precision, max_iter,
+                                 tol, ctypes.byref(res), _stream(stream))
+    return st, res

@@ -32,6 +32,10 @@ enum {
 
 enum { DP_POLICY_FULL_PIVOT = 0, DP_POLICY_NONZERO_COLUMN = 1 };
 
+/* Arithmetic of the O(n^3) trailing update.  Pivot search, delay / fallback
+ * decisions, panel and TRSM are FP64 in both modes. */
+enum { DP_PRECISION_FP64 = 0, DP_PRECISION_MIXED_BF16X3 = 1 };
+
 /* Tuning and semantics knobs; dp_options_init() fills the defaults that
  * reproduce the reference exactly (threshold 0, full-pivot fallback). */
 typedef struct dp_options {
@@ -42,7 +46,9 @@ typedef struct dp_options {
   int panel_rows;    /* target rows per CTA in the panel kernel; 0 = automatic */
   int nb_outer;      /* outer block width of the trailing update; 0 = automatic */
   int panel_kernel;  /* 0 automatic (cluster panel when it fits), 1 cluster, 2 grid-wide */
-  int reserved[2];
+  int precision;     /* DP_PRECISION_FP64 (reference arithmetic) or
+                        DP_PRECISION_MIXED_BF16X3 (tensor-core trailing update) */
+  int reserved[1];
 } dp_options;
 
 void dp_options_init(dp_options *opt);
@@ -73,6 +79,34 @@ int dp_getrf_hybrid_host(int m, int n, double *a, int lda, int *ipiv, int *jpiv,
 int dp_getrf_device_ex(int m, int n, double *d_a, int lda, int *ipiv, int *jpiv, int *info,
                        void *stream, const dp_options *opt);
 
+/* Solve A X = B with the factors of dp_getrf_device (no reference
+ * counterpart: the reference stops at the factorisation).  P*A*Q = L*U from
+ * the swap histories ipiv / jpiv (HOST arrays of n entries, as returned by
+ * dp_getrf_*); the factorisation must be complete (info == n).  d_b (n x nrhs,
+ * device) is overwritten with X.  Synchronises `stream`. */
+int dp_getrs_device(int n, int nrhs, const double *d_lu, int ldlu, const int *ipiv,
+                    const int *jpiv, double *d_b, int ldb, void *stream);
+
+typedef struct dp_ir_result {
+  int info;              /* factorisation info of the last factorisation */
+  int iterations;        /* refinement corrections applied (all factorisations) */
+  int refactored;        /* 1 when the mixed factors stalled and FP64 was used */
+  int converged;         /* 1 when backward_error <= tol */
+  double backward_error; /* max_c ||b_c - A x_c||_inf / (||A||_inf ||x_c||_inf + ||b_c||_inf) */
+  double factor_ms;      /* device time of the factorisation(s) */
+  double total_ms;       /* device time of the whole solve */
+} dp_ir_result;
+
+/* Solve A X = B by a (mixed-precision) delayed LU and FP64 iterative
+ * refinement (no reference counterpart).  d_a (n x n) is not modified; d_b
+ * (n x nrhs) is overwritten with X.  precision: DP_PRECISION_*; refinement
+ * stops at backward error <= tol, after max_iter corrections, or when the
+ * error stops halving - then a mixed-precision solve is re-factored in FP64.
+ * Synchronises `stream`. */
+int dp_gesv_ir_device(int n, int nrhs, const double *d_a, int lda, double *d_b, int ldb,
+                      int precision, int max_iter, double tol, dp_ir_result *result,
+                      void *stream);
+
 /* Per-kernel-family device timing (no reference counterpart; the reference
  * only times whole calls with std::chrono, delayed_lu_cuda/benchmark.cu:54-57).
  * When enabled, every call records CUDA events around each launch group on
@@ -86,6 +120,7 @@ enum {
   DP_KFAM_SEARCH = 4,/* fallback search over the active submatrix */
   DP_KFAM_SWAP = 5,  /* fallback full-row / full-column swaps and records */
   DP_KFAM_OTHER = 6, /* record initialisation */
+  DP_KFAM_GEMM_MIXED = 7, /* A22 -= L21 U12 on tcgen05 (BF16x3, incl. operand split) */
   DP_KFAM_COUNT = 8
 };
 typedef struct dp_kernel_stats {
