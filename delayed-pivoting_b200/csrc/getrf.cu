@@ -640,6 +640,106 @@ int getrf_host(int m, int n, double* a, int lda, int* ipiv, int* jpiv, int* info
   return status;
 }
 
+// ------------------------------------------- allocation-free variant ----
+// Some callers must not allocate device memory during a call: code running
+// under a memory manager that owns the whole device pool, callers that
+// budget every byte of HBM up front, or processes whose allocator is not the
+// CUDA runtime's.  getrf_device_noalloc runs the same plain-FP64 delayed LU
+// as getrf_device but takes its scratch (state block, device swap records,
+// panel swap lists, fallback-search candidates) from one file-scope device
+// array instead of cudaMallocAsync.  It always uses the cluster panel, which
+// needs no cross-CTA mailboxes, so the scratch stays small.
+//
+// The array belongs to the library: every GPU that loads it holds
+// kNoallocScratchBytes for as long as the process lives, every call uses the
+// same array (calls that overlap on the GPU - other threads or other streams
+// - race with each other and must be serialised by the caller), and each call
+// clears what it needs at start.  Limits: at most kNoallocMaxPivots pivots,
+// and the tallest panel must fit the cluster panel kernel.
+constexpr int kNoallocMaxPivots = 32768;
+constexpr size_t kNoallocScratchBytes = 320 * 1024;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
+
+// Device address of g_noalloc_scratch per device, looked up once (the host
+// name of a __device__ array is only a host-side handle, never a device
+// address).  The lookup is a host-side query and allocates nothing; it runs
+// on the first call on each device, which must therefore come before any
+// stream capture that contains the call.
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[64] = {};
+
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return kCudaFailure;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) {
+      cudaGetLastError();
+      return kCudaFailure;
+    }
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return kOk;
+}
+
+int getrf_device_noalloc(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* info,
+                         cudaStream_t st) {
+  if (info == nullptr) return kInvalidArgument;
+  *info = -1;
+  if (!valid_arguments(m, n, d_a, lda, ipiv, jpiv)) return kInvalidArgument;
+  const int pivots = std::min(m, n);
+  if (pivots > kNoallocMaxPivots) return kInvalidArgument;  // beyond the fixed scratch
+  Options o;
+  o.panel_kernel = 1;  // cluster panel only: no mailbox scratch
+  DeviceInfo di;
+  if (pivots > 0 && device_info(di) != kOk) return kCudaFailure;
+  if (pivots > 0) {
+    // the first panel is the tallest; every later one fits if it does
+    int w = std::min(o.nb, pivots), C = 0, R = 0;
+    if (!plan_cluster(m, w, di, C, R)) return kInvalidArgument;
+  }
+  *info = pivots;
+  for (int k = 0; k < pivots; ++k) ipiv[k] = jpiv[k] = k;
+  if (pivots == 0) return kOk;
+
+  void* scratch = nullptr;
+  if (noalloc_scratch(&scratch) != kOk) {
+    *info = -1;
+    return kCudaFailure;
+  }
+  Workspace ws;
+  const size_t bytes = layout_workspace(ws, nullptr, pivots, 0, kMaxPanelWidth, 0);
+  if (bytes > kNoallocScratchBytes) {
+    *info = -1;
+    return kInvalidArgument;
+  }
+  char* base = static_cast<char*>(scratch);
+  layout_workspace(ws, base, pivots, 0, kMaxPanelWidth, 0);
+  int status = kOk;
+  if (cudaMemsetAsync(base, 0, bytes, st) != cudaSuccess) status = kCudaFailure;
+  int inf = pivots;
+  Recorder rec(st);
+  rec.on = false;  // no timing events on this path
+  if (status == kOk) status = factorize(m, n, d_a, lda, o, ws, di, st, inf, rec);
+  if (status == kOk) {
+    if (cudaMemcpyAsync(ipiv, ws.d_ipiv, sizeof(int) * pivots, cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(jpiv, ws.d_jpiv, sizeof(int) * pivots, cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess)
+      status = kCudaFailure;
+  }
+  if (cudaStreamSynchronize(st) != cudaSuccess && status == kOk) status = kCudaFailure;
+  if (status != kOk) {
+    cudaGetLastError();
+    *info = -1;
+    return status;
+  }
+  *info = inf;
+  return kOk;
+}
+
 }  // namespace dp
 
 // ---------------------------------------------------------------- C ABI ----
@@ -701,6 +801,12 @@ void dp_stats_get(dp_kernel_stats* out) {
   if (!out) return;
   std::lock_guard<std::mutex> lock(dp::g_stats_mutex);
   *out = dp::g_stats;
+}
+
+int dp_getrf_device_noalloc(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* info,
+                            void* stream) {
+  return dp::getrf_device_noalloc(m, n, d_a, lda, ipiv, jpiv, info,
+                                  static_cast<cudaStream_t>(stream));
 }
 
 const char* dp_status_string(int status) {

@@ -22,7 +22,7 @@ from .api import (  # noqa: F401
     delayed_getrf_cuda_native_device, delayed_getrf_cuda_native_host,
     delayed_getrf_cuda_hybrid_device, delayed_getrf_cuda_hybrid_host,
     delayed_getrf_cuda_status_string, getrf_device_ex, getrs_device, gesv_ir_device, IRResult,
-    PRECISION_FP64, PRECISION_MIXED_BF16X3,
+    PRECISION_FP64, PRECISION_MIXED_BF16X3, getrf_device_noalloc,
 )
 from .inputs import (  # noqa: F401
     normal_matrix, plant_columns, mt64_nth, planted_matrix, uniform_stream, normal_vector,

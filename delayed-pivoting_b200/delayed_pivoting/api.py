@@ -60,7 +60,8 @@ def lib() -> ctypes.CDLL:
         L = ctypes.CDLL(str(path))
         ip = ctypes.POINTER(ctypes.c_int)
         for name in ("dp_getrf_device", "dp_getrf_host", "dp_getrf_native_device",
-                     "dp_getrf_native_host", "dp_getrf_hybrid_device", "dp_getrf_hybrid_host"):
+                     "dp_getrf_native_host", "dp_getrf_hybrid_device", "dp_getrf_hybrid_host",
+                     "dp_getrf_device_noalloc"):
             f = getattr(L, name)
             f.restype = ctypes.c_int
             f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ip, ip, ip,
@@ -208,3 +209,9 @@ def gesv_ir_device(n, nrhs, d_a, lda, d_b, ldb, precision=PRECISION_MIXED_BF16X3
     st = lib().dp_gesv_ir_device(n, nrhs, _dptr(d_a), lda, _dptr(d_b), ldb, precision, max_iter,
                                  tol, ctypes.byref(res), _stream(stream))
     return st, res
+
+
+def getrf_device_noalloc(m, n, d_a, lda, ipiv, jpiv, stream=None):
+    """dp_getrf_device_noalloc: dp_getrf_device without any device allocation
+    (scratch in a fixed array inside the library).  Returns (status, info)."""
+    return _call("dp_getrf_device_noalloc", m, n, _dptr(d_a), lda, ipiv, jpiv, stream)

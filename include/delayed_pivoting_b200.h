@@ -74,6 +74,22 @@ int dp_getrf_hybrid_device(int m, int n, double *d_a, int lda, int *ipiv, int *j
 int dp_getrf_hybrid_host(int m, int n, double *a, int lda, int *ipiv, int *jpiv, int *info,
                          void *stream);
 
+/* Allocation-free dp_getrf_device (no counterpart in the reference, which
+ * allocates its temporaries with cudaMalloc on every call).  For callers that
+ * cannot allocate device memory while factoring - a memory manager that owns
+ * the whole pool, a fixed HBM budget, an allocator other than the CUDA
+ * runtime's.  Same arguments, results and errors as dp_getrf_device (plain
+ * FP64, reference semantics); its scratch is one 320 KiB array inside the
+ * library, held on every GPU that loads the library until the process exits.
+ * Limits: min(m,n) <= 32768 and the first panel must fit the cluster panel
+ * kernel; larger inputs return DP_INVALID_ARGUMENT with info = -1.  All calls
+ * share the array: calls that overlap on the GPU (other threads, other
+ * streams) race and must be serialised by the caller.  The first call on a
+ * device looks the array's device address up; make it before capturing a
+ * stream that contains the call. */
+int dp_getrf_device_noalloc(int m, int n, double *d_a, int lda, int *ipiv, int *jpiv, int *info,
+                            void *stream);
+
 /* dp_getrf_device with explicit options (opt == NULL: defaults).  Also the
  * column-fallback policy of delayed_lu/delayed_dgetrf_column.hpp:18. */
 int dp_getrf_device_ex(int m, int n, double *d_a, int lda, int *ipiv, int *jpiv, int *info,
