@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--cpu-n", type=int, default=8192, help="CPU baseline sample size")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="trailing-update arithmetic of the factorisation")
     return ap.parse_args()
 
 
@@ -225,13 +227,15 @@ def main():
     jpiv = np.zeros(n, dtype=np.int32)
     stream = torch.cuda.current_stream(dev)
     L = dp.lib()
+    prec = dp.PRECISION_MIXED_BF16X3 if args.precision == "mixed" else dp.PRECISION_FP64
 
     def step(timed_events=None):
         work.copy_(orig)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        st, info = dp.getrf_device_ex(n, n, work, n, ipiv, jpiv, stream=stream, nb=args.nb)
+        st, info = dp.getrf_device_ex(n, n, work, n, ipiv, jpiv, stream=stream, nb=args.nb,
+                                      precision=prec)
         e1.record(stream)
         if st != 0:
             raise RuntimeError(dp.delayed_getrf_cuda_status_string(st))
@@ -322,7 +326,7 @@ def main():
                "sample": f"one delayed_getrf of n={args.cpu_n} (same generator, 0.1%/0.02% "
                          f"planted columns), {t_cpu:.2f} s, OpenBLAS {threads} threads"}
     if rank == 0:
-        fam = ["panel", "laswp", "trsm", "gemm", "search", "swap"]
+        fam = ["panel", "laswp", "trsm", "gemm", "search", "swap", "other", "gemm_mixed"]
         kern = {}
         for i, nm in enumerate(fam):
             if stats["launches"][i] == 0:
