@@ -12,6 +12,7 @@ _LIB_DIR = _PKG / "lib"
 SUCCESS, INVALID_ARGUMENT, ALLOCATION_FAILED, CUDA_FAILURE, LIBRARY_FAILURE, DEVICE_TIMEOUT = range(6)
 POLICY_FULL_PIVOT, POLICY_NONZERO_COLUMN = 0, 1
 PRECISION_FP64, PRECISION_MIXED_BF16X3 = 0, 1
+BATCH_MAX_N, BATCH_MAX_NB, BATCH_BUCKETS = 512, 32, 4
 
 _lib = None
 _gen = None
@@ -43,6 +44,17 @@ class IRResult(ctypes.Structure):
         ("backward_error", ctypes.c_double),
         ("factor_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double),
+    ]
+
+
+class BatchOptions(ctypes.Structure):
+    """dp_batch_options: threshold, precision, panel width per order bucket."""
+
+    _fields_ = [
+        ("threshold", ctypes.c_double),
+        ("precision", ctypes.c_int),
+        ("nb_bucket", ctypes.c_int * BATCH_BUCKETS),
+        ("reserved", ctypes.c_int * 2),
     ]
 
 
@@ -82,6 +94,27 @@ def lib() -> ctypes.CDLL:
         L.dp_stats_reset.argtypes = []
         L.dp_status_string.restype = ctypes.c_char_p
         L.dp_status_string.argtypes = [ctypes.c_int]
+        vp, ll = ctypes.c_void_p, ctypes.c_longlong
+        bo = ctypes.POINTER(BatchOptions)
+        L.dp_batch_options_init.restype = None
+        L.dp_batch_options_init.argtypes = [bo]
+        L.dp_batch_create.restype = ctypes.c_int
+        L.dp_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, vp, vp, bo]
+        L.dp_batch_layout.restype = ctypes.c_int
+        L.dp_batch_layout.argtypes = [vp, vp, vp, ctypes.POINTER(ll), ctypes.POINTER(ll)]
+        L.dp_batch_set_options.restype = ctypes.c_int
+        L.dp_batch_set_options.argtypes = [vp, bo]
+        for f in (L.dp_batch_getrf_async, L.dp_batch_getrf_graph):
+            f.restype = ctypes.c_int
+            f.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.dp_batch_destroy.restype = None
+        L.dp_batch_destroy.argtypes = [vp]
+        L.dp_batch_autotune.restype = ctypes.c_int
+        L.dp_batch_autotune.argtypes = [bo, ctypes.c_int, ctypes.c_ulonglong, vp]
+        L.dp_batch_tune_save.restype = ctypes.c_int
+        L.dp_batch_tune_save.argtypes = [ctypes.c_char_p, bo]
+        L.dp_batch_tune_load.restype = ctypes.c_int
+        L.dp_batch_tune_load.argtypes = [ctypes.c_char_p, bo]
         L.dp_options_init.restype = None
         L.dp_options_init.argtypes = [ctypes.POINTER(Options)]
         _lib = L
@@ -215,3 +248,90 @@ def getrf_device_noalloc(m, n, d_a, lda, ipiv, jpiv, stream=None):
     """dp_getrf_device_noalloc: dp_getrf_device without any device allocation
     (scratch in a fixed array inside the library).  Returns (status, info)."""
     return _call("dp_getrf_device_noalloc", m, n, _dptr(d_a), lda, ipiv, jpiv, stream)
+
+
+# ---- batched factorisation (dp_batch_*) -------------------------------------
+
+def batch_options(threshold=0.0, nb_bucket=None, precision=PRECISION_FP64) -> BatchOptions:
+    opt = BatchOptions()
+    lib().dp_batch_options_init(ctypes.byref(opt))
+    opt.threshold = threshold
+    opt.precision = precision
+    if nb_bucket is not None:
+        if isinstance(nb_bucket, int):
+            nb_bucket = [nb_bucket] * BATCH_BUCKETS
+        for i, v in enumerate(nb_bucket):
+            opt.nb_bucket[i] = int(v)
+    return opt
+
+
+class BatchError(RuntimeError):
+    def __init__(self, status, what):
+        super().__init__(f"{what}: status {status}")
+        self.status = status
+
+
+class Batch:
+    """A dp_batch plan: the orders of a batch of square matrices, their
+    layout in one device buffer, and the device work queue of the persistent
+    kernel.  Matrix i is column-major with lda = n[i] at element offset
+    ``offsets[i]``; its records are the n[i] entries at ``record_offsets[i]``
+    of the device ipiv / jpiv arrays, its info ``info[i]``."""
+
+    def __init__(self, ns, offsets=None, options: BatchOptions | None = None):
+        self._h = None
+        self.ns = np.ascontiguousarray(ns, dtype=np.int32)
+        off = None if offsets is None else np.ascontiguousarray(offsets, dtype=np.int64)
+        h = ctypes.c_void_p()
+        st = lib().dp_batch_create(ctypes.byref(h), len(self.ns), self.ns.ctypes.data,
+                                   None if off is None else off.ctypes.data,
+                                   None if options is None else ctypes.byref(options))
+        if st != SUCCESS:
+            raise BatchError(st, "dp_batch_create")
+        self._h = h
+        n = len(self.ns)
+        self.offsets = np.zeros(n, dtype=np.int64)
+        self.record_offsets = np.zeros(n, dtype=np.int64)
+        te, tr = ctypes.c_longlong(), ctypes.c_longlong()
+        lib().dp_batch_layout(h, self.offsets.ctypes.data, self.record_offsets.ctypes.data,
+                              ctypes.byref(te), ctypes.byref(tr))
+        self.total_elements, self.total_records = te.value, tr.value
+
+    def set_options(self, options: BatchOptions) -> int:
+        return lib().dp_batch_set_options(self._h, ctypes.byref(options))
+
+    def getrf_async(self, d_base, d_ipiv, d_jpiv, d_info, stream=None) -> int:
+        return lib().dp_batch_getrf_async(self._h, _dptr(d_base), _dptr(d_ipiv), _dptr(d_jpiv),
+                                          _dptr(d_info), _stream(stream))
+
+    def getrf_graph(self, d_base, d_ipiv, d_jpiv, d_info, stream=None) -> int:
+        return lib().dp_batch_getrf_graph(self._h, _dptr(d_base), _dptr(d_ipiv), _dptr(d_jpiv),
+                                          _dptr(d_info), _stream(stream))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().dp_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_autotune(options: BatchOptions | None = None, samples=12, seed=2024, stream=None):
+    """dp_batch_autotune: returns (status, options with the tuned widths)."""
+    opt = options if options is not None else batch_options()
+    st = lib().dp_batch_autotune(ctypes.byref(opt), samples, seed, _stream(stream))
+    return st, opt
+
+
+def batch_tune_save(path, options: BatchOptions) -> int:
+    return lib().dp_batch_tune_save(str(path).encode(), ctypes.byref(options))
+
+
+def batch_tune_load(path, options: BatchOptions | None = None):
+    opt = options if options is not None else batch_options()
+    st = lib().dp_batch_tune_load(str(path).encode(), ctypes.byref(opt))
+    return st, opt

@@ -54,3 +54,46 @@ def normal_vector(count: int, seed: int) -> np.ndarray:
     if count:
         matgen().dpgen_normal_vector(out.ctypes.data, count, seed)
     return out
+
+
+# ---- batches of small matrices -------------------------------------------
+
+def batch_orders(count: int, seed: int, lo: int = 32, hi: int = 512, p_zero: float = 0.3):
+    """Orders log-uniform in [lo, hi] and, per matrix, 0-2 exact-zero columns
+    (two independent draws with probability p_zero each).  Returns (ns, n_zero)
+    as int32 arrays."""
+    u = uniform_stream(3 * count, seed).reshape(count, 3) if count else np.zeros((0, 3))
+    ns = np.floor(np.exp(np.log(lo) + u[:, 0] * (np.log(hi + 1) - np.log(lo))))
+    ns = np.clip(ns, lo, hi).astype(np.int32)
+    n_zero = (u[:, 1] < p_zero).astype(np.int32) + (u[:, 2] < p_zero).astype(np.int32)
+    return ns, n_zero.astype(np.int32)
+
+
+def batch_matrix_seed(seed: int, i: int) -> int:
+    return (seed * 1_000_003 + i) & 0xFFFFFFFFFFFFFFFF
+
+
+def fill_batch(buf: np.ndarray, offsets, ns, n_zero, seed: int) -> None:
+    """Writes matrix i (N(0,1), n_zero[i] planted exact-zero columns, column-major,
+    lda = ns[i]) at element offsets[i] of the float64 host buffer `buf`."""
+    G = matgen()
+    assert buf.dtype == np.float64 and buf.flags.c_contiguous
+    base = buf.ctypes.data
+    scratch = np.zeros(4, dtype=np.int32)
+    for i, (n, off, nz) in enumerate(zip(ns, offsets, n_zero)):
+        n, off, nz = int(n), int(off), int(nz)
+        assert off + n * n <= buf.size
+        ptr = base + 8 * off
+        s = batch_matrix_seed(seed, i)
+        G.dpgen_normal_matrix(n, n, ptr, n, s)
+        if nz:
+            rc = G.dpgen_plant_columns(n, n, ptr, n, s, 0, 1e-18, nz, scratch.ctypes.data,
+                                       scratch[2:].ctypes.data)
+            if rc != 0:
+                raise ValueError("bad planted-column counts")
+
+
+def batch_matrix(ns, n_zero, seed: int, i: int) -> np.ndarray:
+    """Matrix i of fill_batch as an (n x n) Fortran array."""
+    n = int(ns[i])
+    return planted_matrix(n, n, batch_matrix_seed(seed, i), 0, int(n_zero[i]))

@@ -123,6 +123,60 @@ int dp_gesv_ir_device(int n, int nrhs, const double *d_a, int lda, double *d_b, 
                       int precision, int max_iter, double tol, dp_ir_result *result,
                       void *stream);
 
+/* ---- Batched factorisation (no reference counterpart: the reference factors
+ * one matrix per call).  Thousands of independent square matrices of orders
+ * 1..DP_BATCH_MAX_N, each column-major with lda = its order, factored by ONE
+ * persistent kernel launch that pulls matrices from a device work queue
+ * (largest first).  Each matrix gets exactly the single-matrix semantics of
+ * dp_getrf_device (delayed_lu/delayed_dgetrf.cpp:129-251): same records, same
+ * info, compact L\U in place.  Records stay on the device: matrix i's ipiv /
+ * jpiv are the n_i entries at its record offset, info[i] its info. */
+#define DP_BATCH_MAX_N 512
+#define DP_BATCH_MAX_NB 32
+#define DP_BATCH_BUCKETS 4 /* panel-width buckets: n < 64, < 128, < 256, <= 512 */
+
+typedef struct dp_batch_options {
+  double threshold;                /* accept a pivot iff |alpha| > threshold */
+  int precision;                   /* DP_PRECISION_FP64 */
+  int nb_bucket[DP_BATCH_BUCKETS]; /* panel width per order bucket, 1..DP_BATCH_MAX_NB */
+  int reserved[2];
+} dp_batch_options;
+
+void dp_batch_options_init(dp_batch_options *opt);
+
+typedef struct dp_batch dp_batch; /* a plan: the orders, the layout, the queue */
+
+/* n: host array of `count` orders.  offsets: host array of each matrix's
+ * first element in the caller's buffer, or NULL for the packed layout (each
+ * matrix after the previous one, rounded up to 4 elements).  Allocates the
+ * plan's small device arrays (on the current device). */
+int dp_batch_create(dp_batch **plan, int count, const int *n, const long long *offsets,
+                    const dp_batch_options *opt);
+/* The plan's matrix offsets (elements), record offsets, buffer and record
+ * totals; any output may be NULL. */
+int dp_batch_layout(const dp_batch *plan, long long *offsets, long long *record_offsets,
+                    long long *total_elements, long long *total_records);
+int dp_batch_set_options(dp_batch *plan, const dp_batch_options *opt);
+/* Enqueue the factorisation of every matrix of d_base on `stream` (device
+ * records d_ipiv / d_jpiv of total_records entries, d_info of count); returns
+ * without synchronising and may be captured into a CUDA graph.  One plan runs
+ * one launch at a time (the launches share the plan's work counter). */
+int dp_batch_getrf_async(dp_batch *plan, double *d_base, int *d_ipiv, int *d_jpiv, int *d_info,
+                         void *stream);
+/* The same launch replayed from a CUDA graph the plan captures on first use
+ * (and again when the pointers or options change). */
+int dp_batch_getrf_graph(dp_batch *plan, double *d_base, int *d_ipiv, int *d_jpiv, int *d_info,
+                         void *stream);
+void dp_batch_destroy(dp_batch *plan);
+
+/* Autotuner: for each bucket, times every candidate panel width on `samples`
+ * seeded N(0,1) matrices whose orders spread log-uniformly over the bucket,
+ * and writes the fastest into opt->nb_bucket.  Synchronises `stream`. */
+int dp_batch_autotune(dp_batch_options *opt, int samples, unsigned long long seed, void *stream);
+/* Tuning table file: one line per bucket, "<smallest n> <largest n> <nb>". */
+int dp_batch_tune_save(const char *path, const dp_batch_options *opt);
+int dp_batch_tune_load(const char *path, dp_batch_options *opt);
+
 /* Per-kernel-family device timing (no reference counterpart; the reference
  * only times whole calls with std::chrono, delayed_lu_cuda/benchmark.cu:54-57).
  * When enabled, every call records CUDA events around each launch group on

@@ -6,6 +6,10 @@ OpenBLAS).  Run from the repository root:
     python tests/golden/make_golden.py            # all cases except n=16384
     python tests/golden/make_golden.py --large    # also the n=16384 case
 
+It also writes tests/golden/batch/config4_subset64.npz: the reference's
+records for a seeded 64-matrix subset of the batched workload (orders
+log-uniform in [32, 512], 0-2 exact-zero columns each).
+
 Each case is written to tests/golden/<name>.npz with the inputs' recipe
 (generator seed and planted columns, or the literal matrix for the reference's
 own small known-answer cases), the reference's ipiv / jpiv / info, and its
@@ -44,6 +48,7 @@ GENERATED = [
     ("all_zero_9x9", 9, 9, 9, 6, 0, 9, 0),
 ]
 LARGE = [("config2_n16384", 16384, 16384, 16384, 16384, 16, 3, 0)]
+BATCH_SUBSET = ("config4_subset64", 64, 8192)  # (name, count, seed)
 
 
 def reference_known_answer():
@@ -103,6 +108,28 @@ def main():
                             scaled_residual=res)
         swaps = int((jpiv != np.arange(len(jpiv))).sum())
         print(f"{name}: info={info} column_swaps={swaps} scaled_residual={res:.3g}")
+    batch_subset()
+
+
+def batch_subset():
+    name, count, seed = BATCH_SUBSET
+    ns, n_zero = dp.batch_orders(count, seed)
+    ipivs, jpivs, infos, worst = [], [], [], 0.0
+    for i in range(count):
+        n = int(ns[i])
+        a = dp.batch_matrix(ns, n_zero, seed, i)
+        ipiv, jpiv, info, res = run_reference(a, n, n, 0)
+        ipivs.append(ipiv)
+        jpivs.append(jpiv)
+        infos.append(info)
+        worst = max(worst, res)
+    (OUT / "batch").mkdir(exist_ok=True)
+    np.savez_compressed(OUT / "batch" / f"{name}.npz", count=count, seed=seed, ns=ns,
+                        n_zero=n_zero, ipiv=np.concatenate(ipivs), jpiv=np.concatenate(jpivs),
+                        info=np.array(infos, dtype=np.int32))
+    delayed = int((np.array(infos) < ns).sum())
+    print(f"{name}: {count} matrices, n in [{ns.min()}, {ns.max()}], {int(n_zero.sum())} zero "
+          f"columns, {delayed} delayed, worst scaled_residual={worst:.3g}")
 
 
 if __name__ == "__main__":
