@@ -96,8 +96,9 @@ __host__ __device__ inline int bucket_of(int n) {
 
 struct Smem {
   // dynamic part: P [pr * kMaxNb], then Bs [kStageN * kLdb]
-  double crow[2][kWarps][kSb];     // each warp's candidate row (sub-panel part), by step parity
-  double rval[2][kWarps];
+  double crow[2][kWarps][kSb + 1]; // each warp's candidate row (sub-panel part) and the
+                                   // reciprocal of its pivot entry, by step parity
+  double rval[2][kWarps];          // each warp's best magnitude (>= 0) and logical row
   int rkey[2][kWarps];
   double psave[kSb][kLdsave];      // the current sub-panel's pivot rows, whole window
   short mv_dst[2 * kMaxNb];        // the panel's composite row permutation:
@@ -120,6 +121,20 @@ __device__ __forceinline__ void mma_f64(double (&c)[4], double a0, double a1, do
 // Candidate (magnitude v, logical row key) beats (cv, ck)?
 __device__ __forceinline__ bool beats(double v, int key, double cv, int ck) {
   return v > cv || (v == cv && key < ck);
+}
+
+// Best (largest magnitude, then smallest key) of the warp's candidates.  A
+// magnitude is >= 0 (a lane without a candidate offers 0 with key kNone), so
+// its bit pattern orders like its value: max of the high word, then of the
+// low word among the lanes holding that high word, then min key among the
+// lanes holding the maximum - three warp reductions.
+__device__ __forceinline__ void warp_best(double v, int key, double& bv, int& bk) {
+  const unsigned long long u = (unsigned long long)__double_as_longlong(v);
+  const unsigned hi = (unsigned)(u >> 32), lo = (unsigned)u;
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+  bk = __reduce_min_sync(0xffffffffu, (hi == mhi && lo == mlo) ? key : kNone);
+  bv = __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
 }
 
 // Factor panel columns [b, b + w) of the n x n matrix A (rows b..n-1).
@@ -151,39 +166,40 @@ __device__ __forceinline__ int panel_regs(double* A, int n, int lda, int b, int 
       x[i][c] = (r < rows && c < w) ? A[idx(b + r, b + c, lda)] : 0.0;
   }
 
-  // warp best of the lane candidates (cv, ck from the lane's row ci); the
-  // winning lane pushes its sub-panel columns j.. to s.crow[par][warp]
+  // warp best of the lane candidates (cv >= 0, ck from the lane's row ci);
+  // the winning lane pushes its sub-panel columns j.., the reciprocal of its
+  // entry in column j (computed by every lane ahead of the reductions, off
+  // the path after the barrier) and the warp's result
   auto push = [&](int j, int par, double cv, int ck, int ci) {
-    double wv = cv;
-    int wk = ck;
+    double pv = 0.0;
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, wv, off);
-      const int ok = __shfl_xor_sync(0xffffffffu, wk, off);
-      if (beats(ov, ok, wv, wk)) {
-        wv = ov;
-        wk = ok;
+    for (int c = 0; c < kSb; ++c)
+      if (c == j) pv = ci ? x[kRpt - 1][c] : x[0][c];
+    const double rinv = 1.0 / pv;
+    double wv;
+    int wk;
+    warp_best(cv, ck, wv, wk);
+    if (wk != kNone ? ck == wk : lane == 0) {
+      if (wk != kNone) {
+#pragma unroll
+        for (int c = 0; c < kSb; ++c)
+          if (c >= j) s.crow[par][warp][c] = ci ? x[kRpt - 1][c] : x[0][c];
+        s.crow[par][warp][kSb] = rinv;
       }
-    }
-    if (wk != kNone && ck == wk) {
-#pragma unroll
-      for (int c = 0; c < kSb; ++c)
-        if (c >= j) s.crow[par][warp][c] = ci ? x[kRpt - 1][c] : x[0][c];
-    }
-    if (lane == 0) {
       s.rval[par][warp] = wv;
       s.rkey[par][warp] = wk;
     }
   };
   // candidate of window column 0 among the rows at logical positions >= first
   auto first_candidate = [&](int first, bool placed) {
-    double cv = -1.0;
+    double cv = 0.0;
     int ck = kNone, ci = 0;
 #pragma unroll
     for (int i = 0; i < kRpt; ++i) {
       if (lp[i] == kNone || lp[i] < first) continue;
       // a placed pivot (after a fallback) is the only candidate of its step
-      const double v = placed ? (lp[i] == first ? INFINITY : -1.0) : fabs(x[i][0]);
+      if (placed && lp[i] != first) continue;
+      const double v = placed ? INFINITY : fabs(x[i][0]);
       if (beats(v, lp[i], cv, ck)) {
         cv = v;
         ck = lp[i];
@@ -206,18 +222,12 @@ __device__ __forceinline__ int panel_regs(double* A, int n, int lda, int b, int 
     for (int j = 0; j < kSb; ++j) {
       if (j >= sw) break;
       const int st = base + j, par = st & 1;
-      double bv = s.rval[par][0];
-      int bk = s.rkey[par][0], bw = 0;
-#pragma unroll
-      for (int q = 1; q < kWarps; ++q) {
-        const double v = s.rval[par][q];
-        const int k = s.rkey[par][q];
-        if (beats(v, k, bv, bk)) {
-          bv = v;
-          bk = k;
-          bw = q;
-        }
-      }
+      double bv;
+      int bk;
+      warp_best(s.rval[par][lane & (kWarps - 1)], s.rkey[par][lane & (kWarps - 1)], bv, bk);
+      // the warp that offered the winner (keys of real candidates are unique)
+      const int bw = max(0, __ffs(__ballot_sync(0xffffffffu, lane < kWarps && bk != kNone &&
+                                                                s.rkey[par][lane] == bk)) - 1);
       const bool placed = positioned && st == 0;
       if (!placed && !(bv > thr)) {
         stop = st;
@@ -227,8 +237,8 @@ __device__ __forceinline__ int panel_regs(double* A, int n, int lda, int b, int 
       const double* prow = s.crow[par][bw];
       const int p = bk;  // logical position of the pivot row before the swap
       if (tid == 0 && !placed) ipiv[b + st] = b + p;
-      const double inv = 1.0 / prow[j];
-      double cv = -1.0;
+      const double inv = prow[kSb];
+      double cv = 0.0;
       int ck = kNone, ci = 0;
 #pragma unroll
       for (int i = 0; i < kRpt; ++i) {
