@@ -48,6 +48,7 @@
 
 #include "delayed_pivoting_b200.h"
 #include "dp_device.cuh"
+#include "serve_kernels.h"
 
 namespace dp {
 namespace batch {
@@ -685,22 +686,42 @@ bool valid_batch_options(const dp_batch_options* o) {
 }
 
 int launch(dp_batch* bp, double* d_base, int* d_ipiv, int* d_jpiv, int* d_info, cudaStream_t st) {
-  using namespace dp::batch;
+  return dp::batch::launch_raw(bp->count, bp->max_n, bp->sms, bp->d_n, bp->d_offsets, bp->d_rec,
+                               bp->d_order, bp->d_queue, d_base, d_ipiv, d_jpiv, d_info, bp->opt,
+                               st);
+}
+
+bool aligned8(const void* p) { return ((uintptr_t)p & 7) == 0; }
+
+}  // namespace
+
+namespace dp {
+namespace batch {
+
+// The batched launch on caller-managed device arrays (the server's small-
+// request path, which allocates from the stream-ordered pool): d_n, d_off,
+// d_rec, d_order describe `count` matrices as in a dp_batch plan, d_queue is
+// one int of scratch.
+int launch_raw(int count, int max_n, int sms, const int* d_n, const long long* d_off,
+               const long long* d_rec, const int* d_order, int* d_queue, double* base, int* ipiv,
+               int* jpiv, int* info, const dp_batch_options& opt, cudaStream_t st) {
+  if (count <= 0) return DP_SUCCESS;
+  if (max_n < 1 || max_n > DP_BATCH_MAX_N || !valid_batch_options(&opt)) return DP_INVALID_ARGUMENT;
   Params p;
-  p.base = d_base;
-  p.offsets = bp->d_offsets;
-  p.ns = bp->d_n;
-  p.rec_offsets = bp->d_rec;
-  p.order = bp->d_order;
-  p.count = bp->count;
-  p.queue = bp->d_queue;
-  p.ipiv = d_ipiv;
-  p.jpiv = d_jpiv;
-  p.info = d_info;
-  p.threshold = bp->opt.threshold;
-  for (int i = 0; i < DP_BATCH_BUCKETS; ++i) p.nb_bucket[i] = bp->opt.nb_bucket[i];
-  p.pr = panel_ld(std::max(bp->max_n, 1));
-  const size_t smem = dynamic_smem(bp->max_n);
+  p.base = base;
+  p.offsets = d_off;
+  p.ns = d_n;
+  p.rec_offsets = d_rec;
+  p.order = d_order;
+  p.count = count;
+  p.queue = d_queue;
+  p.ipiv = ipiv;
+  p.jpiv = jpiv;
+  p.info = info;
+  p.threshold = opt.threshold;
+  for (int i = 0; i < DP_BATCH_BUCKETS; ++i) p.nb_bucket[i] = opt.nb_bucket[i];
+  p.pr = panel_ld(max_n);
+  const size_t smem = dynamic_smem(max_n);
   if (cudaFuncSetAttribute(batched_getrf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
     return DP_CUDA_FAILURE;
@@ -709,13 +730,16 @@ int launch(dp_batch* bp, double* d_base, int* d_ipiv, int* d_jpiv, int* d_info, 
                                                     smem) != cudaSuccess ||
       per_sm < 1)
     return DP_CUDA_FAILURE;
-  const int grid = std::max(1, std::min(bp->count, bp->sms * per_sm));
-  if (cudaMemsetAsync(bp->d_queue, 0, sizeof(int), st) != cudaSuccess) return DP_CUDA_FAILURE;
+  const int grid = std::max(1, std::min(count, sms * per_sm));
+  if (cudaMemsetAsync(d_queue, 0, sizeof(int), st) != cudaSuccess) return DP_CUDA_FAILURE;
   batched_getrf_kernel<<<grid, kThreads, smem, st>>>(p);
   return cudaGetLastError() == cudaSuccess ? DP_SUCCESS : DP_CUDA_FAILURE;
 }
 
-bool aligned8(const void* p) { return ((uintptr_t)p & 7) == 0; }
+}  // namespace batch
+}  // namespace dp
+
+namespace {
 
 const int kBucketLo[DP_BATCH_BUCKETS] = {1, 64, 128, 256};
 const int kBucketHi[DP_BATCH_BUCKETS] = {63, 127, 255, 512};

@@ -1,9 +1,11 @@
 // Kernel parameter blocks and host-side launch wrappers of the
 // delayed-pivoting LU.  Internal to the library (not part of the C ABI).
 #pragma once
+#include <vector>
 
 #include <cuda_runtime.h>
 
+#include "delayed_pivoting_b200.h"
 #include "dp_device.cuh"
 
 namespace dp {
@@ -83,5 +85,31 @@ void launch_swap_col(double* a, long long lda, int m, int c1, int c2, cudaStream
 
 void launch_identity_records(int* ipiv, int* jpiv, int count, cudaStream_t s);
 void launch_set_record(int* ipiv, int* jpiv, int k, int p, int q, cudaStream_t s);
+
+// ---- resident factorisations (solve.cu) ----------------------------------
+
+// A factorisation kept on the device for repeated solves: the compact L\U,
+// its swap histories (host) and their composite row / column orders (device).
+struct Factor {
+  int n = 0;
+  int info = -1;
+  int precision = 0;                  // DP_PRECISION_* of the factors held now
+  int refactored = 0;                 // 1 once a stalled refinement forced FP64
+  double normA = 0.0;                 // ||A||_inf
+  double factor_ms = 0.0;             // device time of all factorisations
+  double* lu = nullptr;
+  int* d_perm = nullptr;              // row order [n], column order [n]
+  std::vector<int> ipiv, jpiv;
+};
+
+// Device bytes a Factor of order n holds.
+size_t factor_bytes(int n);
+// Factor A (n x n, lda, device, not modified) at `precision`; synchronises st.
+int factor_create(Factor** out, int n, const double* A, int lda, int precision, cudaStream_t st);
+// Solve A X = B with FP64 refinement; B (n x nrhs, device) becomes X.  Mixed
+// factors whose refinement stalls are replaced by plain FP64 factors of A.
+int factor_solve(Factor* f, const double* A, int lda, double* B, int ldb, int nrhs, int max_iter,
+                 double tol, dp_ir_result* res, cudaStream_t st);
+void factor_destroy(Factor* f, cudaStream_t st);
 
 }  // namespace dp

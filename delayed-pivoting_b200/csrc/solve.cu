@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <new>
 #include <vector>
 
 #include "delayed_pivoting_b200.h"
@@ -206,6 +207,226 @@ int backward_error(const double* A, int lda, int n, const double* B, int ldb, co
 
 }  // namespace
 
+namespace {
+
+// lu <- A, factor at `prec`, composite orders to the device.
+int factorize(Factor& f, const double* A, int lda, int prec, cudaStream_t st) {
+  const int n = f.n;
+  copy_kernel<<<grid_of((long long)n * n), 256, 0, st>>>(A, lda, f.lu, n, n, n);
+  dp_options opt;
+  dp_options_init(&opt);
+  opt.precision = prec;
+  int info = -1;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, st);
+  const int s = getrf_device(n, n, f.lu, n, f.ipiv.data(), f.jpiv.data(), &info, st, &opt);
+  cudaEventRecord(e1, st);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  f.factor_ms += ms;
+  f.info = info;
+  f.precision = prec;
+  if (s != kOk || info < n) return s;
+  std::vector<int> order(2 * (size_t)n);
+  for (int i = 0; i < n; ++i) order[i] = order[n + i] = i;
+  for (int k = 0; k < n; ++k) {
+    std::swap(order[k], order[f.ipiv[k]]);
+    std::swap(order[n + k], order[n + f.jpiv[k]]);
+  }
+  if (cudaMemcpyAsync(f.d_perm, order.data(), sizeof(int) * 2 * (size_t)n, cudaMemcpyHostToDevice,
+                      st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return kCudaFailure;
+  return kOk;
+}
+
+// X = A^{-1} B through the factors (X, tmp: n x nrhs, leading dimension n).
+void solve_with(const Factor& f, const double* B, int ldb, double* X, double* tmp, int nrhs,
+                cudaStream_t st) {
+  const int n = f.n;
+  const long long total = (long long)n * nrhs;
+  gather_rows_kernel<<<grid_of(total), 256, 0, st>>>(B, ldb, tmp, n, f.d_perm, n, nrhs);
+  forward_solve(f.lu, n, n, tmp, n, nrhs, st);
+  backward_solve(f.lu, n, n, tmp, n, nrhs, st);
+  scatter_rows_kernel<<<grid_of(total), 256, 0, st>>>(tmp, n, X, n, f.d_perm + n, n, nrhs);
+}
+
+}  // namespace
+
+void factor_destroy(Factor* f, cudaStream_t st) {
+  if (!f) return;
+  if (f->lu) cudaFreeAsync(f->lu, st);
+  if (f->d_perm) cudaFreeAsync(f->d_perm, st);
+  cudaStreamSynchronize(st);
+  delete f;
+}
+
+size_t factor_bytes(int n) { return sizeof(double) * (size_t)n * n + sizeof(int) * 2 * (size_t)n; }
+
+int factor_create(Factor** out, int n, const double* A, int lda, int precision, cudaStream_t st) {
+  if (!out) return kInvalidArgument;
+  *out = nullptr;
+  if (n < 1 || lda < n || !A ||
+      (precision != DP_PRECISION_FP64 && precision != DP_PRECISION_MIXED_BF16X3))
+    return kInvalidArgument;
+  auto* f = new (std::nothrow) Factor;
+  if (!f) return kAllocationFailed;
+  f->n = n;
+  f->ipiv.resize(n);
+  f->jpiv.resize(n);
+  double* normA = nullptr;
+  if (cudaMallocAsync(reinterpret_cast<void**>(&f->lu), sizeof(double) * (size_t)n * n, st) !=
+          cudaSuccess ||
+      cudaMallocAsync(reinterpret_cast<void**>(&f->d_perm), sizeof(int) * 2 * (size_t)n, st) !=
+          cudaSuccess ||
+      cudaMallocAsync(reinterpret_cast<void**>(&normA), sizeof(double), st) != cudaSuccess) {
+    cudaGetLastError();
+    if (normA) cudaFreeAsync(normA, st);
+    factor_destroy(f, st);
+    return kAllocationFailed;
+  }
+  int status = kOk;
+  if (cudaMemsetAsync(normA, 0, sizeof(double), st) != cudaSuccess) status = kCudaFailure;
+  if (status == kOk) {
+    row_abs_sum_kernel<<<(n + 255) / 256, 256, 0, st>>>(A, lda, n, normA);
+    if (cudaMemcpyAsync(&f->normA, normA, sizeof(double), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      status = kCudaFailure;
+  }
+  cudaFreeAsync(normA, st);
+  if (status == kOk) status = factorize(*f, A, lda, precision, st);
+  if (status != kOk) {
+    factor_destroy(f, st);
+    return status;
+  }
+  *out = f;
+  return kOk;
+}
+
+// Solve A X = B with the factors and FP64 refinement (A: the matrix the
+// factors came from, B overwritten with X).  A refinement on mixed-precision
+// factors that stalls (error not halved) or misses the tolerance re-factors
+// A in plain FP64 - the factors stay FP64 for later solves.
+int factor_solve(Factor* f, const double* A, int lda, double* B, int ldb, int nrhs, int max_iter,
+                 double tol, dp_ir_result* res, cudaStream_t st) {
+  if (!res) return kInvalidArgument;
+  std::memset(res, 0, sizeof(*res));
+  res->info = f ? f->info : -1;
+  res->backward_error = INFINITY;
+  if (!f || nrhs < 0 || lda < f->n || ldb < f->n || max_iter < 0 || !(tol >= 0.0) || !A ||
+      (nrhs > 0 && !B))
+    return kInvalidArgument;
+  const int n = f->n;
+  if (f->info < n && f->precision != DP_PRECISION_FP64) {
+    // a mixed-precision factorisation that delayed: decide in plain FP64
+    f->refactored = 1;
+    const double fms0 = f->factor_ms;
+    const int s = factorize(*f, A, lda, DP_PRECISION_FP64, st);
+    res->factor_ms = f->factor_ms - fms0;
+    res->info = f->info;
+    res->refactored = 1;
+    if (s != kOk) return s;
+  }
+  if (f->info < n) return kOk;  // singular: no solution
+  if (nrhs == 0) {
+    res->backward_error = 0.0;
+    res->converged = 1;
+    return kOk;
+  }
+  const size_t nr = (size_t)n * nrhs;
+  double *X = nullptr, *R = nullptr, *T = nullptr, *norms = nullptr;
+  auto release = [&] {
+    if (X) cudaFreeAsync(X, st);
+    if (R) cudaFreeAsync(R, st);
+    if (T) cudaFreeAsync(T, st);
+    if (norms) cudaFreeAsync(norms, st);
+    cudaStreamSynchronize(st);
+  };
+  if (cudaMallocAsync(reinterpret_cast<void**>(&X), nr * sizeof(double), st) != cudaSuccess ||
+      cudaMallocAsync(reinterpret_cast<void**>(&R), nr * sizeof(double), st) != cudaSuccess ||
+      cudaMallocAsync(reinterpret_cast<void**>(&T), nr * sizeof(double), st) != cudaSuccess ||
+      cudaMallocAsync(reinterpret_cast<void**>(&norms), 2 * (size_t)nrhs * sizeof(double), st) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    release();
+    return kAllocationFailed;
+  }
+  std::vector<double> normB(nrhs);
+  int status = kOk;
+  {
+    if (cudaMemsetAsync(norms, 0, sizeof(double) * nrhs, st) != cudaSuccess) status = kCudaFailure;
+    dim3 g((unsigned)std::min(64, (n + 255) / 256), (unsigned)nrhs);
+    colmax_kernel<<<g, 256, 0, st>>>(B, ldb, n, nrhs, norms);
+    if (status == kOk &&
+        (cudaMemcpyAsync(normB.data(), norms, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st) !=
+             cudaSuccess ||
+         cudaStreamSynchronize(st) != cudaSuccess))
+      status = kCudaFailure;
+  }
+
+  auto refine = [&](int iters_left, bool& converged) -> int {
+    converged = false;
+    double prev = INFINITY;
+    for (int it = 0;; ++it) {
+      double berr = INFINITY;
+      int s = backward_error(A, lda, n, B, ldb, X, n, nrhs, R, norms, f->normA, normB, berr, st);
+      if (s != kOk) return s;
+      res->backward_error = berr;
+      if (berr <= tol) {
+        converged = true;
+        return kOk;
+      }
+      if (it >= iters_left) return kOk;
+      if (it > 0 && !(berr <= 0.5 * prev)) return kOk;  // stalled
+      prev = berr;
+      solve_with(*f, R, n, R, T, nrhs, st);
+      axpy_kernel<<<grid_of((long long)nr), 256, 0, st>>>(R, n, X, n, n, nrhs);
+      res->iterations += 1;
+    }
+  };
+
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  cudaEventRecord(t0, st);
+  const double fms0 = f->factor_ms - res->factor_ms;
+  bool converged = false;
+  if (status == kOk) {
+    solve_with(*f, B, ldb, X, T, nrhs, st);
+    status = refine(max_iter, converged);
+  }
+  if (status == kOk && !converged && f->precision != DP_PRECISION_FP64) {
+    // the mixed-precision factors cannot carry this matrix: plain FP64
+    f->refactored = 1;
+    status = factorize(*f, A, lda, DP_PRECISION_FP64, st);
+    if (status == kOk && f->info == n) {
+      solve_with(*f, B, ldb, X, T, nrhs, st);
+      status = refine(max_iter, converged);
+    }
+  }
+  cudaEventRecord(t1, st);
+  cudaEventSynchronize(t1);
+  float tot = 0.f;
+  cudaEventElapsedTime(&tot, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  res->total_ms = tot;
+  res->factor_ms = f->factor_ms - fms0;
+  res->info = f->info;
+  res->refactored = f->refactored;
+  res->converged = converged ? 1 : 0;
+  if (status == kOk && f->info == n)
+    copy_kernel<<<grid_of((long long)nr), 256, 0, st>>>(X, n, B, ldb, n, nrhs);
+  release();
+  return status;
+}
+
 int gesv_ir_device(int n, int nrhs, const double* A, int lda, double* B, int ldb, int precision,
                    int max_iter, double tol, dp_ir_result* res, cudaStream_t st) {
   if (!res) return kInvalidArgument;
@@ -222,114 +443,18 @@ int gesv_ir_device(int n, int nrhs, const double* A, int lda, double* B, int ldb
     return kOk;
   }
   if (!A || !B) return kInvalidArgument;
-
-  const size_t nn = (size_t)n * n, nr = (size_t)n * nrhs;
-  double *lu = nullptr, *X = nullptr, *R = nullptr, *norms = nullptr;
-  auto release = [&] {
-    if (lu) cudaFreeAsync(lu, st);
-    if (X) cudaFreeAsync(X, st);
-    if (R) cudaFreeAsync(R, st);
-    if (norms) cudaFreeAsync(norms, st);
-    cudaStreamSynchronize(st);
-  };
-  if (cudaMallocAsync(reinterpret_cast<void**>(&lu), nn * sizeof(double), st) != cudaSuccess ||
-      cudaMallocAsync(reinterpret_cast<void**>(&X), nr * sizeof(double), st) != cudaSuccess ||
-      cudaMallocAsync(reinterpret_cast<void**>(&R), nr * sizeof(double), st) != cudaSuccess ||
-      cudaMallocAsync(reinterpret_cast<void**>(&norms), (2 * (size_t)nrhs + 1) * sizeof(double),
-                      st) != cudaSuccess) {
-    cudaGetLastError();
-    release();
-    return kAllocationFailed;
-  }
-  std::vector<int> ipiv(n), jpiv(n);
-  std::vector<double> normB(nrhs);
-  double normA = 0.0;
-  int status = kOk;
-
-  // ||A||_inf and ||B_c||_inf
-  if (cudaMemsetAsync(norms, 0, (2 * (size_t)nrhs + 1) * sizeof(double), st) != cudaSuccess)
-    status = kCudaFailure;
-  if (status == kOk) {
-    row_abs_sum_kernel<<<(n + 255) / 256, 256, 0, st>>>(A, lda, n, norms + 2 * nrhs);
-    dim3 g((unsigned)std::min(64, (n + 255) / 256), (unsigned)nrhs);
-    colmax_kernel<<<g, 256, 0, st>>>(B, ldb, n, nrhs, norms);
-    std::vector<double> h(2 * (size_t)nrhs + 1);
-    if (cudaMemcpyAsync(h.data(), norms, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st) !=
-            cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-      status = kCudaFailure;
-    else {
-      normA = h[2 * nrhs];
-      for (int c = 0; c < nrhs; ++c) normB[c] = h[c];
-    }
-  }
-
-  auto factor_and_solve = [&](int prec) -> int {
-    const long long total = (long long)nn;
-    copy_kernel<<<grid_of(total), 256, 0, st>>>(A, lda, lu, n, n, n);
-    dp_options opt;
-    dp_options_init(&opt);
-    opt.precision = prec;
-    int info = -1;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, st);
-    int s = getrf_device(n, n, lu, n, ipiv.data(), jpiv.data(), &info, st, &opt);
-    cudaEventRecord(e1, st);
-    cudaEventSynchronize(e1);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    res->factor_ms += ms;
-    res->info = info;
-    if (s != kOk) return s;
-    if (info < n) return kOk;  // singular: no solution
-    copy_kernel<<<grid_of((long long)nr), 256, 0, st>>>(B, ldb, X, n, n, nrhs);
-    return getrs_device(n, nrhs, lu, n, ipiv.data(), jpiv.data(), X, n, st);
-  };
-
-  // refinement loop; returns status, sets converged
-  auto refine = [&](int iters_left, bool& converged, bool& stalled) -> int {
-    converged = stalled = false;
-    double prev = INFINITY;
-    for (int it = 0;; ++it) {
-      double berr = INFINITY;
-      int s = backward_error(A, lda, n, B, ldb, X, n, nrhs, R, norms, normA, normB, berr, st);
-      if (s != kOk) return s;
-      res->backward_error = berr;
-      if (berr <= tol) {
-        converged = true;
-        return kOk;
-      }
-      if (it >= iters_left) return kOk;
-      if (it > 0 && !(berr <= 0.5 * prev)) {
-        stalled = true;
-        return kOk;
-      }
-      prev = berr;
-      s = getrs_device(n, nrhs, lu, n, ipiv.data(), jpiv.data(), R, n, st);
-      if (s != kOk) return s;
-      axpy_kernel<<<grid_of((long long)nr), 256, 0, st>>>(R, n, X, n, n, nrhs);
-      res->iterations += 1;
-    }
-  };
-
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
   cudaEventRecord(t0, st);
-  if (status == kOk) status = factor_and_solve(precision);
-  bool converged = false, stalled = false;
-  if (status == kOk && res->info == n) status = refine(max_iter, converged, stalled);
-  if (status == kOk && precision != DP_PRECISION_FP64 && !converged) {
-    // refinement on the mixed-precision factors stalled (or the mixed
-    // factorisation delayed): re-factor on the plain FP64 path
-    res->refactored = 1;
-    status = factor_and_solve(DP_PRECISION_FP64);
-    if (status == kOk && res->info == n) status = refine(max_iter, converged, stalled);
+  Factor* f = nullptr;
+  int status = factor_create(&f, n, A, lda, precision, st);
+  const double factor_ms = f ? f->factor_ms : 0.0;
+  if (status == kOk) {
+    status = factor_solve(f, A, lda, B, ldb, nrhs, max_iter, tol, res, st);
+    res->factor_ms += factor_ms;
   }
+  if (f) factor_destroy(f, st);
   cudaEventRecord(t1, st);
   cudaEventSynchronize(t1);
   float tot = 0.f;
@@ -337,10 +462,6 @@ int gesv_ir_device(int n, int nrhs, const double* A, int lda, double* B, int ldb
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
   res->total_ms = tot;
-  res->converged = converged ? 1 : 0;
-  if (status == kOk && res->info == n)
-    copy_kernel<<<grid_of((long long)nr), 256, 0, st>>>(X, n, B, ldb, n, nrhs);
-  release();
   return status;
 }
 
@@ -358,6 +479,46 @@ int dp_gesv_ir_device(int n, int nrhs, const double* d_a, int lda, double* d_b, 
                       int precision, int max_iter, double tol, dp_ir_result* result, void* stream) {
   return dp::gesv_ir_device(n, nrhs, d_a, lda, d_b, ldb, precision, max_iter, tol, result,
                             static_cast<cudaStream_t>(stream));
+}
+
+struct dp_factor {
+  dp::Factor* f;
+};
+
+int dp_factor_create(dp_factor** out, int n, const double* d_a, int lda, int precision,
+                     void* stream) {
+  if (!out) return DP_INVALID_ARGUMENT;
+  *out = nullptr;
+  dp::Factor* f = nullptr;
+  const int s = dp::factor_create(&f, n, d_a, lda, precision, static_cast<cudaStream_t>(stream));
+  if (s != DP_SUCCESS) return s;
+  *out = new (std::nothrow) dp_factor{f};
+  if (!*out) {
+    dp::factor_destroy(f, static_cast<cudaStream_t>(stream));
+    return DP_ALLOCATION_FAILED;
+  }
+  return DP_SUCCESS;
+}
+
+int dp_factor_info(const dp_factor* h, int* info, int* precision, double* factor_ms) {
+  if (!h) return DP_INVALID_ARGUMENT;
+  if (info) *info = h->f->info;
+  if (precision) *precision = h->f->precision;
+  if (factor_ms) *factor_ms = h->f->factor_ms;
+  return DP_SUCCESS;
+}
+
+int dp_factor_solve(dp_factor* h, const double* d_a, int lda, double* d_b, int ldb, int nrhs,
+                    int max_iter, double tol, dp_ir_result* result, void* stream) {
+  if (!h) return DP_INVALID_ARGUMENT;
+  return dp::factor_solve(h->f, d_a, lda, d_b, ldb, nrhs, max_iter, tol, result,
+                          static_cast<cudaStream_t>(stream));
+}
+
+void dp_factor_destroy(dp_factor* h, void* stream) {
+  if (!h) return;
+  dp::factor_destroy(h->f, static_cast<cudaStream_t>(stream));
+  delete h;
 }
 
 }  // extern "C"

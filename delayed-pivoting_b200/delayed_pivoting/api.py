@@ -58,6 +58,71 @@ class BatchOptions(ctypes.Structure):
     ]
 
 
+class ServerOptions(ctypes.Structure):
+    """dp_server_options: HBM budget, precision, workers, batching, refinement."""
+
+    _fields_ = [
+        ("budget_bytes", ctypes.c_ulonglong),
+        ("precision", ctypes.c_int),
+        ("large_workers", ctypes.c_int),
+        ("small_max_n", ctypes.c_int),
+        ("small_max_batch", ctypes.c_int),
+        ("max_iter", ctypes.c_int),
+        ("tol", ctypes.c_double),
+        ("reserved", ctypes.c_int * 4),
+    ]
+
+
+class Request(ctypes.Structure):
+    """dp_request: factor + solve (factor_id 0) or a follow-up solve."""
+
+    _fields_ = [
+        ("id", ctypes.c_ulonglong),
+        ("factor_id", ctypes.c_ulonglong),
+        ("n", ctypes.c_int),
+        ("d_a", ctypes.c_void_p),
+        ("lda", ctypes.c_int),
+        ("d_b", ctypes.c_void_p),
+        ("ldb", ctypes.c_int),
+        ("nrhs", ctypes.c_int),
+        ("followups", ctypes.c_int),
+        ("reserved", ctypes.c_int),
+    ]
+
+
+class RequestResult(ctypes.Structure):
+    """dp_request_result: status, info, precision, refinement, timestamps."""
+
+    _fields_ = [
+        ("id", ctypes.c_ulonglong),
+        ("status", ctypes.c_int),
+        ("info", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("iterations", ctypes.c_int),
+        ("refactored", ctypes.c_int),
+        ("path", ctypes.c_int),
+        ("backward_error", ctypes.c_double),
+        ("t_submit", ctypes.c_double),
+        ("t_admit", ctypes.c_double),
+        ("t_start", ctypes.c_double),
+        ("t_done", ctypes.c_double),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("bytes_in_use", ctypes.c_ulonglong),
+        ("bytes_peak", ctypes.c_ulonglong),
+        ("submitted", ctypes.c_longlong),
+        ("completed", ctypes.c_longlong),
+        ("pending", ctypes.c_longlong),
+        ("residents", ctypes.c_longlong),
+        ("small_launches", ctypes.c_longlong),
+        ("small_items", ctypes.c_longlong),
+        ("large_items", ctypes.c_longlong),
+    ]
+
+
 def library_path() -> Path:
     return _LIB_DIR / "libdelayed_lu_b200.so"
 
@@ -115,6 +180,31 @@ def lib() -> ctypes.CDLL:
         L.dp_batch_tune_save.argtypes = [ctypes.c_char_p, bo]
         L.dp_batch_tune_load.restype = ctypes.c_int
         L.dp_batch_tune_load.argtypes = [ctypes.c_char_p, bo]
+        L.dp_factor_create.restype = ctypes.c_int
+        L.dp_factor_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, vp, ctypes.c_int,
+                                       ctypes.c_int, vp]
+        L.dp_factor_info.restype = ctypes.c_int
+        L.dp_factor_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_double)]
+        L.dp_factor_solve.restype = ctypes.c_int
+        L.dp_factor_solve.argtypes = [vp, vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_double, ctypes.POINTER(IRResult), vp]
+        L.dp_factor_destroy.restype = None
+        L.dp_factor_destroy.argtypes = [vp, vp]
+        L.dp_server_options_init.restype = None
+        L.dp_server_options_init.argtypes = [ctypes.POINTER(ServerOptions)]
+        L.dp_server_create.restype = ctypes.c_int
+        L.dp_server_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(ServerOptions)]
+        L.dp_server_submit.restype = ctypes.c_int
+        L.dp_server_submit.argtypes = [vp, ctypes.POINTER(Request)]
+        L.dp_server_poll.restype = ctypes.c_int
+        L.dp_server_poll.argtypes = [vp, ctypes.POINTER(RequestResult), ctypes.c_int, ctypes.c_int]
+        L.dp_server_stats_get.restype = ctypes.c_int
+        L.dp_server_stats_get.argtypes = [vp, ctypes.POINTER(ServerStats)]
+        L.dp_server_clock.restype = ctypes.c_double
+        L.dp_server_clock.argtypes = []
+        L.dp_server_destroy.restype = None
+        L.dp_server_destroy.argtypes = [vp]
         L.dp_options_init.restype = None
         L.dp_options_init.argtypes = [ctypes.POINTER(Options)]
         _lib = L
@@ -335,3 +425,96 @@ def batch_tune_load(path, options: BatchOptions | None = None):
     opt = options if options is not None else batch_options()
     st = lib().dp_batch_tune_load(str(path).encode(), ctypes.byref(opt))
     return st, opt
+
+
+# ---- resident factors (dp_factor_*) ----------------------------------------
+
+class Factor:
+    """dp_factor: a factorisation kept on the device for repeated refined solves."""
+
+    def __init__(self, n, d_a, lda, precision=PRECISION_MIXED_BF16X3, stream=None):
+        self._h = None
+        h = ctypes.c_void_p()
+        st = lib().dp_factor_create(ctypes.byref(h), n, _dptr(d_a), lda, precision,
+                                    _stream(stream))
+        if st != SUCCESS:
+            raise BatchError(st, "dp_factor_create")
+        self._h, self.n, self.d_a, self.lda = h, n, d_a, lda
+
+    def info(self):
+        """(info, precision of the factors held now, factorisation ms so far)."""
+        i, p, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        lib().dp_factor_info(self._h, ctypes.byref(i), ctypes.byref(p), ctypes.byref(ms))
+        return i.value, p.value, ms.value
+
+    def solve(self, d_b, ldb, nrhs, max_iter=10, tol=1e-14, stream=None):
+        """Overwrites d_b with X; returns (status, IRResult)."""
+        res = IRResult()
+        st = lib().dp_factor_solve(self._h, _dptr(self.d_a), self.lda, _dptr(d_b), ldb, nrhs,
+                                   max_iter, tol, ctypes.byref(res), _stream(stream))
+        return st, res
+
+    def close(self, stream=None):
+        if getattr(self, "_h", None):
+            lib().dp_factor_destroy(self._h, _stream(stream))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- serving (dp_server_*) ---------------------------------------------------
+
+def server_options(**kw) -> ServerOptions:
+    opt = ServerOptions()
+    lib().dp_server_options_init(ctypes.byref(opt))
+    for k, v in kw.items():
+        setattr(opt, k, v)
+    return opt
+
+
+def server_clock() -> float:
+    return lib().dp_server_clock()
+
+
+class Server:
+    """dp_server: admits factor+solve requests and follow-up solves against an
+    HBM budget and runs them overlapped on the current GPU."""
+
+    def __init__(self, options: ServerOptions | None = None, **kw):
+        self._h = None
+        opt = options if options is not None else server_options(**kw)
+        h = ctypes.c_void_p()
+        st = lib().dp_server_create(ctypes.byref(h), ctypes.byref(opt))
+        if st != SUCCESS:
+            raise BatchError(st, "dp_server_create")
+        self._h, self.options = h, opt
+
+    def submit(self, rid, n, d_a, lda, d_b, ldb, nrhs, followups=0, factor_id=0) -> int:
+        r = Request(id=rid, factor_id=factor_id, n=n, d_a=_dptr(d_a), lda=lda, d_b=_dptr(d_b),
+                    ldb=ldb, nrhs=nrhs, followups=followups)
+        return lib().dp_server_submit(self._h, ctypes.byref(r))
+
+    def poll(self, max_results=256, wait_ms=0):
+        buf = (RequestResult * max_results)()
+        k = lib().dp_server_poll(self._h, buf, max_results, wait_ms)
+        return [buf[i] for i in range(k)]
+
+    def stats(self) -> ServerStats:
+        s = ServerStats()
+        lib().dp_server_stats_get(self._h, ctypes.byref(s))
+        return s
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().dp_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

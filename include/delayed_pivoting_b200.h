@@ -123,6 +123,26 @@ int dp_gesv_ir_device(int n, int nrhs, const double *d_a, int lda, double *d_b, 
                       int precision, int max_iter, double tol, dp_ir_result *result,
                       void *stream);
 
+/* ---- Resident factorisations (no reference counterpart): factor once, solve
+ * many right-hand sides later with FP64 refinement.  The factors live on the
+ * device until dp_factor_destroy; the caller keeps d_a (the matrix the
+ * factors came from, needed for the refinement residuals) valid and
+ * unmodified meanwhile. */
+typedef struct dp_factor dp_factor;
+/* Factor d_a (n x n, device, not modified) at `precision` (DP_PRECISION_*).
+ * Synchronises `stream`.  A singular matrix gives a factor with info < n. */
+int dp_factor_create(dp_factor **factor, int n, const double *d_a, int lda, int precision,
+                     void *stream);
+/* info of the factorisation, precision of the factors held now (a stalled
+ * mixed-precision refinement replaces them by FP64 factors), device
+ * milliseconds of all factorisations so far; outputs may be NULL. */
+int dp_factor_info(const dp_factor *factor, int *info, int *precision, double *factor_ms);
+/* Solve A X = B: d_b (n x nrhs, device) becomes X; refinement as in
+ * dp_gesv_ir_device.  Synchronises `stream`. */
+int dp_factor_solve(dp_factor *factor, const double *d_a, int lda, double *d_b, int ldb,
+                    int nrhs, int max_iter, double tol, dp_ir_result *result, void *stream);
+void dp_factor_destroy(dp_factor *factor, void *stream);
+
 /* ---- Batched factorisation (no reference counterpart: the reference factors
  * one matrix per call).  Thousands of independent square matrices of orders
  * 1..DP_BATCH_MAX_N, each column-major with lda = its order, factored by ONE
@@ -176,6 +196,81 @@ int dp_batch_autotune(dp_batch_options *opt, int samples, unsigned long long see
 /* Tuning table file: one line per bucket, "<smallest n> <largest n> <nb>". */
 int dp_batch_tune_save(const char *path, const dp_batch_options *opt);
 int dp_batch_tune_load(const char *path, dp_batch_options *opt);
+
+/* ---- Serving (no reference counterpart): a request loop on one GPU.
+ * Requests to factor a matrix and solve right-hand sides arrive at any time
+ * from any host thread; the server admits them against an HBM budget as
+ * memory frees up, sends orders <= small_max_n through the persistent batched
+ * factorisation (many requests per launch) and larger ones through the
+ * blocked factorisation on concurrent streams, refines every solve in FP64,
+ * and keeps factors resident for follow-up solves.  Every solve of a request
+ * is computed the same way whether it runs alone or among others.
+ * The server works on its own streams: a request's device buffers must hold
+ * their data when it is submitted (synchronise the stream that wrote them),
+ * and X is in d_b once the request's result has been polled. */
+typedef struct dp_server_options {
+  unsigned long long budget_bytes; /* HBM admission budget (0: 160 GB) */
+  int precision;       /* DP_PRECISION_* of the blocked factorisations */
+  int large_workers;   /* concurrent blocked factorisations (streams); 0: 6 */
+  int small_max_n;     /* orders up to this take the batched path (<= DP_BATCH_MAX_N); 0: 512,
+                          -1: none */
+  int small_max_batch; /* requests per batched launch; 0: 2048 */
+  int max_iter;        /* refinement steps per solve; 0: 10 */
+  double tol;          /* backward-error target; 0: 1e-14 */
+  int reserved[4];
+} dp_server_options;
+
+void dp_server_options_init(dp_server_options *opt);
+
+typedef struct dp_request {
+  unsigned long long id;        /* caller's tag, unique among live requests, != 0 */
+  unsigned long long factor_id; /* 0: factor d_a; else a follow-up solve on the resident
+                                   factors of request factor_id */
+  int n;
+  const double *d_a;            /* n x n, device; read only; must stay valid until the
+                                   request's factors are released */
+  int lda;
+  double *d_b;                  /* n x nrhs right-hand sides, device; becomes X */
+  int ldb;
+  int nrhs;                     /* 1..64 */
+  int followups;                /* new factorisation: number of follow-up solves that will
+                                   name it; its factors stay resident until they are done */
+  int reserved;
+} dp_request;
+
+typedef struct dp_request_result {
+  unsigned long long id;
+  int status;            /* DP_* */
+  int info;              /* factorisation info (n: nonsingular) */
+  int precision;         /* arithmetic of the factors that produced X */
+  int iterations;        /* refinement corrections */
+  int refactored;        /* 1: mixed factors stalled, re-factored in FP64 */
+  int path;              /* 0: batched (small), 1: blocked (large) */
+  double backward_error; /* max_c ||b_c - A x_c||_inf / (||A||_inf ||x_c||_inf + ||b_c||_inf) */
+  double t_submit, t_admit, t_start, t_done; /* dp_server_clock() seconds */
+} dp_request_result;
+
+typedef struct dp_server_stats {
+  unsigned long long bytes_in_use, bytes_peak;
+  long long submitted, completed, pending, residents;
+  long long small_launches, small_items, large_items;
+} dp_server_stats;
+
+typedef struct dp_server dp_server;
+/* Creates the server on the current device and starts its host threads. */
+int dp_server_create(dp_server **server, const dp_server_options *opt);
+/* Queues a request (thread-safe, returns at once).  DP_INVALID_ARGUMENT for
+ * bad sizes or pointers, a duplicate id, or a request that can never fit the
+ * budget. */
+int dp_server_submit(dp_server *server, const dp_request *request);
+/* Moves up to `max` completed results into `out`, waiting up to wait_ms for
+ * the first one; returns how many were moved. */
+int dp_server_poll(dp_server *server, dp_request_result *out, int max, int wait_ms);
+int dp_server_stats_get(dp_server *server, dp_server_stats *out);
+/* Seconds on the server's monotonic clock (the timestamps of the results). */
+double dp_server_clock(void);
+/* Waits for every queued request, releases all resident factors, stops. */
+void dp_server_destroy(dp_server *server);
 
 /* Per-kernel-family device timing (no reference counterpart; the reference
  * only times whole calls with std::chrono, delayed_lu_cuda/benchmark.cu:54-57).
