@@ -1,18 +1,32 @@
 """Benchmark of the B200 delayed-pivoting LU.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--n 16384]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload serve|lu|batched]
 
-One step = one plain-FP64 delayed_getrf of an n x n N(0,1) matrix with
-0.1 % tiny (x1e-18) and 0.02 % exact-zero columns (n = 16384: 16 + 3), the
-single-GPU configuration of the reference's plain path.  Inputs are
-generated once (seeded MT19937-64), kept resident in HBM, and restored by a
-device copy before every step, outside the timed region; the 2 GiB matrix is
-larger than L2, so no flush is needed between steps.  Throughput is
-2/3 n^3 / t in GFLOP/s (delayed_lu_cuda/benchmark.cu:67).
+Workloads (one JSON line on rank 0 each run):
 
-Rank 0 prints one JSON line.  With N > 1 (torchrun) each rank factors its own
-matrix (replicas: a single LU does not shard) and `value` is the sum over
-ranks divided by the slowest rank's time.
+serve (default; the headline metric: solves/s and p99 latency of the served
+    mixed-precision form against plain FP64 at backward error <= 1e-14).  One
+    step = one burst of --requests factor+solve requests (n log-uniform in
+    [64, 8192] on a 24-size grid, A = U diag(sigma) V^T with kappa
+    log-uniform in [1e2, 1e6] for 90 % and 1e10 for 10 %, 1-32 right-hand
+    sides, 0-4 follow-up solves each) through dp_server; value = solves per
+    second of the mixed-precision server.  Latency comes from an open-loop
+    Poisson stream at 70 % of the measured capacity, with host timestamps at
+    submission and completion; the plain-FP64 server runs the same bursts
+    and the same stream.
+lu  one plain-FP64 delayed_getrf of an n x n N(0,1) matrix with 0.1 % tiny
+    (x1e-18) and 0.02 % exact-zero columns (n = 16384: 16 + 3), 2/3 n^3 / t in
+    GFLOP/s (delayed_lu_cuda/benchmark.cu:67).
+batched  one persistent launch (CUDA graph) factoring 8192 matrices, n
+    log-uniform in [32, 512], 0-2 exact-zero columns each; matrices/s.
+
+Inputs are generated once (seeded), kept resident in HBM and restored by a
+device copy before every step, outside the timed region; every step's inputs
+are larger than L2, so no flush is needed between steps.  With N > 1
+(torchrun) each rank runs its own replica (a single LU does not shard;
+batches and request streams are independent per GPU) and `value` is the sum
+over ranks divided by the slowest rank's time.
 """
 from __future__ import annotations
 
@@ -48,7 +62,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
-                    help="trailing-update arithmetic of the factorisation")
+                    help="trailing-update arithmetic of the factorisation (lu workload)")
+    ap.add_argument("--workload", default="serve", choices=["serve", "lu", "batched"])
+    ap.add_argument("--requests", type=int, default=1000, help="requests per serve step")
+    ap.add_argument("--load", type=float, default=0.7, help="open-loop load / capacity")
+    ap.add_argument("--count", type=int, default=8192, help="matrices per batched step")
     return ap.parse_args()
 
 
@@ -170,6 +188,10 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if args.workload == "serve":
+        return serve_reference_arm(args)
+    if args.workload == "batched":
+        return batched_reference_arm(args)
     threads = os.cpu_count() or 1
     n = args.cpu_n
     times = []
@@ -200,7 +222,14 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "serve":
+        return run_serve(args)
+    if args.workload == "batched":
+        return run_batched(args)
+    return run_lu(args)
 
+
+def run_lu(args):
     import torch
     import delayed_pivoting as dp
 
@@ -362,6 +391,475 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+# ---------------------------------------------------------------- serve ----
+
+SERVE_METRIC = "solves/s, p99 latency: served mixed-prec vs plain FP64 LU @ bwd err<=1e-14"
+SERVE_WORKLOAD = ("served stream: n log-uniform [64, 8192] (24-order grid), A = U diag(sigma) "
+                  "V^T, kappa log-uniform [1e2, 1e6] (90%) / 1e10 (10%), 1-32 RHS, 0-4 follow-up "
+                  "solves, HBM budget 160 GB")
+
+
+def _dist_setup(torch):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+
+        dist = dist_mod
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+    return world, rank, local, dev, dist
+
+
+def _max_over_ranks(torch, dist, dev, v):
+    if not dist:
+        return v
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _sum_over_ranks(torch, dist, dev, v):
+    if not dist:
+        return v
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def _pct(xs, q):
+    return float(np.percentile(np.asarray(xs), q)) if len(xs) else None
+
+
+def _serve_summary(reqs, results):
+    lat = [(r.t_done - r.t_submit) * 1e3 for r in results.values()]
+    berr = [r.backward_error for r in results.values()]
+    bad = [r.id for r in results.values() if r.status != 0 or not (r.backward_error <= 1e-14)]
+    ill = [q for q in reqs if q.kappa >= 1e10]
+    ill_fp64 = sum(1 for q in ill if results[q.rid].precision == 0)
+    refac_other = sum(1 for q in reqs if q.kappa < 1e10 and results[q.rid].refactored)
+    return {"p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99), "max_ms": max(lat) if lat else None,
+            "berr_max": max(berr) if berr else None, "berr_p50": _pct(berr, 50),
+            "berr_p99": _pct(berr, 99), "violations": len(bad),
+            "kappa_1e10_requests": len(ill), "kappa_1e10_ended_fp64": ill_fp64,
+            "refactored_below_1e10": refac_other}
+
+
+def _cpu_serve_baseline(pool, reqs, budget_flops=6e11):
+    """The reference's CPU delayed_getrf (oracle/_ref, OpenBLAS on every host
+    core) on the leading requests of the stream, up to budget_flops of
+    factorisation work; each request's solves are counted as served by its
+    factorisation (the reference has no solve), so this overstates the CPU."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+
+    kind, fn = ("reference", orc.ref_getrf) if orc.ref_available() else ("port", orc.oracle_getrf)
+    threads = os.cpu_count() or 1
+    if kind == "reference":
+        orc.ref_lib().ref_set_threads(threads)
+    t_tot, solves, used, count = 0.0, 0, 0.0, 0
+    for q in reqs:
+        f = 2.0 / 3.0 * q.n ** 3
+        if count > 0 and used + f > budget_flops:
+            continue
+        a = np.asfortranarray(pool[(q.n, q.kappa)].cpu().numpy().T)
+        t0 = time.perf_counter()
+        fn(a)
+        t_tot += time.perf_counter() - t0
+        solves += len(q.solves)
+        used += f
+        count += 1
+    return {"value": solves / t_tot, "unit": "solves/s", "cores": threads, "kind": kind,
+            "sample": f"{count} requests of the stream ({solves} solves, {used:.3g} factorisation "
+                      f"flops) factored by delayed_getrf in {t_tot:.1f} s; solves not timed"}
+
+
+def run_serve(args):
+    import torch
+    import delayed_pivoting as dp
+    from delayed_pivoting import serving as sv
+
+    world, rank, local, dev, dist = _dist_setup(torch)
+    L = dp.lib()
+    L.dp_kernel_launches.restype = ctypes_longlong()
+    seed = args.seed + rank
+    R = args.requests
+    reqs = sv.make_stream(R, seed)
+    warm = reqs[:max(10, R // 10)]
+    pool = sv.MatrixPool(torch, [(q.n, q.kappa) for q in reqs], seed=seed)
+    rhs = sv.RhsSet(torch, pool, reqs, seed=seed + 1)
+    solves_per_step = sum(len(q.solves) for q in reqs)
+
+    def bursts(server, k, stream):
+        ms = []
+        res = None
+        for _ in range(k):
+            rhs.reset(torch)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            res, _, _ = sv.replay(server, pool, rhs, stream)
+            torch.cuda.synchronize()
+            e1.record()
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return ms, res
+
+    out = {}
+    for mode, prec in (("mixed", dp.PRECISION_MIXED_BF16X3), ("plain", dp.PRECISION_FP64)):
+        srv = dp.Server(precision=prec)
+        bursts(srv, max(1, args.warmup if mode == "mixed" else 1), warm)
+        if dist:
+            dist.barrier()
+        k = args.steps if mode == "mixed" else max(1, min(args.steps, 2))
+        l0 = L.dp_kernel_launches()
+        with ClockSampler(local) as clk:
+            ms, res = bursts(srv, k, reqs)
+        launches = L.dp_kernel_launches() - l0
+        ms_tot = _max_over_ranks(torch, dist, dev, sum(ms))
+        capacity = _sum_over_ranks(torch, dist, dev, solves_per_step * k) / (ms_tot * 1e-3)
+        out[mode] = {"ms": ms, "ms_tot": ms_tot, "capacity": capacity, "burst": _serve_summary(
+            reqs, res), "clocks": clk.summary(), "launches": launches, "server": srv}
+    # open-loop latency at the same offered load for both servers
+    rate = args.load * (R / (out["mixed"]["ms_tot"] / args.steps * 1e-3))
+    for mode in ("mixed", "plain"):
+        srv = out[mode]["server"]
+        rhs.reset(torch)
+        res, first, last = sv.replay(srv, pool, rhs, reqs, rate=rate, seed=seed + 2)
+        out[mode]["open"] = _serve_summary(reqs, res)
+        out[mode]["open"]["span_s"] = last - first
+    # kernel families of the mixed server (one extra burst with device timing on)
+    srv = out["mixed"]["server"]
+    L.dp_stats_reset()
+    L.dp_stats_enable(1)
+    bursts(srv, 1, reqs)
+    L.dp_stats_enable(0)
+    stats = _stats(L)
+    for mode in ("mixed", "plain"):
+        out[mode]["server"].close()
+        out[mode]["server"] = None
+
+    # e2e: requests whose matrices and right-hand sides start in pinned host
+    # memory; H2D copies, serving and the D2H of every X inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        ereqs = reqs[:max(10, R // 4)]
+        hostA = {}
+        for q in ereqs:
+            if (q.n, q.kappa) not in hostA:
+                hostA[(q.n, q.kappa)] = pool[(q.n, q.kappa)].cpu().pin_memory()
+        hostB = {s.rid: rhs.src[s.rid].cpu().pin_memory() for q in ereqs for s in q.solves}
+        hostX = {k: torch.empty_like(v).pin_memory() for k, v in hostB.items()}
+        devA = [torch.empty_like(pool[(q.n, q.kappa)]) for q in ereqs]
+        srv = dp.Server(precision=dp.PRECISION_MIXED_BF16X3)
+        cs = torch.cuda.Stream()
+        h2d = sum(8 * q.n * q.n for q in ereqs) + sum(v.numel() * 8 for v in hostB.values())
+        d2h = sum(v.numel() * 8 for v in hostB.values())
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(cs)
+        results = {}
+        for q, dA in zip(ereqs, devA):
+            with torch.cuda.stream(cs):
+                dA.copy_(hostA[(q.n, q.kappa)], non_blocking=True)
+                for s_ in q.solves:
+                    rhs.work[s_.rid].copy_(hostB[s_.rid], non_blocking=True)
+            cs.synchronize()
+            for s_ in q.solves:
+                b = rhs.work[s_.rid]
+                if s_.factor_id == 0:
+                    st = srv.submit(s_.rid, q.n, dA, q.n, b, q.n, s_.nrhs,
+                                    followups=len(q.solves) - 1)
+                else:
+                    st = srv.submit(s_.rid, q.n, None, q.n, b, q.n, s_.nrhs,
+                                    factor_id=s_.factor_id)
+                assert st == 0
+            for r in srv.poll(1024, 0):
+                results[r.id] = r
+        total = sum(len(q.solves) for q in ereqs)
+        while len(results) < total:
+            for r in srv.poll(1024, 20):
+                results[r.id] = r
+        with torch.cuda.stream(cs):
+            for k_, v in hostX.items():
+                v.copy_(rhs.work[k_], non_blocking=True)
+        e1.record(cs)
+        e1.synchronize()
+        srv.close()
+        e_ms = _max_over_ranks(torch, dist, dev, e0.elapsed_time(e1))
+        e2e = {"value": _sum_over_ranks(torch, dist, dev, total) / (e_ms * 1e-3),
+               "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": e_ms, "requests": len(ereqs),
+               "api": "dp_server_submit / dp_server_poll (mixed), inputs from pinned host memory",
+               "backward_error_max": max(r.backward_error for r in results.values())}
+        del devA, hostA, hostB, hostX
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = _cpu_serve_baseline(pool, reqs)
+
+    peaks = measured_peaks()
+    g = 7  # DP_KFAM_GEMM_MIXED
+    gm_ms = stats["ms"][g]
+    algo_tf = stats["flops"][g] / (gm_ms * 1e-3) / 1e12 if gm_ms > 0 else 0.0
+    bf16 = peaks.get("bf16_tflops_sustained") or peaks.get("bf16_tflops")
+    roofline = {"bound": "tensor", "kernel": "gemm_bf16x3_kernel (tcgen05 kind::f16, 3 products)",
+                "achieved": 3 * algo_tf, "peak": bf16, "unit": "TFLOP/s",
+                "frac": 3 * algo_tf / bf16 if bf16 else None,
+                "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (measured)",
+                "traffic": None, "algorithmic_fp64_tflops": algo_tf,
+                "per_launch_flops": stats["flops"][g] / max(stats["launches"][g], 1),
+                "avg_launch_ms": gm_ms / max(stats["launches"][g], 1)}
+    fam = ["panel", "laswp", "trsm", "gemm", "search", "swap", "other", "gemm_mixed"]
+    kern = {nm: {"ms": stats["ms"][i], "launches": stats["launches"][i],
+                 "tflops": (stats["flops"][i] / (stats["ms"][i] * 1e-3) / 1e12
+                            if stats["flops"][i] and stats["ms"][i] else None)}
+            for i, nm in enumerate(fam) if stats["launches"][i]}
+    if rank == 0:
+        m, pl = out["mixed"], out["plain"]
+        line = {
+            "metric": SERVE_METRIC, "value": m["capacity"], "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms_tot"] / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded QR-conditioned matrices, seeded Poisson stream",
+            "config": {"workload": SERVE_WORKLOAD, "requests_per_step": R,
+                       "solves_per_step": solves_per_step, "precision": "mixed BF16x3 + FP64 IR",
+                       "pool_gb": pool.bytes / 1e9, "parallelism": f"replicas x{world}",
+                       "l2": "inputs per step >> L2 (no flush needed)"},
+            "p99_ms": m["open"]["p99_ms"], "p50_ms": m["open"]["p50_ms"],
+            "open_loop": {"rate_rps": rate, "load": args.load, "mixed": m["open"],
+                          "plain": pl["open"]},
+            "burst": {"mixed": m["burst"], "plain": pl["burst"]},
+            "plain_fp64": {"solves_per_s": pl["capacity"], "ms_per_step": pl["ms_tot"] / len(pl["ms"]),
+                           "p50_ms": pl["open"]["p50_ms"], "p99_ms": pl["open"]["p99_ms"],
+                           "mixed_over_plain": m["capacity"] / pl["capacity"]},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(m["launches"]),
+            "clocks": m["clocks"],
+            "kernels_mixed_burst": kern,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def serve_reference_arm(args):
+    """The reference's CPU delayed_getrf on a bounded sample of the same stream
+    per step (each request's solves counted as served by its factorisation)."""
+    import torch
+    from delayed_pivoting import serving as sv
+
+    reqs = sv.make_stream(args.requests, args.seed)
+    vals, cpu = [], None
+    sample = reqs[:64]
+
+    class HostPool:
+        def __init__(self):
+            self.cache = {}
+
+        def __getitem__(self, key):
+            if key not in self.cache:
+                n, kappa = key
+                g = torch.Generator().manual_seed(args.seed * 100003 + n)
+                u, _ = torch.linalg.qr(torch.randn(n, n, dtype=torch.float64, generator=g))
+                v, _ = torch.linalg.qr(torch.randn(n, n, dtype=torch.float64, generator=g))
+                s = torch.logspace(0, -np.log10(kappa), n, dtype=torch.float64)
+                self.cache[key] = ((u * s) @ v.T).T.contiguous()
+            return self.cache[key]
+
+    pool = HostPool()
+    t_all = 0.0
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        cpu = _cpu_serve_baseline(pool, sample, budget_flops=2e11)
+        if i >= args.warmup:
+            vals.append(cpu["value"])
+            t_all += time.perf_counter() - t0
+    value = float(np.mean(vals))
+    line = {"impl": "reference", "metric": SERVE_METRIC, "value": value, "unit": "solves/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_all / max(args.steps, 1) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded QR-conditioned matrices (host), seeded stream",
+            "config": {"workload": SERVE_WORKLOAD, "requests_per_step": args.requests},
+            "cpu_baseline": dict(cpu, value=value),
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# -------------------------------------------------------------- batched ----
+
+BATCH_METRIC = "batched delayed_getrf matrices/s (8192 matrices, n log-uniform [32, 512])"
+
+
+def run_batched(args):
+    import torch
+    import delayed_pivoting as dp
+
+    world, rank, local, dev, dist = _dist_setup(torch)
+    L = dp.lib()
+    L.dp_kernel_launches.restype = ctypes_longlong()
+    count, seed = args.count, 8192 + rank
+    ns, nz = dp.batch_orders(count, seed)
+    st, tuned = dp.batch_autotune(samples=16)
+    b = dp.Batch(ns, options=tuned)
+    host = np.zeros(b.total_elements, dtype=np.float64)
+    dp.fill_batch(host, b.offsets, ns, nz, seed)
+    src = torch.from_numpy(host).to(dev)
+    work = torch.empty_like(src)
+    ip = torch.empty(b.total_records, dtype=torch.int32, device=dev)
+    jp = torch.empty_like(ip)
+    info = torch.empty(count, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        work.copy_(src)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        assert b.getrf_graph(work, ip, jp, info, stream=stream) == 0
+        e1.record(stream)
+        return e0, e1
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    l0 = L.dp_kernel_launches()
+    with ClockSampler(local) as clk:
+        ev = [step() for _ in range(args.steps)]
+        torch.cuda.synchronize()
+    launches = L.dp_kernel_launches() - l0
+    ms = _max_over_ranks(torch, dist, dev, sum(a.elapsed_time(c) for a, c in ev))
+    value = _sum_over_ranks(torch, dist, dev, count * args.steps) / (ms * 1e-3)
+    fl = float((2.0 / 3.0 * ns.astype(np.float64) ** 3).sum())
+    fp64 = fp64_peak_tflops(torch, dev)
+    tf = fl * args.steps / (ms * 1e-3) / 1e12
+    bytes_alg = float((16.0 * ns.astype(np.float64) ** 2).sum())
+
+    # e2e: matrices from pinned host memory through the plan (H2D, launch, D2H
+    # of factors and records), timed on the stream
+    e2e = None
+    if not args.no_e2e:
+        hsrc = torch.from_numpy(host).pin_memory()
+        hout = torch.empty_like(hsrc).pin_memory()
+        hip = torch.empty(b.total_records, dtype=torch.int32).pin_memory()
+        hjp = torch.empty_like(hip).pin_memory()
+        hinfo = torch.empty(count, dtype=torch.int32).pin_memory()
+        e_ms = 0.0
+        k = max(1, min(args.steps, 3))
+        for i in range(k + 1):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            work.copy_(hsrc, non_blocking=True)
+            assert b.getrf_graph(work, ip, jp, info, stream=stream) == 0
+            hout.copy_(work, non_blocking=True)
+            hip.copy_(ip, non_blocking=True)
+            hjp.copy_(jp, non_blocking=True)
+            hinfo.copy_(info, non_blocking=True)
+            e1.record(stream)
+            e1.synchronize()
+            if i:
+                e_ms += e0.elapsed_time(e1)
+        e_ms = _max_over_ranks(torch, dist, dev, e_ms / k)
+        e2e = {"value": _sum_over_ranks(torch, dist, dev, count) / (e_ms * 1e-3),
+               "unit": "matrices/s", "h2d_bytes_per_step": host.nbytes,
+               "d2h_bytes_per_step": host.nbytes + 8 * b.total_records + 4 * count,
+               "ms_per_step": e_ms, "api": "Batch.getrf_graph (dp_batch_getrf_graph)"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = _cpu_batched_baseline(ns, nz, seed)
+    if rank == 0:
+        line = {"metric": BATCH_METRIC, "value": value, "unit": "matrices/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic: N(0,1) MT19937-64 per matrix, 0-2 zero columns (p = 0.3)",
+                "config": {"workload": f"batched delayed_getrf, {count} matrices, n log-uniform "
+                                       f"[32, 512], one CUDA-graph launch per step",
+                           "nb_bucket": list(tuned.nb_bucket), "gflop_per_step": fl / 1e9,
+                           "parallelism": f"replicas x{world}",
+                           "l2": f"{host.nbytes / 1e9:.2f} GB per step > L2 (no flush needed)"},
+                "roofline": {"bound": "tensor", "kernel": "batched_getrf_kernel (whole launch)",
+                             "achieved": tf, "peak": fp64, "unit": "TFLOP/s", "frac": tf / fp64,
+                             "peak_source": "cuBLAS DGEMM 8192^3 measured live",
+                             "hbm_gbs": bytes_alg * args.steps / (ms * 1e-3) / 1e9,
+                             "hbm_peak_gbs": measured_peaks().get("hbm_gbs"), "traffic": None},
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def _cpu_batched_baseline(ns, nz, seed, budget_s=15.0):
+    """The reference's delayed_getrf on the host cores, matrix after matrix
+    (OpenBLAS threads inside each), over the first matrices of the batch."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import delayed_pivoting as dp
+    import oracle as orc
+
+    kind, fn = ("reference", orc.ref_getrf) if orc.ref_available() else ("port", orc.oracle_getrf)
+    threads = os.cpu_count() or 1
+    if kind == "reference":
+        orc.ref_lib().ref_set_threads(threads)
+    t, k = 0.0, 0
+    while k < len(ns) and t < budget_s:
+        a = dp.batch_matrix(ns, nz, seed, k)
+        t0 = time.perf_counter()
+        fn(a)
+        t += time.perf_counter() - t0
+        k += 1
+    return {"value": k / t, "unit": "matrices/s", "cores": threads, "kind": kind,
+            "sample": f"first {k} matrices of the batch, one delayed_getrf each, {t:.1f} s"}
+
+
+def batched_reference_arm(args):
+    import delayed_pivoting as dp
+
+    ns, nz = dp.batch_orders(args.count, 8192)
+    vals, cpu, t_all = [], None, 0.0
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        cpu = _cpu_batched_baseline(ns, nz, 8192, budget_s=10.0)
+        if i >= args.warmup:
+            vals.append(cpu["value"])
+            t_all += time.perf_counter() - t0
+    value = float(np.mean(vals))
+    print(json.dumps({"impl": "reference", "metric": BATCH_METRIC, "value": value,
+                      "unit": "matrices/s", "n_gpus": args.gpus, "steps": args.steps,
+                      "warmup": args.warmup, "ms_per_step": t_all / max(args.steps, 1) * 1e3,
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                      "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": f"batched delayed_getrf, {args.count} matrices"},
+                      "cpu_baseline": dict(cpu, value=value),
+                      "e2e": {"value": value, "unit": "matrices/s", "h2d_bytes_per_step": 0,
+                              "d2h_bytes_per_step": 0}}), flush=True)
+    return 0
+
+
+def ctypes_longlong():
+    import ctypes
+
+    return ctypes.c_longlong
 
 
 def _stats(L):

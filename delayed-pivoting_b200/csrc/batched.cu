@@ -732,6 +732,7 @@ int launch_raw(int count, int max_n, int sms, const int* d_n, const long long* d
     return DP_CUDA_FAILURE;
   const int grid = std::max(1, std::min(count, sms * per_sm));
   if (cudaMemsetAsync(d_queue, 0, sizeof(int), st) != cudaSuccess) return DP_CUDA_FAILURE;
+  dp::note_launch();
   batched_getrf_kernel<<<grid, kThreads, smem, st>>>(p);
   return cudaGetLastError() == cudaSuccess ? DP_SUCCESS : DP_CUDA_FAILURE;
 }
@@ -935,6 +936,7 @@ int dp_batch_autotune(dp_batch_options* opt, int samples, unsigned long long see
         cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
       rc = DP_ALLOCATION_FAILED;
     } else {
+      dp::note_launch();
       dp::batch::fill_normal_kernel<<<1184, 256, 0, st>>>(d_src, bp->total_elements,
                                                           seed + 0x1000003ull * bk);
       float best_ms = 1e30f;

@@ -4,10 +4,18 @@
 #pragma once
 
 #include <cstddef>
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
 namespace dp {
+
+// Kernel launches issued by this library since it was loaded (every launch
+// site calls note_launch); read through dp_kernel_launches().
+inline std::atomic<long long> g_kernel_launches{0};
+inline void note_launch(long long k = 1) {
+  g_kernel_launches.fetch_add(k, std::memory_order_relaxed);
+}
 
 // Status codes shared by kernels and host (values of the C ABI).
 enum : int {

@@ -86,6 +86,26 @@ void launch_swap_col(double* a, long long lda, int m, int c1, int c2, cudaStream
 void launch_identity_records(int* ipiv, int* jpiv, int count, cudaStream_t s);
 void launch_set_record(int* ipiv, int* jpiv, int k, int p, int q, cudaStream_t s);
 
+// ---- triangular solves with many right-hand sides (trisolve.cu) ----------
+
+// Y (n x nrhs, nrhs <= tri_solve_rhs_max()) <- L^{-1} Y (unit lower) or
+// U^{-1} Y (upper with diagonal), one cooperative launch; `flags` holds
+// tri_solve_flag_count(n) words whose values differ from `epoch` (nonzero,
+// new for every launch that uses the same flags); a bounded wait that runs
+// out sets *status = kDeviceTimeout.
+// `inv` holds the inverses of the 64 x 64 diagonal blocks of L and U
+// (launch_diag_inverse, tri_inverse_doubles(n) doubles, 16-byte aligned).
+int tri_solve_rhs_max();
+int tri_solve_flag_count(int n);
+size_t tri_inverse_doubles(int n);
+int launch_diag_inverse(const double* lu, long long ldlu, int n, double* inv, cudaStream_t st);
+int launch_tri_lower_unit(const double* L, long long ldl, int n, const double* inv, double* Y,
+                          long long ldy, int nrhs, unsigned* flags, unsigned epoch, int* status,
+                          cudaStream_t st);
+int launch_tri_upper(const double* U, long long ldu, int n, const double* inv, double* Y,
+                     long long ldy, int nrhs, unsigned* flags, unsigned epoch, int* status,
+                     cudaStream_t st);
+
 // ---- resident factorisations (solve.cu) ----------------------------------
 
 // A factorisation kept on the device for repeated solves: the compact L\U,
@@ -99,6 +119,9 @@ struct Factor {
   double factor_ms = 0.0;             // device time of all factorisations
   double* lu = nullptr;
   int* d_perm = nullptr;              // row order [n], column order [n]
+  unsigned* d_flags = nullptr;        // triangular-solve block flags, then a status word
+  double* d_inv = nullptr;            // inverses of the diagonal blocks of L and U
+  unsigned epoch = 0;                 // last epoch used on d_flags
   std::vector<int> ipiv, jpiv;
 };
 

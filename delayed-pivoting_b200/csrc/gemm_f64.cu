@@ -197,18 +197,25 @@ void launch(int M, int N, int K, const double* A, long long lda, const double* B
     configured = true;
   }
   dim3 grid((M + C::BM - 1) / C::BM, (N + C::BN - 1) / C::BN);
+  dp::note_launch();
   dgemm_minus_kernel<C><<<grid, C::THREADS, C::SMEM, s>>>(M, N, K, A, lda, B, ldb, Cm, ldc);
 }
 
 // Production configuration: 128 x 128 tiles, 8 warps of 64 x 32.
 using Big = Cfg<128, 128, 32, 3, 2, 4, 1>;
+// Few columns (the refinement residual B - A X, N = right-hand sides): 64 x 32
+// tiles, 4 warps of 16 x 32, two CTAs per SM, so M / 64 CTAs stream A.
+using Skinny = Cfg<64, 32, 32, 4, 4, 1, 2>;
 
 }  // namespace gemm
 
 void launch_gemm_minus(int M, int N, int K, const double* A, long long lda, const double* B,
                        long long ldb, double* C, long long ldc, cudaStream_t s) {
   if (M <= 0 || N <= 0 || K <= 0) return;
-  gemm::launch<gemm::Big>(M, N, K, A, lda, B, ldb, C, ldc, s);
+  if (N <= 32)
+    gemm::launch<gemm::Skinny>(M, N, K, A, lda, B, ldb, C, ldc, s);
+  else
+    gemm::launch<gemm::Big>(M, N, K, A, lda, B, ldb, C, ldc, s);
 }
 
 }  // namespace dp

@@ -351,12 +351,14 @@ int launch_gemm_minus_mixed(int M, int N, int K, const double* A, long long lda,
   auto* al = ah + (size_t)M * kp;
   auto* bh = al + (size_t)M * kp;
   auto* bl = bh + (size_t)N * kp;
+  dp::note_launch();
   split_a_kernel<<<dim3((M + 31) / 32, (kp + 31) / 32), dim3(32, 8), 0, s>>>(A, lda, M, K, kp, ah,
                                                                             al);
   {
     const long long total = (long long)N * kp;
     long long grid = (total + 255) / 256;
     if (grid > 148 * 16) grid = 148 * 16;
+    dp::note_launch();
     split_b_kernel<<<(int)grid, 256, 0, s>>>(B, ldb, K, N, kp, bh, bl);
   }
   CUtensorMap tah, tal, tbh, tbl;
@@ -364,6 +366,7 @@ int launch_gemm_minus_mixed(int M, int N, int K, const double* A, long long lda,
       !make_map(&tbl, bl, N, kp))
     return kLibraryFailure;
   dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
+  dp::note_launch();
   gemm_bf16x3_kernel<<<grid, kThreads, kSmem, s>>>(tah, tal, tbh, tbl, M, N, kp / BK, C, ldc,
                                                    status);
   return cudaGetLastError() == cudaSuccess ? kOk : kCudaFailure;

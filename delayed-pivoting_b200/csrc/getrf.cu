@@ -440,9 +440,11 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
         cfg.stream = st;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
+        dp::note_launch();
         DP_CHECK_CUDA(cudaLaunchKernelEx(&cfg, panel_cluster_kernel, pp));
       } else {
         void* args[] = {&pp};
+        dp::note_launch();
         DP_CHECK_CUDA(cudaLaunchCooperativeKernel((const void*)panel_factor_kernel, G,
                                                   kPanelThreadsHost, args, panel_smem_bytes(w, R),
                                                   st));
@@ -857,3 +859,5 @@ DelayedGetrfCudaStatus delayed_getrf_cuda_hybrid_host(int m, int n, double* a, i
 const char* delayed_getrf_cuda_status_string(DelayedGetrfCudaStatus status) {
   return dp_status_string(static_cast<int>(status));
 }
+
+extern "C" long long dp_kernel_launches(void) { return dp::g_kernel_launches.load(); }

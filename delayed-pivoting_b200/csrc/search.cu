@@ -149,17 +149,20 @@ void launch_search_active(const double* a, long long lda, int m, int n, int k, S
   long long grid = (cols + warps - 1) / warps;
   if (grid > max_blocks) grid = max_blocks;
   if (grid < 1) grid = 1;
+  dp::note_launch();
   search_active_kernel<<<(int)grid, kSearchThreads, 0, s>>>(a, lda, m, n, k, state, block_cands);
 }
 
 void launch_search_nonzero_column(const double* a, long long lda, int m, int n, int k,
                                   double threshold, State* state, cudaStream_t s) {
+  dp::note_launch();
   reset_fallback_kernel<<<1, 1, 0, s>>>(state, k);
   const long long cols = (long long)n - k - 1;
   const int warps = kSearchThreads / 32;
   long long grid = (cols + warps - 1) / warps;
   if (grid > 148 * 8) grid = 148 * 8;
   if (grid < 1) grid = 1;
+  dp::note_launch();
   search_nonzero_column_kernel<<<(int)grid, kSearchThreads, 0, s>>>(a, lda, m, n, k, threshold,
                                                                    state);
 }

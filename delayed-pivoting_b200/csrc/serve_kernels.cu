@@ -238,6 +238,7 @@ size_t solve_smem(int max_n) { return sizeof(double) * (size_t)kChunk * (max_n +
 int launch_orders(const int* ns, const long long* rec, const int* ipiv, const int* jpiv,
                   int* row_order, int* col_order, int count, cudaStream_t st) {
   if (count <= 0) return kOk;
+  dp::note_launch();
   orders_kernel<<<count, 32, 0, st>>>(ns, rec, ipiv, jpiv, row_order, col_order, count);
   return cudaGetLastError() == cudaSuccess ? kOk : kCudaFailure;
 }
@@ -248,6 +249,7 @@ int launch_solve(const SolveItem* items, int count, int max_n, cudaStream_t st) 
   if (cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
       cudaSuccess)
     return kCudaFailure;
+  dp::note_launch();
   solve_kernel<<<count, kThreads, sm, st>>>(items);
   return cudaGetLastError() == cudaSuccess ? kOk : kCudaFailure;
 }
@@ -258,18 +260,21 @@ int launch_residual(const ResidualItem* items, double* err, int count, int max_n
   if (cudaFuncSetAttribute(residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)sm) != cudaSuccess)
     return kCudaFailure;
+  dp::note_launch();
   residual_kernel<<<count, kThreads, sm, st>>>(items, err);
   return cudaGetLastError() == cudaSuccess ? kOk : kCudaFailure;
 }
 
 int launch_axpy(const AxpyItem* items, int count, cudaStream_t st) {
   if (count <= 0) return kOk;
+  dp::note_launch();
   axpy_kernel<<<count, kThreads, 0, st>>>(items);
   return cudaGetLastError() == cudaSuccess ? kOk : kCudaFailure;
 }
 
 int launch_copy(const CopyItem* items, int count, cudaStream_t st) {
   if (count <= 0) return kOk;
+  dp::note_launch();
   copy_kernel<<<count, kThreads, 0, st>>>(items);
   return cudaGetLastError() == cudaSuccess ? kOk : kCudaFailure;
 }

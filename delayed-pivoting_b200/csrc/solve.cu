@@ -107,30 +107,48 @@ int grid_of(long long work) {
 
 }  // namespace
 
-// L y = b (unit lower, n x n at lu) in place on B (n x nrhs).
-void forward_solve(const double* lu, long long ldlu, int n, double* B, long long ldb, int nrhs,
-                   cudaStream_t st) {
-  const int tw = trsm_max_width();
-  for (int b = 0; b < n; b += tw) {
-    const int w = std::min(tw, n - b);
-    launch_trsm_lower_unit(lu + idx(b, b, ldlu), ldlu, B + b, ldb, w, nrhs, st);
-    if (b + w < n)
-      launch_gemm_minus(n - b - w, nrhs, w, lu + idx(b + w, b, ldlu), ldlu, B + b, ldb, B + b + w,
-                        ldb, st);
+// T (n x nrhs at leading dimension n) <- U^{-1} L^{-1} T with the compact L\U
+// at lu: the two triangular solves in launches of up to tri_solve_rhs_max()
+// right-hand sides, each with a fresh epoch of `flags`.
+int lu_solve_inplace(const double* lu, long long ldlu, int n, const double* inv, double* T,
+                     int nrhs, unsigned* flags, unsigned& epoch, cudaStream_t st) {
+  int* status = reinterpret_cast<int*>(flags + tri_solve_flag_count(n));
+  const int cmax = tri_solve_rhs_max();
+  for (int c0 = 0; c0 < nrhs; c0 += cmax) {
+    const int nc = std::min(cmax, nrhs - c0);
+    for (int up = 0; up < 2; ++up) {
+      if (++epoch == 0) ++epoch;
+      const int s = up ? launch_tri_upper(lu, ldlu, n, inv, T + (size_t)c0 * n, n, nc, flags,
+                                          epoch, status, st)
+                       : launch_tri_lower_unit(lu, ldlu, n, inv, T + (size_t)c0 * n, n, nc,
+                                               flags, epoch, status, st);
+      if (s != kOk) return s;
+    }
   }
+  return kOk;
 }
 
-// U x = y (upper with diagonal, n x n at lu) in place on B (n x nrhs).
-void backward_solve(const double* lu, long long ldlu, int n, double* B, long long ldb, int nrhs,
-                    cudaStream_t st) {
-  const int tw = trsm_max_width();
-  const int nblocks = (n + tw - 1) / tw;
-  for (int bi = nblocks - 1; bi >= 0; --bi) {
-    const int b = bi * tw;
-    const int w = std::min(tw, n - b);
-    launch_trsm_upper(lu + idx(b, b, ldlu), ldlu, B + b, ldb, w, nrhs, st);
-    if (b > 0) launch_gemm_minus(b, nrhs, w, lu + idx(0, b, ldlu), ldlu, B + b, ldb, B, ldb, st);
+// Flags + status word for lu_solve_inplace at order n (zeroed).
+int alloc_flags(int n, unsigned** flags, cudaStream_t st) {
+  const size_t bytes = sizeof(unsigned) * ((size_t)tri_solve_flag_count(n) + 1);
+  if (cudaMallocAsync(reinterpret_cast<void**>(flags), bytes, st) != cudaSuccess) {
+    cudaGetLastError();
+    *flags = nullptr;
+    return kAllocationFailed;
   }
+  if (cudaMemsetAsync(*flags, 0, bytes, st) != cudaSuccess) return kCudaFailure;
+  return kOk;
+}
+
+// kOk, or the status a triangular solve left in the flags' status word
+// (synchronises st).
+int solve_status(const unsigned* flags, int n, cudaStream_t st) {
+  int h = 0;
+  if (cudaMemcpyAsync(&h, flags + tri_solve_flag_count(n), sizeof(int), cudaMemcpyDeviceToHost,
+                      st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return kCudaFailure;
+  return h == 0 ? kOk : h;
 }
 
 int getrs_device(int n, int nrhs, const double* lu, int ldlu, const int* ipiv, const int* jpiv,
@@ -147,9 +165,21 @@ int getrs_device(int n, int nrhs, const double* lu, int ldlu, const int* ipiv, c
   }
   int* d_perm = nullptr;
   double* tmp = nullptr;
+  unsigned* flags = nullptr;
+  unsigned epoch = 0;
+  double* inv = nullptr;
+  if (alloc_flags(n, &flags, st) != kOk) return kAllocationFailed;
+  if (cudaMallocAsync(reinterpret_cast<void**>(&inv), sizeof(double) * tri_inverse_doubles(n),
+                      st) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFreeAsync(flags, st);
+    return kAllocationFailed;
+  }
   if (cudaMallocAsync(reinterpret_cast<void**>(&d_perm), sizeof(int) * 2 * (size_t)n, st) !=
       cudaSuccess) {
     cudaGetLastError();
+    cudaFreeAsync(flags, st);
+    cudaFreeAsync(inv, st);
     return kAllocationFailed;
   }
   if (cudaMallocAsync(reinterpret_cast<void**>(&tmp), sizeof(double) * (size_t)n * nrhs, st) !=
@@ -166,14 +196,21 @@ int getrs_device(int n, int nrhs, const double* lu, int ldlu, const int* ipiv, c
     status = kCudaFailure;
   if (status == kOk) {
     const long long total = (long long)n * nrhs;
+    dp::note_launch();
     gather_rows_kernel<<<grid_of(total), 256, 0, st>>>(B, ldb, tmp, n, d_perm, n, nrhs);
-    forward_solve(lu, ldlu, n, tmp, n, nrhs, st);
-    backward_solve(lu, ldlu, n, tmp, n, nrhs, st);
-    scatter_rows_kernel<<<grid_of(total), 256, 0, st>>>(tmp, n, B, ldb, d_perm + n, n, nrhs);
-    if (cudaGetLastError() != cudaSuccess) status = kCudaFailure;
+    status = launch_diag_inverse(lu, ldlu, n, inv, st);
+    if (status == kOk) status = lu_solve_inplace(lu, ldlu, n, inv, tmp, nrhs, flags, epoch, st);
+    if (status == kOk) {
+      dp::note_launch();
+      scatter_rows_kernel<<<grid_of(total), 256, 0, st>>>(tmp, n, B, ldb, d_perm + n, n, nrhs);
+    }
+    if (cudaGetLastError() != cudaSuccess && status == kOk) status = kCudaFailure;
+    if (status == kOk) status = solve_status(flags, n, st);
   }
   cudaFreeAsync(tmp, st);
   cudaFreeAsync(d_perm, st);
+  cudaFreeAsync(flags, st);
+  cudaFreeAsync(inv, st);
   if (cudaStreamSynchronize(st) != cudaSuccess && status == kOk) status = kCudaFailure;
   return status;
 }
@@ -185,11 +222,14 @@ int backward_error(const double* A, int lda, int n, const double* B, int ldb, co
                    int ldx, int nrhs, double* R, double* norms, double normA,
                    const std::vector<double>& normB, double& berr, cudaStream_t st) {
   const long long total = (long long)n * nrhs;
+  dp::note_launch();
   copy_kernel<<<grid_of(total), 256, 0, st>>>(B, ldb, R, n, n, nrhs);
   launch_gemm_minus(n, nrhs, n, A, lda, X, ldx, R, n, st);
   if (cudaMemsetAsync(norms, 0, sizeof(double) * 2 * nrhs, st) != cudaSuccess) return kCudaFailure;
   dim3 g((unsigned)std::min(64, (n + 255) / 256), (unsigned)nrhs);
+  dp::note_launch();
   colmax_kernel<<<g, 256, 0, st>>>(R, n, n, nrhs, norms);
+  dp::note_launch();
   colmax_kernel<<<g, 256, 0, st>>>(X, ldx, n, nrhs, norms + nrhs);
   std::vector<double> h(2 * (size_t)nrhs);
   if (cudaMemcpyAsync(h.data(), norms, sizeof(double) * 2 * nrhs, cudaMemcpyDeviceToHost, st) !=
@@ -212,6 +252,7 @@ namespace {
 // lu <- A, factor at `prec`, composite orders to the device.
 int factorize(Factor& f, const double* A, int lda, int prec, cudaStream_t st) {
   const int n = f.n;
+  dp::note_launch();
   copy_kernel<<<grid_of((long long)n * n), 256, 0, st>>>(A, lda, f.lu, n, n, n);
   dp_options opt;
   dp_options_init(&opt);
@@ -240,20 +281,23 @@ int factorize(Factor& f, const double* A, int lda, int prec, cudaStream_t st) {
   }
   if (cudaMemcpyAsync(f.d_perm, order.data(), sizeof(int) * 2 * (size_t)n, cudaMemcpyHostToDevice,
                       st) != cudaSuccess ||
-      cudaStreamSynchronize(st) != cudaSuccess)
+      launch_diag_inverse(f.lu, n, n, f.d_inv, st) != kOk || cudaStreamSynchronize(st) != cudaSuccess)
     return kCudaFailure;
   return kOk;
 }
 
 // X = A^{-1} B through the factors (X, tmp: n x nrhs, leading dimension n).
-void solve_with(const Factor& f, const double* B, int ldb, double* X, double* tmp, int nrhs,
-                cudaStream_t st) {
+int solve_with(Factor& f, const double* B, int ldb, double* X, double* tmp, int nrhs,
+               cudaStream_t st) {
   const int n = f.n;
   const long long total = (long long)n * nrhs;
+  dp::note_launch();
   gather_rows_kernel<<<grid_of(total), 256, 0, st>>>(B, ldb, tmp, n, f.d_perm, n, nrhs);
-  forward_solve(f.lu, n, n, tmp, n, nrhs, st);
-  backward_solve(f.lu, n, n, tmp, n, nrhs, st);
+  const int s = lu_solve_inplace(f.lu, n, n, f.d_inv, tmp, nrhs, f.d_flags, f.epoch, st);
+  if (s != kOk) return s;
+  dp::note_launch();
   scatter_rows_kernel<<<grid_of(total), 256, 0, st>>>(tmp, n, X, n, f.d_perm + n, n, nrhs);
+  return cudaGetLastError() == cudaSuccess ? kOk : kCudaFailure;
 }
 
 }  // namespace
@@ -262,11 +306,16 @@ void factor_destroy(Factor* f, cudaStream_t st) {
   if (!f) return;
   if (f->lu) cudaFreeAsync(f->lu, st);
   if (f->d_perm) cudaFreeAsync(f->d_perm, st);
+  if (f->d_flags) cudaFreeAsync(f->d_flags, st);
+  if (f->d_inv) cudaFreeAsync(f->d_inv, st);
   cudaStreamSynchronize(st);
   delete f;
 }
 
-size_t factor_bytes(int n) { return sizeof(double) * (size_t)n * n + sizeof(int) * 2 * (size_t)n; }
+size_t factor_bytes(int n) {
+  return sizeof(double) * ((size_t)n * n + tri_inverse_doubles(n)) + sizeof(int) * 2 * (size_t)n +
+         sizeof(unsigned) * ((size_t)tri_solve_flag_count(n) + 1);
+}
 
 int factor_create(Factor** out, int n, const double* A, int lda, int precision, cudaStream_t st) {
   if (!out) return kInvalidArgument;
@@ -290,9 +339,22 @@ int factor_create(Factor** out, int n, const double* A, int lda, int precision, 
     factor_destroy(f, st);
     return kAllocationFailed;
   }
-  int status = kOk;
+  int status = alloc_flags(n, &f->d_flags, st);
+  if (status == kOk &&
+      cudaMallocAsync(reinterpret_cast<void**>(&f->d_inv), sizeof(double) * tri_inverse_doubles(n),
+                      st) != cudaSuccess) {
+    cudaGetLastError();
+    f->d_inv = nullptr;
+    status = kAllocationFailed;
+  }
+  if (status != kOk) {
+    cudaFreeAsync(normA, st);
+    factor_destroy(f, st);
+    return status;
+  }
   if (cudaMemsetAsync(normA, 0, sizeof(double), st) != cudaSuccess) status = kCudaFailure;
   if (status == kOk) {
+    dp::note_launch();
     row_abs_sum_kernel<<<(n + 255) / 256, 256, 0, st>>>(A, lda, n, normA);
     if (cudaMemcpyAsync(&f->normA, normA, sizeof(double), cudaMemcpyDeviceToHost, st) !=
             cudaSuccess ||
@@ -362,6 +424,7 @@ int factor_solve(Factor* f, const double* A, int lda, double* B, int ldb, int nr
   {
     if (cudaMemsetAsync(norms, 0, sizeof(double) * nrhs, st) != cudaSuccess) status = kCudaFailure;
     dim3 g((unsigned)std::min(64, (n + 255) / 256), (unsigned)nrhs);
+    dp::note_launch();
     colmax_kernel<<<g, 256, 0, st>>>(B, ldb, n, nrhs, norms);
     if (status == kOk &&
         (cudaMemcpyAsync(normB.data(), norms, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st) !=
@@ -385,7 +448,9 @@ int factor_solve(Factor* f, const double* A, int lda, double* B, int ldb, int nr
       if (it >= iters_left) return kOk;
       if (it > 0 && !(berr <= 0.5 * prev)) return kOk;  // stalled
       prev = berr;
-      solve_with(*f, R, n, R, T, nrhs, st);
+      s = solve_with(*f, R, n, R, T, nrhs, st);
+      if (s != kOk) return s;
+      dp::note_launch();
       axpy_kernel<<<grid_of((long long)nr), 256, 0, st>>>(R, n, X, n, n, nrhs);
       res->iterations += 1;
     }
@@ -398,16 +463,16 @@ int factor_solve(Factor* f, const double* A, int lda, double* B, int ldb, int nr
   const double fms0 = f->factor_ms - res->factor_ms;
   bool converged = false;
   if (status == kOk) {
-    solve_with(*f, B, ldb, X, T, nrhs, st);
-    status = refine(max_iter, converged);
+    status = solve_with(*f, B, ldb, X, T, nrhs, st);
+    if (status == kOk) status = refine(max_iter, converged);
   }
   if (status == kOk && !converged && f->precision != DP_PRECISION_FP64) {
     // the mixed-precision factors cannot carry this matrix: plain FP64
     f->refactored = 1;
     status = factorize(*f, A, lda, DP_PRECISION_FP64, st);
     if (status == kOk && f->info == n) {
-      solve_with(*f, B, ldb, X, T, nrhs, st);
-      status = refine(max_iter, converged);
+      status = solve_with(*f, B, ldb, X, T, nrhs, st);
+      if (status == kOk) status = refine(max_iter, converged);
     }
   }
   cudaEventRecord(t1, st);
@@ -416,13 +481,16 @@ int factor_solve(Factor* f, const double* A, int lda, double* B, int ldb, int nr
   cudaEventElapsedTime(&tot, t0, t1);
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
+  if (status == kOk) status = solve_status(f->d_flags, n, st);
   res->total_ms = tot;
   res->factor_ms = f->factor_ms - fms0;
   res->info = f->info;
   res->refactored = f->refactored;
   res->converged = converged ? 1 : 0;
-  if (status == kOk && f->info == n)
+  if (status == kOk && f->info == n) {
+    dp::note_launch();
     copy_kernel<<<grid_of((long long)nr), 256, 0, st>>>(X, n, B, ldb, n, nrhs);
+  }
   release();
   return status;
 }

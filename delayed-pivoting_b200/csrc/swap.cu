@@ -132,26 +132,31 @@ void launch_laswp(double* a, long long lda, int begin, int nblock, const int* sw
   if (ncols <= 0 || nblock <= 0) return;
   const int warps = kLaswpThreads / 32;
   const int grid = grid_for(ncols, warps, 148 * 16);
+  dp::note_launch();
   laswp_kernel<<<grid, kLaswpThreads, 0, s>>>(a, lda, begin, nblock, swap_block, swap_extra,
                                               state, c0, c1, c2, c3);
 }
 
 void launch_swap_row(double* a, long long lda, int n, int r1, int r2, cudaStream_t s) {
   if (r1 == r2 || n <= 0) return;
+  dp::note_launch();
   swap_row_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(a, lda, n, r1, r2);
 }
 
 void launch_swap_col(double* a, long long lda, int m, int c1, int c2, cudaStream_t s) {
   if (c1 == c2 || m <= 0) return;
+  dp::note_launch();
   swap_col_kernel<<<grid_for(m, 256, 148 * 8), 256, 0, s>>>(a, lda, m, c1, c2);
 }
 
 void launch_set_record(int* ipiv, int* jpiv, int k, int p, int q, cudaStream_t s) {
+  dp::note_launch();
   set_record_kernel<<<1, 1, 0, s>>>(ipiv, jpiv, k, p, q);
 }
 
 void launch_identity_records(int* ipiv, int* jpiv, int count, cudaStream_t s) {
   if (count <= 0) return;
+  dp::note_launch();
   identity_records_kernel<<<grid_for(count, 256, 148 * 4), 256, 0, s>>>(ipiv, jpiv, count);
 }
 

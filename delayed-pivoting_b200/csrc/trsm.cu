@@ -187,6 +187,7 @@ void launch_trsm_lower_unit(const double* L, long long ldl, double* B, long long
   if (w <= 1 || nc <= 0) return;  // w == 1: unit diagonal, nothing to solve
   configure();
   const int grid = (nc + kTrsmCols - 1) / kTrsmCols;
+  dp::note_launch();
   trsm_lower_unit_kernel<<<grid, kTrsmThreads, kTrsmSmem, s>>>(L, ldl, B, ldb, w, nc);
 }
 
@@ -195,6 +196,7 @@ void launch_trsm_upper(const double* U, long long ldu, double* B, long long ldb,
   if (w <= 0 || nc <= 0) return;
   configure();
   const int grid = (nc + kTrsmCols - 1) / kTrsmCols;
+  dp::note_launch();
   trsm_upper_kernel<<<grid, kTrsmThreads, kTrsmSmem, s>>>(U, ldu, B, ldb, w, nc);
 }
 

@@ -299,6 +299,10 @@ void dp_stats_enable(int on);
 void dp_stats_reset(void);
 void dp_stats_get(dp_kernel_stats *out);
 
+/* Kernel launches this library has issued since it was loaded, on every
+ * stream and host thread (no reference counterpart). */
+long long dp_kernel_launches(void);
+
 /* delayed_dgetrf_cuda.hpp:63 (delayed_getrf_cuda_status_string). */
 const char *dp_status_string(int status);
 
