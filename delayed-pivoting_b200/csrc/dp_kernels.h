@@ -61,13 +61,22 @@ void launch_trsm_upper(const double* U, long long ldu, double* B, long long ldb,
 void launch_gemm_minus(int M, int N, int K, const double* A, long long lda, const double* B,
                        long long ldb, double* C, long long ldc, cudaStream_t s);
 
-// C(M x N) -= A(M x K) * B(K x N) on the tensor cores (BF16 hi/lo split,
-// three products, FP32 accumulation in TMEM); scratch of
-// mixed_scratch_bytes(M, N, K) bytes.  Returns a status code.
-size_t mixed_scratch_bytes(int max_rows, int max_cols, int max_k);
+// C(M x N) -= A(M x K) * B(K x N) on the tensor cores (BF16 split into
+// `terms` pieces: 2 -> three products, 3 -> six products; FP32 accumulation in
+// TMEM); scratch of mixed_scratch_bytes(M, N, K, terms) bytes.  Returns a
+// status code.
+size_t mixed_scratch_bytes(int max_rows, int max_cols, int max_k, int terms);
 int launch_gemm_minus_mixed(int M, int N, int K, const double* A, long long lda, const double* B,
-                            long long ldb, double* C, long long ldc, void* scratch, int* status,
-                            cudaStream_t s);
+                            long long ldb, double* C, long long ldc, void* scratch, int terms,
+                            int* status, cudaStream_t s);
+// Split pieces of a mixed precision (0 for DP_PRECISION_FP64).
+inline int mixed_terms(int precision) {
+  return precision == DP_PRECISION_MIXED_BF16X6 ? 3 : precision == DP_PRECISION_MIXED_BF16X3 ? 2 : 0;
+}
+inline bool valid_precision(int precision) {
+  return precision == DP_PRECISION_FP64 || precision == DP_PRECISION_MIXED_BF16X3 ||
+         precision == DP_PRECISION_MIXED_BF16X6;
+}
 
 // Full-pivot search over a(k:m, k:n); result in state->fallback.
 void launch_search_active(const double* a, long long lda, int m, int n, int k, State* state,

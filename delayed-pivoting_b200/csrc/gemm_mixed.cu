@@ -1,13 +1,17 @@
 // Mixed-precision Schur-complement update on the 5th-generation tensor cores:
 //   C(M x N, FP64) -= A(M x K, FP64) * B(K x N, FP64)
-// with the product formed from a BF16 hi/lo split of A and B as
-//   Ah*Bh + Ah*Bl + Al*Bh          (three tcgen05.mma kind::f16 products)
+// with the product formed from a BF16 split of A and B into TERMS pieces
+// (x = x1 + x2 [+ x3], each piece the BF16 rounding of what the earlier ones
+// left) and the products whose pieces sum to at most TERMS - 1 ranks below
+// the leading one:
+//   TERMS = 2 (BF16x3):  A1B1 + A1B2 + A2B1                   (3 products)
+//   TERMS = 3 (BF16x6):  A1B1 + A1B2 + A2B1 + A1B3 + A2B2 + A3B1  (6 products)
 // accumulated in FP32 in tensor memory, then subtracted from C in FP64.
 // This replaces the FP64 trailing update (delayed_lu/delayed_dgetrf.cpp:80-83)
 // in the mixed-precision factorisation; pivot search, delay / fallback
 // decisions and the panel stay in FP64.  Relative error of one update is about
-// 2^-16 (the dropped Al*Bl term and the BF16 rounding of the low parts) plus
-// FP32 accumulation; FP64 iterative refinement recovers full accuracy.
+// 2^-16 with three products and about 2^-24 (FP32 accumulation) with six;
+// FP64 iterative refinement recovers full accuracy.
 //
 // Pipeline (one CTA per 128 x 128 tile of C, 4 warps):
 //   split_*_kernel  FP64 column-major -> BF16 hi / lo, K-major, K padded to 64
@@ -35,21 +39,30 @@ namespace mixed {
 constexpr int BM = 128, BN = 128, BK = 64;  // BK: BF16 elements per 128-byte swizzle row
 constexpr int kThreads = 128;
 constexpr int kTileBytes = BM * BK * 2;     // 16 KB per operand tile (BN == BM)
-constexpr int kStageBytes = 4 * kTileBytes; // Ah, Al, Bh, Bl
 constexpr int kStages = 2;
-constexpr size_t kSmem = (size_t)kStages * kStageBytes + 1024;  // + alignment slack
 constexpr unsigned kTmemCols = BN;
+// A pieces then B pieces per stage
+template <int TERMS>
+constexpr int stage_bytes() { return 2 * TERMS * kTileBytes; }
+template <int TERMS>
+constexpr size_t smem_bytes() { return (size_t)kStages * stage_bytes<TERMS>() + 1024; }
 
 // ---------------------------------------------------------------- split ----
-__device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
-  hi = __double2bfloat16(x);
-  lo = __double2bfloat16(x - (double)__bfloat162float(hi));
+template <int TERMS>
+__device__ __forceinline__ void split_bf16(double x, __nv_bfloat16 (&piece)[TERMS]) {
+#pragma unroll
+  for (int t = 0; t < TERMS; ++t) {
+    piece[t] = __double2bfloat16(x);
+    x -= (double)__bfloat162float(piece[t]);
+  }
 }
 
-// A (M x K, column-major, lda) -> Ah, Al as [M][Kp] (K contiguous).  32x32
-// tiles transposed through shared memory so both sides stay coalesced.
+// A (M x K, column-major, lda) -> pieces [t][M][Kp] (K contiguous), piece t at
+// out + t * M * Kp.  32x32 tiles transposed through shared memory so both
+// sides stay coalesced.
+template <int TERMS>
 __global__ void split_a_kernel(const double* __restrict__ A, long long lda, int M, int K, int Kp,
-                               __nv_bfloat16* __restrict__ Ah, __nv_bfloat16* __restrict__ Al) {
+                               __nv_bfloat16* __restrict__ out) {
   __shared__ double t[32][33];
   const int m0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
@@ -61,26 +74,27 @@ __global__ void split_a_kernel(const double* __restrict__ A, long long lda, int 
   for (int i = ty; i < 32; i += 8) {
     const int m = m0 + i, k = k0 + tx;
     if (m < M && k < Kp) {
-      __nv_bfloat16 h, l;
-      split_bf16(t[tx][i], h, l);
-      Ah[(size_t)m * Kp + k] = h;
-      Al[(size_t)m * Kp + k] = l;
+      __nv_bfloat16 pc[TERMS];
+      split_bf16<TERMS>(t[tx][i], pc);
+#pragma unroll
+      for (int q = 0; q < TERMS; ++q) out[(size_t)q * M * Kp + (size_t)m * Kp + k] = pc[q];
     }
   }
 }
 
-// B (K x N, column-major, ldb) -> Bh, Bl as [N][Kp] (K contiguous).
+// B (K x N, column-major, ldb) -> pieces [t][N][Kp] (K contiguous).
+template <int TERMS>
 __global__ void split_b_kernel(const double* __restrict__ B, long long ldb, int K, int N, int Kp,
-                               __nv_bfloat16* __restrict__ Bh, __nv_bfloat16* __restrict__ Bl) {
+                               __nv_bfloat16* __restrict__ out) {
   const long long total = (long long)N * Kp;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
     const int n = (int)(e / Kp), k = (int)(e - (long long)n * Kp);
     const double x = k < K ? B[idx(k, n, ldb)] : 0.0;
-    __nv_bfloat16 h, l;
-    split_bf16(x, h, l);
-    Bh[e] = h;
-    Bl[e] = l;
+    __nv_bfloat16 pc[TERMS];
+    split_bf16<TERMS>(x, pc);
+#pragma unroll
+    for (int q = 0; q < TERMS; ++q) out[(size_t)q * total + e] = pc[q];
   }
 }
 
@@ -174,10 +188,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
 }
 
 // -------------------------------------------------------------- GEMM ----
+struct Maps {
+  CUtensorMap a[3], b[3];
+};
+
+template <int TERMS>
 __global__ void __launch_bounds__(kThreads, 1)
-gemm_bf16x3_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
-                   const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl,
-                   int M, int N, int kchunks, double* C, long long ldc, int* status) {
+gemm_bf16x3_kernel(const __grid_constant__ Maps tm, int M, int N, int kchunks, double* C,
+                   long long ldc, int* status) {
+  constexpr int kStageBytes = stage_bytes<TERMS>();
   extern __shared__ unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages], done_bar;
   __shared__ uint32_t tmem_base_sh;
@@ -213,10 +232,11 @@ gemm_bf16x3_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_consta
     auto load_chunk = [&](int c, int s) {
       unsigned char* st = smem + (size_t)s * kStageBytes;
       mbar_expect_tx(&full_bar[s], kStageBytes);
-      tma_load_2d(st + 0 * kTileBytes, &tmAh, &full_bar[s], c * BK, m0);
-      tma_load_2d(st + 1 * kTileBytes, &tmAl, &full_bar[s], c * BK, m0);
-      tma_load_2d(st + 2 * kTileBytes, &tmBh, &full_bar[s], c * BK, n0);
-      tma_load_2d(st + 3 * kTileBytes, &tmBl, &full_bar[s], c * BK, n0);
+#pragma unroll
+      for (int q = 0; q < TERMS; ++q) {
+        tma_load_2d(st + q * kTileBytes, &tm.a[q], &full_bar[s], c * BK, m0);
+        tma_load_2d(st + (TERMS + q) * kTileBytes, &tm.b[q], &full_bar[s], c * BK, n0);
+      }
     };
     const uint32_t idesc = idesc_bf16_f32(BM, BN);
     for (int c = 0; c < kchunks && c < kStages; ++c) load_chunk(c, c);
@@ -232,13 +252,21 @@ gemm_bf16x3_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_consta
       unsigned char* st = smem + (size_t)s * kStageBytes;
 #pragma unroll
       for (int kk = 0; kk < BK / 16; ++kk) {
-        const uint64_t ah = umma_desc_k_sw128(st + 0 * kTileBytes + kk * 32);
-        const uint64_t al = umma_desc_k_sw128(st + 1 * kTileBytes + kk * 32);
-        const uint64_t bh = umma_desc_k_sw128(st + 2 * kTileBytes + kk * 32);
-        const uint64_t bl = umma_desc_k_sw128(st + 3 * kTileBytes + kk * 32);
-        umma_f16(tmem, ah, bh, idesc, (c > 0 || kk > 0) ? 1u : 0u);
-        umma_f16(tmem, ah, bl, idesc, 1u);
-        umma_f16(tmem, al, bh, idesc, 1u);
+        uint64_t ad[TERMS], bd[TERMS];
+#pragma unroll
+        for (int q = 0; q < TERMS; ++q) {
+          ad[q] = umma_desc_k_sw128(st + q * kTileBytes + kk * 32);
+          bd[q] = umma_desc_k_sw128(st + (TERMS + q) * kTileBytes + kk * 32);
+        }
+        // products of pieces (i, j) with i + j <= TERMS - 1, leading one first
+        bool first = c == 0 && kk == 0;
+#pragma unroll
+        for (int d = 0; d < TERMS; ++d)
+#pragma unroll
+          for (int i = 0; i <= d; ++i) {
+            umma_f16(tmem, ad[i], bd[d - i], idesc, first ? 0u : 1u);
+            first = false;
+          }
       }
       umma_commit(&empty_bar[s]);
       if (c + kStages < kchunks) {
@@ -327,49 +355,55 @@ bool make_map(CUtensorMap* tm, void* base, int rows, int kp) {
 
 }  // namespace mixed
 
-size_t mixed_scratch_bytes(int max_rows, int max_cols, int max_k) {
+size_t mixed_scratch_bytes(int max_rows, int max_cols, int max_k, int terms) {
   const size_t kp = (size_t)((max_k + mixed::BK - 1) / mixed::BK) * mixed::BK;
-  return 2 * ((size_t)max_rows + (size_t)max_cols) * kp * sizeof(__nv_bfloat16) + 4096;
+  return (size_t)terms * ((size_t)max_rows + (size_t)max_cols) * kp * sizeof(__nv_bfloat16) + 4096;
 }
 
-// C(M x N) -= A(M x K) * B(K x N) through the BF16x3 tensor-core path.
-// scratch must hold mixed_scratch_bytes(M, N, K) bytes (256-byte aligned).
-int launch_gemm_minus_mixed(int M, int N, int K, const double* A, long long lda, const double* B,
-                            long long ldb, double* C, long long ldc, void* scratch, int* status,
-                            cudaStream_t s) {
-  using namespace mixed;
-  if (M <= 0 || N <= 0 || K <= 0) return kOk;
-  static bool configured = false;
-  if (!configured) {
-    if (cudaFuncSetAttribute(gemm_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kSmem) != cudaSuccess)
-      return kCudaFailure;
-    configured = true;
-  }
+namespace mixed {
+
+template <int TERMS>
+int launch(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
+           double* C, long long ldc, void* scratch, int* status, cudaStream_t s) {
+  if (cudaFuncSetAttribute(gemm_bf16x3_kernel<TERMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem_bytes<TERMS>()) != cudaSuccess)
+    return kCudaFailure;
   const int kp = (K + BK - 1) / BK * BK;
-  auto* ah = reinterpret_cast<__nv_bfloat16*>(scratch);
-  auto* al = ah + (size_t)M * kp;
-  auto* bh = al + (size_t)M * kp;
-  auto* bl = bh + (size_t)N * kp;
+  auto* ap = reinterpret_cast<__nv_bfloat16*>(scratch);  // [TERMS][M][kp]
+  auto* bp = ap + (size_t)TERMS * M * kp;                 // [TERMS][N][kp]
   dp::note_launch();
-  split_a_kernel<<<dim3((M + 31) / 32, (kp + 31) / 32), dim3(32, 8), 0, s>>>(A, lda, M, K, kp, ah,
-                                                                            al);
+  split_a_kernel<TERMS><<<dim3((M + 31) / 32, (kp + 31) / 32), dim3(32, 8), 0, s>>>(A, lda, M, K,
+                                                                                  kp, ap);
   {
     const long long total = (long long)N * kp;
     long long grid = (total + 255) / 256;
     if (grid > 148 * 16) grid = 148 * 16;
     dp::note_launch();
-    split_b_kernel<<<(int)grid, 256, 0, s>>>(B, ldb, K, N, kp, bh, bl);
+    split_b_kernel<TERMS><<<(int)grid, 256, 0, s>>>(B, ldb, K, N, kp, bp);
   }
-  CUtensorMap tah, tal, tbh, tbl;
-  if (!make_map(&tah, ah, M, kp) || !make_map(&tal, al, M, kp) || !make_map(&tbh, bh, N, kp) ||
-      !make_map(&tbl, bl, N, kp))
-    return kLibraryFailure;
+  Maps tm;
+  for (int q = 0; q < TERMS; ++q)
+    if (!make_map(&tm.a[q], ap + (size_t)q * M * kp, M, kp) ||
+        !make_map(&tm.b[q], bp + (size_t)q * N * kp, N, kp))
+      return kLibraryFailure;
   dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
   dp::note_launch();
-  gemm_bf16x3_kernel<<<grid, kThreads, kSmem, s>>>(tah, tal, tbh, tbl, M, N, kp / BK, C, ldc,
-                                                   status);
+  gemm_bf16x3_kernel<TERMS><<<grid, kThreads, smem_bytes<TERMS>(), s>>>(tm, M, N, kp / BK, C, ldc,
+                                                                       status);
   return cudaGetLastError() == cudaSuccess ? kOk : kCudaFailure;
+}
+
+}  // namespace mixed
+
+// C(M x N) -= A(M x K) * B(K x N) through the BF16 split tensor-core path
+// with `terms` pieces (2: three products, 3: six products).  scratch must
+// hold mixed_scratch_bytes(M, N, K, terms) bytes (256-byte aligned).
+int launch_gemm_minus_mixed(int M, int N, int K, const double* A, long long lda, const double* B,
+                            long long ldb, double* C, long long ldc, void* scratch, int terms,
+                            int* status, cudaStream_t s) {
+  if (M <= 0 || N <= 0 || K <= 0) return kOk;
+  if (terms == 3) return mixed::launch<3>(M, N, K, A, lda, B, ldb, C, ldc, scratch, status, s);
+  return mixed::launch<2>(M, N, K, A, lda, B, ldb, C, ldc, scratch, status, s);
 }
 
 }  // namespace dp

@@ -345,11 +345,11 @@ void trsm_blocked(double* a, long long lda, int r0, int W, int c0, int nc, cudaS
 // Brings columns [c0, n_end) up to date with the eliminated steps
 // [s0, s0 + W): blocked TRSM on rows [s0, s0 + W), then
 // A(r_gemm:m, c0:n_end) -= L(r_gemm:m, s0:s0+W) * U(s0:s0+W, c0:n_end).
-// When `mixed_ws` is set the rank-W update runs on the tensor cores (BF16x3,
-// FP32 accumulation); the TRSM always runs in FP64.
+// When `mixed_ws` is set the rank-W update runs on the tensor cores (BF16
+// split into `terms` pieces, FP32 accumulation); the TRSM always runs in FP64.
 int update_columns(double* a, long long lda, int m, int s0, int W, int r_gemm, int c0, int n_end,
                    cudaStream_t st, Recorder& rec, void* mixed_ws = nullptr,
-                   int* status = nullptr) {
+                   int* status = nullptr, int terms = 2) {
   const int nc = n_end - c0;
   if (W <= 0 || nc <= 0) return kOk;
   trsm_blocked(a, lda, s0, W, c0, nc, st, rec);
@@ -361,7 +361,7 @@ int update_columns(double* a, long long lda, int m, int s0, int W, int r_gemm, i
     rec.begin(DP_KFAM_GEMM_MIXED);
     const int e = launch_gemm_minus_mixed(M, nc, W, a + idx(r_gemm, s0, lda), lda,
                                           a + idx(s0, c0, lda), lda, a + idx(r_gemm, c0, lda), lda,
-                                          mixed_ws, status, st);
+                                          mixed_ws, terms, status, st);
     rec.end(fl, by, 3);
     return e;
   }
@@ -466,11 +466,11 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       DP_CHECK_CUDA(cudaGetLastError());
       b = e;
     }
-    void* mixed_ws = o.precision == DP_PRECISION_MIXED_BF16X3 ? ws.mixed : nullptr;
+    void* mixed_ws = mixed_terms(o.precision) ? ws.mixed : nullptr;
     if (stop < 0) {
       // right of the outer block: the O(n^3) update
       if (int err = update_columns(a, lda, m, B, E - B, E, E, n, st, rec, mixed_ws,
-                                   &ws.state->status))
+                                   &ws.state->status, mixed_terms(o.precision)))
         return err;
       DP_CHECK_CUDA(cudaGetLastError());
       B = E;
@@ -481,7 +481,8 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
     const int k = stop;
     update_columns(a, lda, m, b, k - b, k, e, E, st, rec);  // rest of the outer block
     if (int err = update_columns(a, lda, m, B, k - B, k, E, n, st, rec, mixed_ws,
-                                 &ws.state->status))  // right of the outer block
+                                 &ws.state->status,
+                                 mixed_terms(o.precision)))  // right of the outer block
       return err;
     rec.begin(DP_KFAM_SEARCH);
     if (o.policy == DP_POLICY_NONZERO_COLUMN)
@@ -543,7 +544,7 @@ bool resolve_options(const dp_options* in, Options& o) {
   o.panel_rows = in->panel_rows ? in->panel_rows : kDefaultPanelRows;
   if (in->panel_kernel < 0 || in->panel_kernel > 2) return false;
   o.panel_kernel = in->panel_kernel;
-  if (in->precision != DP_PRECISION_FP64 && in->precision != DP_PRECISION_MIXED_BF16X3)
+  if (!valid_precision(in->precision))
     return false;
   o.precision = in->precision;
   return true;
@@ -570,8 +571,9 @@ int getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* 
   }
   Workspace ws;
   const int w_max = kMaxPanelWidth;
-  const size_t mixed_bytes = o.precision == DP_PRECISION_MIXED_BF16X3
-                                 ? mixed_scratch_bytes(m, n, std::max(o.nb_outer, o.nb))
+  const size_t mixed_bytes = mixed_terms(o.precision)
+                                 ? mixed_scratch_bytes(m, n, std::max(o.nb_outer, o.nb),
+                                                       mixed_terms(o.precision))
                                  : 0;
   const size_t bytes = layout_workspace(ws, nullptr, pivots, di.sms, w_max, mixed_bytes);
   char* base = nullptr;

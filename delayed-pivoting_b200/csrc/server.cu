@@ -624,7 +624,7 @@ void dp_server_options_init(dp_server_options* o) {
   if (!o) return;
   std::memset(o, 0, sizeof(*o));
   o->budget_bytes = 160ull << 30;
-  o->precision = DP_PRECISION_MIXED_BF16X3;
+  o->precision = DP_PRECISION_MIXED_BF16X6;
   o->large_workers = 6;
   o->small_max_n = DP_BATCH_MAX_N;
   o->small_max_batch = 2048;
@@ -648,7 +648,7 @@ int dp_server_create(dp_server** out, const dp_server_options* opt) {
     if (o.max_iter == 0) o.max_iter = 10;
     if (o.tol == 0.0) o.tol = 1e-14;
   }
-  if ((o.precision != DP_PRECISION_FP64 && o.precision != DP_PRECISION_MIXED_BF16X3) ||
+  if (!dp::valid_precision(o.precision) ||
       o.large_workers < 1 || o.large_workers > 64 || o.small_max_n > DP_BATCH_MAX_N ||
       o.small_max_batch < 1 || o.max_iter < 0 || !(o.tol > 0.0))
     return DP_INVALID_ARGUMENT;

@@ -321,7 +321,7 @@ int factor_create(Factor** out, int n, const double* A, int lda, int precision, 
   if (!out) return kInvalidArgument;
   *out = nullptr;
   if (n < 1 || lda < n || !A ||
-      (precision != DP_PRECISION_FP64 && precision != DP_PRECISION_MIXED_BF16X3))
+      !valid_precision(precision))
     return kInvalidArgument;
   auto* f = new (std::nothrow) Factor;
   if (!f) return kAllocationFailed;
@@ -502,7 +502,7 @@ int gesv_ir_device(int n, int nrhs, const double* A, int lda, double* B, int ldb
   res->info = -1;
   res->backward_error = INFINITY;
   if (n < 0 || nrhs < 0 || lda < std::max(1, n) || ldb < std::max(1, n) || max_iter < 0 ||
-      !(tol >= 0.0) || (precision != DP_PRECISION_FP64 && precision != DP_PRECISION_MIXED_BF16X3))
+      !(tol >= 0.0) || !valid_precision(precision))
     return kInvalidArgument;
   if (n == 0 || nrhs == 0) {
     res->info = n;

@@ -31,6 +31,7 @@ constexpr int kTB = 64;           // rows per block
 constexpr int kTT = 256;          // threads
 constexpr int kTRhs = 64;         // right-hand sides per launch
 constexpr int kTAcc = kTRhs / 4;  // accumulators per thread (4 column groups)
+constexpr int kTMaxGrid = 32;     // CTAs of one launch
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
   unsigned v;
@@ -274,8 +275,11 @@ int launch_tri(const double* T, long long ldt, int n, const double* inv, double*
                                                     smem) != cudaSuccess ||
       per_sm < 1)
     return kCudaFailure;
+  // The critical path is the chain of diagonal blocks; a CTA behind it only
+  // has to keep up with the blocks it owns, so 32 CTAs keep the latency of a
+  // full grid while leaving the other SMs to concurrent work (the server).
   const int nblk = (n + kTB - 1) / kTB;
-  const int grid = std::max(1, std::min(nblk, sms * per_sm));
+  const int grid = std::max(1, std::min(std::min(nblk, kTMaxGrid), sms * per_sm));
   void* args[] = {(void*)&T,   (void*)&ldt,  (void*)&n,     (void*)&inv,
                   (void*)&Y,   (void*)&ldy,  (void*)&nrhs,  (void*)&flags,
                   (void*)&epoch, (void*)&status};

@@ -22,7 +22,7 @@ from .api import (  # noqa: F401
     delayed_getrf_cuda_native_device, delayed_getrf_cuda_native_host,
     delayed_getrf_cuda_hybrid_device, delayed_getrf_cuda_hybrid_host,
     delayed_getrf_cuda_status_string, getrf_device_ex, getrs_device, gesv_ir_device, IRResult,
-    PRECISION_FP64, PRECISION_MIXED_BF16X3, getrf_device_noalloc,
+    PRECISION_FP64, PRECISION_MIXED_BF16X3, PRECISION_MIXED_BF16X6, getrf_device_noalloc,
     BATCH_MAX_N, BATCH_MAX_NB, BATCH_BUCKETS, BatchOptions, Batch, BatchError, batch_options,
     batch_autotune, batch_tune_save, batch_tune_load, Factor, Server, ServerOptions, Request,
     RequestResult, ServerStats, server_options, server_clock,

@@ -11,7 +11,7 @@ _LIB_DIR = _PKG / "lib"
 
 SUCCESS, INVALID_ARGUMENT, ALLOCATION_FAILED, CUDA_FAILURE, LIBRARY_FAILURE, DEVICE_TIMEOUT = range(6)
 POLICY_FULL_PIVOT, POLICY_NONZERO_COLUMN = 0, 1
-PRECISION_FP64, PRECISION_MIXED_BF16X3 = 0, 1
+PRECISION_FP64, PRECISION_MIXED_BF16X3, PRECISION_MIXED_BF16X6 = 0, 1, 2
 BATCH_MAX_N, BATCH_MAX_NB, BATCH_BUCKETS = 512, 32, 4
 
 _lib = None

@@ -33,8 +33,11 @@ enum {
 enum { DP_POLICY_FULL_PIVOT = 0, DP_POLICY_NONZERO_COLUMN = 1 };
 
 /* Arithmetic of the O(n^3) trailing update.  Pivot search, delay / fallback
- * decisions, panel and TRSM are FP64 in both modes. */
-enum { DP_PRECISION_FP64 = 0, DP_PRECISION_MIXED_BF16X3 = 1 };
+ * decisions, panel and TRSM are FP64 in every mode.  MIXED_BF16X3: BF16
+ * hi/lo split, three tensor-core products (about 2^-16 relative per update);
+ * MIXED_BF16X6: three-piece split, six products (about 2^-24, FP32-level),
+ * both with FP32 accumulation. */
+enum { DP_PRECISION_FP64 = 0, DP_PRECISION_MIXED_BF16X3 = 1, DP_PRECISION_MIXED_BF16X6 = 2 };
 
 /* Tuning and semantics knobs; dp_options_init() fills the defaults that
  * reproduce the reference exactly (threshold 0, full-pivot fallback). */
@@ -210,7 +213,7 @@ int dp_batch_tune_load(const char *path, dp_batch_options *opt);
  * and X is in d_b once the request's result has been polled. */
 typedef struct dp_server_options {
   unsigned long long budget_bytes; /* HBM admission budget (0: 160 GB) */
-  int precision;       /* DP_PRECISION_* of the blocked factorisations */
+  int precision;       /* DP_PRECISION_* of the blocked factorisations (default: MIXED_BF16X6) */
   int large_workers;   /* concurrent blocked factorisations (streams); 0: 6 */
   int small_max_n;     /* orders up to this take the batched path (<= DP_BATCH_MAX_N); 0: 512,
                           -1: none */

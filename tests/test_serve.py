@@ -21,7 +21,7 @@ TOL = 1e-14
 def test_server_options_defaults():
     o = dp.server_options()
     assert o.budget_bytes == 160 << 30
-    assert o.precision == dp.PRECISION_MIXED_BF16X3
+    assert o.precision == dp.PRECISION_MIXED_BF16X6
     assert o.small_max_n == dp.BATCH_MAX_N and o.max_iter == 10 and o.tol == TOL
 
 
@@ -166,7 +166,8 @@ SIZES = [16, 40, 64, 100, 200, 300, 511, 513, 700, 1200, 37, 450, 900]
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", [dp.PRECISION_MIXED_BF16X3, dp.PRECISION_FP64])
+@pytest.mark.parametrize("precision", [dp.PRECISION_MIXED_BF16X6, dp.PRECISION_MIXED_BF16X3,
+                                       dp.PRECISION_FP64])
 def test_server_mixed_stream(precision):
     torch = _torch()
     reqs = make_requests(torch, 3, SIZES, [1e2, 1e5, 1e10])
@@ -183,11 +184,11 @@ def test_server_mixed_stream(precision):
             assert r.path == (0 if q["n"] <= 512 else 1)
             assert r.t_submit <= r.t_admit <= r.t_start <= r.t_done
         r0 = out[q["id"]][0]
-        if q["n"] > 512 and precision == dp.PRECISION_MIXED_BF16X3:
+        if q["n"] > 512 and precision != dp.PRECISION_FP64:
             if q["kappa"] >= 1e10:
                 assert r0.precision == dp.PRECISION_FP64 and r0.refactored == 1
-            elif q["kappa"] <= 1e2:
-                assert r0.precision == dp.PRECISION_MIXED_BF16X3
+            elif q["kappa"] <= 1e2 or (precision == dp.PRECISION_MIXED_BF16X6 and q["kappa"] <= 1e5):
+                assert r0.precision == precision
     assert st.small_launches >= 1 and st.small_items > 0 and st.large_items > 0
     assert st.residents == 0 and st.bytes_in_use == 0
 
@@ -196,7 +197,7 @@ def test_server_mixed_stream(precision):
 def test_server_result_alone_equals_result_in_mix():
     torch = _torch()
     reqs = make_requests(torch, 5, SIZES, [1e3, 1e6, 1e10])
-    srv = dp.Server(precision=dp.PRECISION_MIXED_BF16X3, large_workers=4)
+    srv = dp.Server(precision=dp.PRECISION_MIXED_BF16X6, large_workers=4)
     alone = run_server(srv, reqs, together=False)
     mix = run_server(srv, reqs, together=True)
     srv.close()

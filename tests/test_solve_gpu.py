@@ -89,7 +89,8 @@ def conditioned(torch, n, kappa, seed):
 
 @pytest.mark.parametrize("kappa", [1e2, 1e4, 1e6, 1e10])
 @pytest.mark.parametrize("nrhs", [1, 64])
-def test_mixed_ir_reaches_fp64_backward_error(kappa, nrhs):
+@pytest.mark.parametrize("precision", [1, 2])  # BF16x3, BF16x6
+def test_mixed_ir_reaches_fp64_backward_error(kappa, nrhs, precision):
     import delayed_pivoting as dp
 
     torch = _torch()
@@ -99,8 +100,8 @@ def test_mixed_ir_reaches_fp64_backward_error(kappa, nrhs):
     B = A @ x_true
     dA = devcopy(A)  # column-major A
     dB = devcopy(B)
-    st, res = dp.gesv_ir_device(n, nrhs, dA, n, dB, n, precision=dp.PRECISION_MIXED_BF16X3,
-                                max_iter=10, tol=1e-14)
+    st, res = dp.gesv_ir_device(n, nrhs, dA, n, dB, n, precision=precision, max_iter=10,
+                                tol=1e-14)
     assert st == 0
     assert res.info == n
     assert res.converged == 1
@@ -115,8 +116,8 @@ def test_mixed_ir_reaches_fp64_backward_error(kappa, nrhs):
     assert ferr <= kappa * 1e-14
     if kappa >= 1e10:
         assert res.refactored == 1  # the mixed factors cannot carry kappa = 1e10
-    if kappa <= 1e2:
-        assert res.refactored == 0
+    if kappa <= 1e2 or (precision == dp.PRECISION_MIXED_BF16X6 and kappa <= 1e6):
+        assert res.refactored == 0  # BF16x6 (about 2^-24) carries kappa up to 1e6
 
 
 def test_fp64_ir_needs_at_most_few_steps():
