@@ -61,10 +61,11 @@ def parse():
     ap.add_argument("--cpu-n", type=int, default=8192, help="CPU baseline sample size")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
-                    help="trailing-update arithmetic of the factorisation (lu workload)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "mixed3"],
+                    help="trailing-update arithmetic of the lu workload: FP64, BF16x6, BF16x3")
     ap.add_argument("--workload", default="serve", choices=["serve", "lu", "batched"])
     ap.add_argument("--requests", type=int, default=1000, help="requests per serve step")
+    ap.add_argument("--max-n", type=int, default=8192, help="largest order of the serve stream")
     ap.add_argument("--load", type=float, default=0.7, help="open-loop load / capacity")
     ap.add_argument("--count", type=int, default=8192, help="matrices per batched step")
     return ap.parse_args()
@@ -256,7 +257,8 @@ def run_lu(args):
     jpiv = np.zeros(n, dtype=np.int32)
     stream = torch.cuda.current_stream(dev)
     L = dp.lib()
-    prec = dp.PRECISION_MIXED_BF16X3 if args.precision == "mixed" else dp.PRECISION_FP64
+    prec = {"fp64": dp.PRECISION_FP64, "mixed": dp.PRECISION_MIXED_BF16X6,
+            "mixed3": dp.PRECISION_MIXED_BF16X3}[args.precision]
 
     def step(timed_events=None):
         work.copy_(orig)
@@ -396,7 +398,7 @@ def run_lu(args):
 # ---------------------------------------------------------------- serve ----
 
 SERVE_METRIC = "solves/s, p99 latency: served mixed-prec vs plain FP64 LU @ bwd err<=1e-14"
-SERVE_WORKLOAD = ("served stream: n log-uniform [64, 8192] (24-order grid), A = U diag(sigma) "
+SERVE_WORKLOAD = ("served stream: n log-uniform [64, max_n = 8192] (24-order grid), A = U diag(sigma) "
                   "V^T, kappa log-uniform [1e2, 1e6] (90%) / 1e10 (10%), 1-32 RHS, 0-4 follow-up "
                   "solves, HBM budget 160 GB")
 
@@ -490,7 +492,7 @@ def run_serve(args):
     L.dp_kernel_launches.restype = ctypes_longlong()
     seed = args.seed + rank
     R = args.requests
-    reqs = sv.make_stream(R, seed)
+    reqs = sv.make_stream(R, seed, hi=args.max_n)
     warm = reqs[:max(10, R // 10)]
     pool = sv.MatrixPool(torch, [(q.n, q.kappa) for q in reqs], seed=seed)
     rhs = sv.RhsSet(torch, pool, reqs, seed=seed + 1)
@@ -629,7 +631,7 @@ def run_serve(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms_tot"] / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: seeded QR-conditioned matrices, seeded Poisson stream",
-            "config": {"workload": SERVE_WORKLOAD, "requests_per_step": R,
+            "config": {"workload": SERVE_WORKLOAD, "requests_per_step": R, "max_n": args.max_n,
                        "solves_per_step": solves_per_step, "precision": "mixed BF16x6 (six-product BF16 split, FP32 accumulation) + FP64 IR",
                        "pool_gb": pool.bytes / 1e9, "parallelism": f"replicas x{world}",
                        "l2": "inputs per step >> L2 (no flush needed)"},
@@ -660,7 +662,7 @@ def serve_reference_arm(args):
     import torch
     from delayed_pivoting import serving as sv
 
-    reqs = sv.make_stream(args.requests, args.seed)
+    reqs = sv.make_stream(args.requests, args.seed, hi=args.max_n)
     vals, cpu = [], None
     sample = reqs[:64]
 

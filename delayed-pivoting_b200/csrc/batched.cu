@@ -722,14 +722,9 @@ int launch_raw(int count, int max_n, int sms, const int* d_n, const long long* d
   for (int i = 0; i < DP_BATCH_BUCKETS; ++i) p.nb_bucket[i] = opt.nb_bucket[i];
   p.pr = panel_ld(max_n);
   const size_t smem = dynamic_smem(max_n);
-  if (cudaFuncSetAttribute(batched_getrf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem) != cudaSuccess)
-    return DP_CUDA_FAILURE;
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_getrf_kernel, kThreads,
-                                                    smem) != cudaSuccess ||
-      per_sm < 1)
-    return DP_CUDA_FAILURE;
+  if (!dp::ensure_smem((const void*)batched_getrf_kernel, smem)) return DP_CUDA_FAILURE;
+  const int per_sm = dp::occupancy_once((const void*)batched_getrf_kernel, kThreads, smem);
+  if (per_sm < 1) return DP_CUDA_FAILURE;
   const int grid = std::max(1, std::min(count, sms * per_sm));
   if (cudaMemsetAsync(d_queue, 0, sizeof(int), st) != cudaSuccess) return DP_CUDA_FAILURE;
   dp::note_launch();

@@ -5,6 +5,9 @@
 
 #include <cstddef>
 #include <atomic>
+#include <map>
+#include <mutex>
+#include <utility>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -15,6 +18,57 @@ namespace dp {
 inline std::atomic<long long> g_kernel_launches{0};
 inline void note_launch(long long k = 1) {
   g_kernel_launches.fetch_add(k, std::memory_order_relaxed);
+}
+
+// Raises the dynamic shared-memory limit of kernel `func` on the current
+// device to at least `bytes`, calling the runtime only when the limit grows
+// (the call costs milliseconds for large limits, far more than a launch).
+inline bool ensure_smem(const void* func, size_t bytes) {
+  static std::mutex m;
+  static std::map<std::pair<const void*, int>, size_t> done;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  std::lock_guard<std::mutex> lock(m);
+  size_t& have = done[{func, dev}];
+  if (have >= bytes) return true;
+  if (cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
+      cudaSuccess)
+    return false;
+  have = bytes;
+  return true;
+}
+
+// Resident CTAs per SM of `func` at `threads` x `smem` on the current device,
+// computed once per (kernel, device, smem); 0 on error.
+inline int occupancy_once(const void* func, int threads, size_t smem) {
+  static std::mutex m;
+  static std::map<std::pair<std::pair<const void*, int>, size_t>, int> memo;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  std::lock_guard<std::mutex> lock(m);
+  auto key = std::make_pair(std::make_pair(func, dev), smem);
+  auto it = memo.find(key);
+  if (it != memo.end()) return it->second;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, threads, smem) != cudaSuccess)
+    per_sm = 0;
+  memo[key] = per_sm;
+  return per_sm;
+}
+
+// Multiprocessors of the current device (memoised per device).
+inline int sm_count() {
+  static std::mutex m;
+  static std::map<int, int> memo;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  std::lock_guard<std::mutex> lock(m);
+  auto it = memo.find(dev);
+  if (it != memo.end()) return it->second;
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 0;
+  memo[dev] = sms;
+  return sms;
 }
 
 // Status codes shared by kernels and host (values of the C ABI).

@@ -190,12 +190,7 @@ dgemm_minus_kernel(int M, int N, int K, const double* __restrict__ A, long long 
 template <class C>
 void launch(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
             double* Cm, long long ldc, cudaStream_t s) {
-  static bool configured = false;
-  if (!configured) {
-    cudaFuncSetAttribute(dgemm_minus_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)C::SMEM);
-    configured = true;
-  }
+  dp::ensure_smem((const void*)dgemm_minus_kernel<C>, C::SMEM);
   dim3 grid((M + C::BM - 1) / C::BM, (N + C::BN - 1) / C::BN);
   dp::note_launch();
   dgemm_minus_kernel<C><<<grid, C::THREADS, C::SMEM, s>>>(M, N, K, A, lda, B, ldb, Cm, ldc);

@@ -365,8 +365,7 @@ namespace mixed {
 template <int TERMS>
 int launch(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
            double* C, long long ldc, void* scratch, int* status, cudaStream_t s) {
-  if (cudaFuncSetAttribute(gemm_bf16x3_kernel<TERMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem_bytes<TERMS>()) != cudaSuccess)
+  if (!ensure_smem((const void*)gemm_bf16x3_kernel<TERMS>, smem_bytes<TERMS>()))
     return kCudaFailure;
   const int kp = (K + BK - 1) / BK * BK;
   auto* ap = reinterpret_cast<__nv_bfloat16*>(scratch);  // [TERMS][M][kp]

@@ -246,9 +246,7 @@ int launch_orders(const int* ns, const long long* rec, const int* ipiv, const in
 int launch_solve(const SolveItem* items, int count, int max_n, cudaStream_t st) {
   if (count <= 0) return kOk;
   const size_t sm = solve_smem(max_n);
-  if (cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
-      cudaSuccess)
-    return kCudaFailure;
+  if (!ensure_smem((const void*)solve_kernel, sm)) return kCudaFailure;
   dp::note_launch();
   solve_kernel<<<count, kThreads, sm, st>>>(items);
   return cudaGetLastError() == cudaSuccess ? kOk : kCudaFailure;
@@ -257,9 +255,7 @@ int launch_solve(const SolveItem* items, int count, int max_n, cudaStream_t st) 
 int launch_residual(const ResidualItem* items, double* err, int count, int max_n, cudaStream_t st) {
   if (count <= 0) return kOk;
   const size_t sm = solve_smem(max_n);
-  if (cudaFuncSetAttribute(residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)sm) != cudaSuccess)
-    return kCudaFailure;
+  if (!ensure_smem((const void*)residual_kernel, sm)) return kCudaFailure;
   dp::note_launch();
   residual_kernel<<<count, kThreads, sm, st>>>(items, err);
   return cudaGetLastError() == cudaSuccess ? kOk : kCudaFailure;

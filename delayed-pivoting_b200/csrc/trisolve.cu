@@ -265,16 +265,10 @@ int launch_tri(const double* T, long long ldt, int n, const double* inv, double*
                long long ldy, int nrhs, unsigned* flags, unsigned epoch, int* status,
                cudaStream_t st) {
   const size_t smem = sizeof(double) * (2 * kTB * kTRhs + 3 * kTB * kTB);
-  if (cudaFuncSetAttribute(tri_solve_kernel<kUpper, MACC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem) != cudaSuccess)
-    return kCudaFailure;
-  int dev = 0, sms = 0, per_sm = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tri_solve_kernel<kUpper, MACC>, kTT,
-                                                    smem) != cudaSuccess ||
-      per_sm < 1)
-    return kCudaFailure;
+  if (!ensure_smem((const void*)tri_solve_kernel<kUpper, MACC>, smem)) return kCudaFailure;
+  const int sms = sm_count();
+  const int per_sm = occupancy_once((const void*)tri_solve_kernel<kUpper, MACC>, kTT, smem);
+  if (sms < 1 || per_sm < 1) return kCudaFailure;
   // The critical path is the chain of diagonal blocks; a CTA behind it only
   // has to keep up with the blocks it owns, so 32 CTAs keep the latency of a
   // full grid while leaving the other SMs to concurrent work (the server).

@@ -167,15 +167,9 @@ trsm_upper_kernel(const double* __restrict__ U, long long ldu, double* B, long l
   stage_out(B, ldb, w, ncols, Bt);
 }
 
-bool g_configured = false;
-
 void configure() {
-  if (g_configured) return;
-  cudaFuncSetAttribute(trsm_lower_unit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)kTrsmSmem);
-  cudaFuncSetAttribute(trsm_upper_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)kTrsmSmem);
-  g_configured = true;
+  ensure_smem((const void*)trsm_lower_unit_kernel, kTrsmSmem);
+  ensure_smem((const void*)trsm_upper_kernel, kTrsmSmem);
 }
 
 }  // namespace
