@@ -45,7 +45,8 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "delayed-pivoting_b200"))
 
-METRIC = "plain FP64 delayed_getrf GFLOP/s (2/3 n^3), n=16384, 0.1% tiny + 0.02% zero columns"
+def lu_metric(n):
+    return f"plain FP64 delayed_getrf GFLOP/s (2/3 n^3), n={n}, 0.1% tiny + 0.02% zero columns"
 UNIT = "GFLOP/s"
 
 
@@ -204,7 +205,7 @@ def run_reference_arm(args):
     tot = sum(times)
     value = flops(n) * len(times) / tot / 1e9
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": lu_metric(args.n), "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / len(times) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: N(0,1) MT19937-64 seeded, planted tiny and zero columns",
@@ -370,13 +371,15 @@ def run_lu(args):
             if stats["bytes"][i]:
                 kern[nm]["gbs"] = stats["bytes"][i] / (stats["ms"][i] * 1e-3) / 1e9
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "metric": lu_metric(n), "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic: N(0,1) MT19937-64 seeded per rank, 16 tiny (x1e-18) + 3 zero columns",
+            "data": f"synthetic: N(0,1) MT19937-64 seeded per rank, {w['n_tiny']} tiny (x1e-18) + "
+                    f"{w['n_zero']} zero columns",
             "config": {"workload": f"delayed_getrf plain FP64 n={n} (single matrix)", "n": n,
                        "nb": args.nb, "parallelism": f"replicas x{world}",
-                       "l2": "input 2 GiB > L2 (no flush needed)", "info": info},
+                       "l2": f"input {8 * n * n / 2**30:.2f} GiB " + (
+                           "> L2 (no flush needed)" if 8 * n * n > 126e6 else "<= L2"), "info": info},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -704,7 +707,8 @@ def serve_reference_arm(args):
 
 # -------------------------------------------------------------- batched ----
 
-BATCH_METRIC = "batched delayed_getrf matrices/s (8192 matrices, n log-uniform [32, 512])"
+def batch_metric(count):
+    return f"batched delayed_getrf matrices/s ({count} matrices, n log-uniform [32, 512])"
 
 
 def run_batched(args):
@@ -789,7 +793,7 @@ def run_batched(args):
     if rank == 0 and not args.no_cpu_baseline:
         cpu = _cpu_batched_baseline(ns, nz, seed)
     if rank == 0:
-        line = {"metric": BATCH_METRIC, "value": value, "unit": "matrices/s", "n_gpus": world,
+        line = {"metric": batch_metric(count), "value": value, "unit": "matrices/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic: N(0,1) MT19937-64 per matrix, 0-2 zero columns (p = 0.3)",
@@ -846,7 +850,7 @@ def batched_reference_arm(args):
             vals.append(cpu["value"])
             t_all += time.perf_counter() - t0
     value = float(np.mean(vals))
-    print(json.dumps({"impl": "reference", "metric": BATCH_METRIC, "value": value,
+    print(json.dumps({"impl": "reference", "metric": batch_metric(args.count), "value": value,
                       "unit": "matrices/s", "n_gpus": args.gpus, "steps": args.steps,
                       "warmup": args.warmup, "ms_per_step": t_all / max(args.steps, 1) * 1e3,
                       "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

@@ -883,6 +883,7 @@ int dp_batch_getrf_graph(dp_batch* bp, double* d_base, int* d_ipiv, int* d_jpiv,
     }
     std::copy(args, args + 4, bp->g_args);
   }
+  dp::note_launch();  // the graph holds one kernel (after the queue reset)
   return cudaGraphLaunch(bp->exec, (cudaStream_t)stream) == cudaSuccess ? DP_SUCCESS
                                                                         : DP_CUDA_FAILURE;
 }
