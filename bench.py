@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=16384)
     ap.add_argument("--nb", type=int, default=64)
+    ap.add_argument("--lookahead", type=int, default=0, choices=[0, 1, 2],
+                    help="LU trailing-update schedule: 0 automatic, 1 two streams, 2 one stream")
     ap.add_argument("--seed", type=int, default=16384)
     ap.add_argument("--cpu-n", type=int, default=8192, help="CPU baseline sample size")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -267,7 +269,7 @@ def run_lu(args):
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         st, info = dp.getrf_device_ex(n, n, work, n, ipiv, jpiv, stream=stream, nb=args.nb,
-                                      precision=prec)
+                                      precision=prec, lookahead=args.lookahead)
         e1.record(stream)
         if st != 0:
             raise RuntimeError(dp.delayed_getrf_cuda_status_string(st))
@@ -385,6 +387,7 @@ def run_lu(args):
             "e2e": e2e,
             "gpu_launches": int(round(launches_per_step * args.steps)),
             "gpu_launches_per_step": launches_per_step,
+            "step_ms": [round(e0.elapsed_time(e1), 3) for e0, e1, _ in events],
             "clocks": clk.summary(),
             "kernels": kern,
             "fp64_peak_tflops": fp64,

@@ -45,6 +45,26 @@ void launch_laswp(double* a, long long lda, int begin, int nblock, const int* sw
                   const int* swap_extra, const State* state, int c0, int c1, int c2, int c3,
                   cudaStream_t s);
 
+// Swap lists of up to kSwapSeqLists consecutive panels (kSwapSeqEntries
+// entries in all) applied in order by one launch of laswp_seq_kernel.
+constexpr int kSwapSeqLists = 64;
+constexpr int kSwapSeqEntries = 2048;
+struct SwapSeq {
+  int lists;
+  int base;  // first row of the first panel
+  int width[kSwapSeqLists];
+  int nextra[kSwapSeqLists];
+};
+
+// Applies the swap lists of `lists` consecutive panels starting at row
+// `base` (panel p of width widths[p], its block part at blk[begin_p - base],
+// its nextra[p] extra pairs at ext[2 (begin_p - base)]) to the columns
+// [c0, c1) and [c2, c3), in panel order.  Returns the number of launches, or
+// -1 when a list exceeds a panel's size.
+int launch_laswp_seq(double* a, long long lda, const int* blk, const int* ext, int base,
+                     const int* widths, const int* nextra, int lists, int c0, int c1, int c2,
+                     int c3, cudaStream_t s);
+
 // B(w x nc) <- L^{-1} B, L unit lower (w x w) at a(r0, r0), B at a(r0, c0);
 // w <= trsm_max_width().
 int trsm_max_width();

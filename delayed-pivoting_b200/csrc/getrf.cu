@@ -14,6 +14,10 @@
 //                   (TRSM + GEMM of width k - begin) -> full or column
 //                   fallback search -> delay (info = k) or swap row/column and
 //                   restart the panel at k with the pivot in place.
+// With look-ahead (the default for more than one outer block) the trailing
+// update of a finished outer block is split: the next block's columns are
+// updated on a high-priority stream that then factors that block's panels,
+// while the rest of the update runs on a low-priority stream behind them.
 #include <algorithm>
 #include <chrono>
 #include <cstdlib>
@@ -100,6 +104,7 @@ struct Options {
   double threshold = 0.0;
   int policy = DP_POLICY_FULL_PIVOT;
   int panel_rows = kDefaultPanelRows;
+  int lookahead = 0;  // 0 automatic (more than one outer block), 1 on, 2 off
 };
 
 struct Workspace {
@@ -115,6 +120,14 @@ struct Workspace {
   int* swap_extra = nullptr;
   Cand* cands = nullptr;
   void* mixed = nullptr;  // BF16 operand scratch of the tensor-core update (mixed precision)
+  // Look-ahead: swap lists of the panels of an outer block, kept until the
+  // block completes (two buffers, alternating between consecutive blocks;
+  // panel [b, e) of block [B, E) at defer_blk + (b - B), defer_ext + 2 (b - B)),
+  // and the error word of the kernels on the trailing-update stream.
+  int* defer_blk = nullptr;
+  int* defer_ext = nullptr;
+  int defer_cap = 0;
+  int* aux_status = nullptr;
   int max_ctas = 0;
   int w_max = 0;
 };
@@ -123,7 +136,7 @@ size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 // Lays the workspace out from `base` (nullptr: only computes the size).
 size_t layout_workspace(Workspace& ws, char* base, int pivots, int max_ctas, int w_max,
-                        size_t mixed_bytes) {
+                        size_t mixed_bytes, int defer_cap = 0) {
   size_t off = 0;
   auto take = [&](size_t bytes) {
     const size_t at = off;
@@ -142,6 +155,12 @@ size_t layout_workspace(Workspace& ws, char* base, int pivots, int max_ctas, int
   ws.swap_block = reinterpret_cast<int*>(take(sizeof(int) * (size_t)w_max));
   ws.swap_extra = reinterpret_cast<int*>(take(sizeof(int) * 2 * (size_t)w_max));
   ws.cands = reinterpret_cast<Cand*>(take(sizeof(Cand) * kMaxSearchBlocks));
+  ws.defer_cap = defer_cap;
+  if (defer_cap > 0) {
+    ws.defer_blk = reinterpret_cast<int*>(take(sizeof(int) * 2 * (size_t)defer_cap));
+    ws.defer_ext = reinterpret_cast<int*>(take(sizeof(int) * 4 * (size_t)defer_cap));
+    ws.aux_status = reinterpret_cast<int*>(take(sizeof(int)));
+  }
   ws.mixed = mixed_bytes ? reinterpret_cast<void*>(take(mixed_bytes)) : nullptr;
   ws.base = base;
   ws.bytes = off;
@@ -254,6 +273,17 @@ void event_put(cudaEvent_t e) {
   g_event_pool.push_back(e);
 }
 
+// Timeline dump (environment variable DP_TIMELINE=<file>, with dp_stats
+// enabled): every recorded launch group is appended to the file as
+// "call lane family start_ms end_ms launches", times relative to an event
+// recorded on the caller's stream when the call starts; lane 0 is the
+// critical-path stream, lane 1 the trailing-update stream.
+const char* timeline_path() {
+  static const char* p = std::getenv("DP_TIMELINE");
+  return p && p[0] ? p : nullptr;
+}
+long long g_timeline_calls = 0;
+
 struct Recorder {
   struct Mark {
     int fam;
@@ -265,6 +295,8 @@ struct Recorder {
   cudaStream_t st = nullptr;
   std::vector<Mark> marks;
   int cur = -1;
+  int lane = 0;
+  cudaEvent_t base = nullptr;  // timeline origin (nullptr: no timeline)
   explicit Recorder(cudaStream_t s) : st(s) {
     std::lock_guard<std::mutex> lock(g_stats_mutex);
     on = g_stats_on;
@@ -291,7 +323,13 @@ struct Recorder {
   void flush(bool ok) {
     if (!on) return;
     std::lock_guard<std::mutex> lock(g_stats_mutex);
+    FILE* tl = ok && base && timeline_path() ? std::fopen(timeline_path(), "a") : nullptr;
     for (Mark& mk : marks) {
+      float t0 = 0.f, t1 = 0.f;
+      if (tl && mk.e1 && cudaEventElapsedTime(&t0, base, mk.e0) == cudaSuccess &&
+          cudaEventElapsedTime(&t1, base, mk.e1) == cudaSuccess)
+        std::fprintf(tl, "%lld %d %d %.4f %.4f %d\n", g_timeline_calls, lane, mk.fam, t0, t1,
+                     mk.launches);
       float ms = 0.f;
       if (ok && mk.e1 && cudaEventElapsedTime(&ms, mk.e0, mk.e1) == cudaSuccess) {
         g_stats.ms[mk.fam] += ms;
@@ -303,6 +341,7 @@ struct Recorder {
       event_put(mk.e1);
     }
     if (ok) g_stats.calls += 1;
+    if (tl) std::fclose(tl);
     marks.clear();
   }
 };
@@ -372,9 +411,80 @@ int update_columns(double* a, long long lda, int m, int s0, int W, int r_gemm, i
   return kOk;
 }
 
+// Streams and events of the look-ahead schedule, created once per host thread
+// and device: `panel` (highest priority) carries the critical path - panels,
+// in-block updates, the next outer block's columns - and `trail` (lowest
+// priority) the bulk of each trailing update, so that panel CTAs are placed
+// ahead of waiting GEMM tiles.
+struct Lanes {
+  cudaStream_t panel = nullptr, trail = nullptr;
+  cudaEvent_t fork = nullptr, block = nullptr, next = nullptr, join = nullptr;
+  bool ready = false;
+  bool init() {
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&panel, cudaStreamNonBlocking, greatest) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&trail, cudaStreamNonBlocking, least) != cudaSuccess)
+      return false;
+    for (cudaEvent_t* e : {&fork, &block, &next, &join})
+      if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) return false;
+    ready = true;
+    return true;
+  }
+  ~Lanes() {
+    for (cudaEvent_t e : {fork, block, next, join})
+      if (e) cudaEventDestroy(e);
+    if (panel) cudaStreamDestroy(panel);
+    if (trail) cudaStreamDestroy(trail);
+  }
+};
+thread_local Lanes g_lanes[64];
+
+Lanes* lanes_for_device() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  Lanes& l = g_lanes[dev];
+  if (!l.ready && !l.init()) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return &l;
+}
+
+// Where factorize issues its work: `s1` always; `s2` (look-ahead) takes the
+// trailing updates right of the next outer block, ordered against `s1` by
+// the events `block` (s1 -> s2: an outer block and the next block's columns
+// are done) and `next` (s2 -> s1: the columns of the block after next have
+// this block's update).
+struct Schedule {
+  cudaStream_t s1 = nullptr, s2 = nullptr;
+  Recorder* r1 = nullptr;
+  Recorder* r2 = nullptr;
+  cudaEvent_t block = nullptr, next = nullptr;
+};
+
+// Applies the deferred swap lists of the panels [B, B + sum widths) of an
+// outer block to the columns [c0, c1) and [c2, c3).
+int apply_deferred(double* a, long long lda, const Workspace& ws, const int* blk,
+                   const int* ext, int B, const std::vector<int>& widths,
+                   const std::vector<int>& extras, int c0, int c1, int c2, int c3,
+                   cudaStream_t st, Recorder& rec) {
+  const long long cols = (long long)std::max(0, c1 - c0) + std::max(0, c3 - c2);
+  if (widths.empty() || cols <= 0) return kOk;
+  double moved = 0.0;
+  for (size_t i = 0; i < widths.size(); ++i) moved += (double)widths[i] + extras[i];
+  rec.begin(DP_KFAM_LASWP);
+  const int launches = launch_laswp_seq(a, lda, blk, ext, B, widths.data(), extras.data(),
+                                        (int)widths.size(), c0, c1, c2, c3, st);
+  rec.end(0.0, 16.0 * moved * (double)cols, std::max(launches, 0));
+  if (launches < 0) return kInvalidArgument;
+  (void)ws;
+  return kOk;
+}
+
 // Two-level blocked delayed LU.  An outer block [B, E) of width NB is
 // factored as a sequence of inner panels [b, e) of width nb (the panel
-// kernel); after each inner panel its row swaps are applied to every column
+// kernel); after each inner panel its row swaps are applied to the columns
 // outside it and the rest of the outer block [e, E) is updated (rank nb);
 // the columns right of the outer block receive one rank-NB update when the
 // block completes.  When a panel stops at step k (no acceptable column
@@ -385,20 +495,42 @@ int update_columns(double* a, long long lda, int m, int s0, int W, int r_gemm, i
 // restarts a new outer block at k with that pivot positioned
 // (delayed_dgetrf.cpp:188-218).  Block sizes only change rounding, never the
 // pivot decisions.
+//
+// Look-ahead (sc.s2 set): inside an outer block a panel's swaps reach only
+// the block's own columns; the swaps outside the block are kept (per panel)
+// and applied when the block completes.  Then, on s1: the block's swaps and
+// update on the next block's columns [E, NE); on s2, behind them: the swaps
+// on [0, B) and [NE, n), the update of the block after next [NE, NNE)
+// (event `next`), and the update of [NNE, n).  The next block's panels run
+// on s1 while s2 works; before touching [NE, NNE) s1 waits for `next`.  A
+// stop drains s2 and applies the block's kept swaps everywhere, which
+// restores the state of the unscheduled order before the materialize /
+// search logic runs.  Every element receives the same operations in the
+// same order either way, so the schedule changes no result.
 int factorize(int m, int n, double* a, long long lda, const Options& o, Workspace& ws,
-              const DeviceInfo& di, cudaStream_t st, int& info, Recorder& rec) {
+              const DeviceInfo& di, const Schedule& sc, int& info) {
+  cudaStream_t st = sc.s1;
+  Recorder& rec = *sc.r1;
+  const bool la = sc.s2 != nullptr;
   const int pivots = std::min(m, n);
   rec.begin(DP_KFAM_OTHER);
   launch_identity_records(ws.d_ipiv, ws.d_jpiv, pivots, st);
   rec.end(0.0, 8.0 * pivots, 1);
   DP_CHECK_CUDA(cudaGetLastError());
   info = pivots;
-  int B = 0, parity = 0;
-  bool positioned = false;
+  int B = 0, parity = 0, half = 0;
+  bool positioned = false, pending = false;
   State hs;
   const int NB = std::max(o.nb_outer, o.nb);
+  const int terms = mixed_terms(o.precision);
+  void* mixed_ws = terms ? ws.mixed : nullptr;
+  std::vector<int> widths, extras;  // the current block's panels (look-ahead)
   while (B < pivots) {
     const int E = std::min(pivots, B + NB);
+    int* blk = la ? ws.defer_blk + (size_t)half * ws.defer_cap : ws.swap_block;
+    int* ext = la ? ws.defer_ext + (size_t)2 * half * ws.defer_cap : ws.swap_extra;
+    widths.clear();
+    extras.clear();
     int b = B, e = B, stop = -1;
     while (b < E) {
       int w = std::min(std::min(o.nb, ws.w_max), E - b);
@@ -406,6 +538,11 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       const bool use_cluster = o.panel_kernel != 2 && plan_cluster(m - b, w, di, G, R);
       if (!use_cluster && !plan_panel(m - b, w, o.panel_rows, di, G, R)) return kInvalidArgument;
       e = b + w;
+      if (la && !use_cluster) {
+        // the cooperative grid needs all its CTAs resident: s2 finishes first
+        DP_CHECK_CUDA(cudaEventRecord(sc.next, sc.s2));
+        DP_CHECK_CUDA(cudaStreamWaitEvent(st, sc.next, 0));
+      }
 
       PanelParams pp;
       pp.a = a;
@@ -424,8 +561,8 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       pp.slots = ws.slots;
       pp.xdata = ws.xdata;
       pp.rowk = ws.rowk;
-      pp.swap_block = ws.swap_block;
-      pp.swap_extra = ws.swap_extra;
+      pp.swap_block = la ? blk + (b - B) : ws.swap_block;
+      pp.swap_extra = la ? ext + 2 * (size_t)(b - B) : ws.swap_extra;
       rec.begin(DP_KFAM_PANEL);
       if (use_cluster) {
         cudaLaunchConfig_t cfg = {};
@@ -455,9 +592,17 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       if (int err = read_state(hs, ws, st)) return err;
       if (hs.status != kOk) return hs.status;
 
+      const double moved = (double)(hs.block_changed + hs.swap_count);
       rec.begin(DP_KFAM_LASWP);
-      launch_laswp(a, lda, b, w, ws.swap_block, ws.swap_extra, ws.state, 0, b, e, n, st);
-      rec.end(0.0, 16.0 * (double)(hs.block_changed + hs.swap_count) * (double)(n - w), 1);
+      if (la) {
+        launch_laswp(a, lda, b, w, pp.swap_block, pp.swap_extra, ws.state, B, b, e, E, st);
+        rec.end(0.0, 16.0 * moved * (double)(E - B - w), 1);
+        widths.push_back(w);
+        extras.push_back(hs.swap_count);
+      } else {
+        launch_laswp(a, lda, b, w, ws.swap_block, ws.swap_extra, ws.state, 0, b, e, n, st);
+        rec.end(0.0, 16.0 * moved * (double)(n - w), 1);
+      }
       if (hs.stop_k >= 0) {
         stop = hs.stop_k;
         break;
@@ -466,23 +611,61 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       DP_CHECK_CUDA(cudaGetLastError());
       b = e;
     }
-    void* mixed_ws = mixed_terms(o.precision) ? ws.mixed : nullptr;
-    if (stop < 0) {
+    if (stop < 0 && !la) {
       // right of the outer block: the O(n^3) update
       if (int err = update_columns(a, lda, m, B, E - B, E, E, n, st, rec, mixed_ws,
-                                   &ws.state->status, mixed_terms(o.precision)))
+                                   &ws.state->status, terms))
         return err;
       DP_CHECK_CUDA(cudaGetLastError());
+      B = E;
+      continue;
+    }
+    if (stop < 0) {
+      const int NE = std::min(pivots, E + NB);   // the next outer block
+      const int NNE = std::min(pivots, NE + NB);  // the block after next
+      // s1: the next block's columns, then on to its panels
+      if (pending) DP_CHECK_CUDA(cudaStreamWaitEvent(st, sc.next, 0));
+      if (int err = apply_deferred(a, lda, ws, blk, ext, B, widths, extras, E, NE, NE, NE, st,
+                                   rec))
+        return err;
+      update_columns(a, lda, m, B, E - B, E, E, NE, st, rec);
+      DP_CHECK_CUDA(cudaGetLastError());
+      DP_CHECK_CUDA(cudaEventRecord(sc.block, st));
+      // s2: everything else, behind the block
+      DP_CHECK_CUDA(cudaStreamWaitEvent(sc.s2, sc.block, 0));
+      if (int err = apply_deferred(a, lda, ws, blk, ext, B, widths, extras, 0, B, NE, n, sc.s2,
+                                   *sc.r2))
+        return err;
+      pending = false;
+      if (NNE > NE) {
+        if (int err = update_columns(a, lda, m, B, E - B, E, NE, NNE, sc.s2, *sc.r2, mixed_ws,
+                                     ws.aux_status, terms))
+          return err;
+        DP_CHECK_CUDA(cudaEventRecord(sc.next, sc.s2));
+        pending = true;
+      }
+      if (int err = update_columns(a, lda, m, B, E - B, E, std::max(NE, NNE), n, sc.s2, *sc.r2,
+                                   mixed_ws, ws.aux_status, terms))
+        return err;
+      DP_CHECK_CUDA(cudaGetLastError());
+      half ^= 1;
       B = E;
       continue;
     }
 
     // Stopped at k inside panel [b, e): materialize, then search.
     const int k = stop;
+    if (la) {
+      // s2 drains; the block's kept swaps reach every column outside it
+      DP_CHECK_CUDA(cudaEventRecord(sc.next, sc.s2));
+      DP_CHECK_CUDA(cudaStreamWaitEvent(st, sc.next, 0));
+      pending = false;
+      if (int err = apply_deferred(a, lda, ws, blk, ext, B, widths, extras, 0, B, E, n, st, rec))
+        return err;
+    }
     update_columns(a, lda, m, b, k - b, k, e, E, st, rec);  // rest of the outer block
     if (int err = update_columns(a, lda, m, B, k - B, k, E, n, st, rec, mixed_ws,
-                                 &ws.state->status,
-                                 mixed_terms(o.precision)))  // right of the outer block
+                                 &ws.state->status, terms))  // right of the outer block
       return err;
     rec.begin(DP_KFAM_SEARCH);
     if (o.policy == DP_POLICY_NONZERO_COLUMN)
@@ -547,6 +730,8 @@ bool resolve_options(const dp_options* in, Options& o) {
   if (!valid_precision(in->precision))
     return false;
   o.precision = in->precision;
+  if (in->lookahead < 0 || in->lookahead > 2) return false;
+  o.lookahead = in->lookahead;
   return true;
 }
 
@@ -575,22 +760,59 @@ int getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* 
                                  ? mixed_scratch_bytes(m, n, std::max(o.nb_outer, o.nb),
                                                        mixed_terms(o.precision))
                                  : 0;
-  const size_t bytes = layout_workspace(ws, nullptr, pivots, di.sms, w_max, mixed_bytes);
+  const int NB = std::max(o.nb_outer, o.nb);
+  Lanes* lanes = nullptr;
+  if (o.lookahead == 1 || (o.lookahead == 0 && pivots > NB)) lanes = lanes_for_device();
+  const int defer_cap = lanes ? std::min(NB, pivots) : 0;
+  const size_t bytes =
+      layout_workspace(ws, nullptr, pivots, di.sms, w_max, mixed_bytes, defer_cap);
   char* base = nullptr;
   if (cudaMallocAsync(reinterpret_cast<void**>(&base), bytes, st) != cudaSuccess) {
     cudaGetLastError();
     *info = -1;
     return kAllocationFailed;
   }
-  layout_workspace(ws, base, pivots, di.sms, w_max, mixed_bytes);
+  layout_workspace(ws, base, pivots, di.sms, w_max, mixed_bytes, defer_cap);
   int status = kOk;
   // the BF16 scratch is fully written before use; clear only the rest
   if (cudaMemsetAsync(base, 0, bytes - mixed_bytes, st) != cudaSuccess) status = kCudaFailure;
   int inf = pivots;
   HostTrace trace;
   g_trace = &trace;
-  Recorder rec(st);
-  if (status == kOk) status = factorize(m, n, d_a, lda, o, ws, di, st, inf, rec);
+  Schedule sc;
+  sc.s1 = lanes ? lanes->panel : st;
+  sc.s2 = lanes ? lanes->trail : nullptr;
+  Recorder rec(sc.s1), rec2(lanes ? lanes->trail : st);
+  sc.r1 = &rec;
+  sc.r2 = &rec2;
+  rec2.lane = 1;
+  cudaEvent_t tl_base = nullptr;
+  if (rec.on && timeline_path()) {
+    tl_base = event_get();
+    cudaEventRecord(tl_base, st);
+    rec.base = rec2.base = tl_base;
+  }
+  if (lanes) {
+    sc.block = lanes->block;
+    sc.next = lanes->next;
+    if (status == kOk && (cudaEventRecord(lanes->fork, st) != cudaSuccess ||
+                          cudaStreamWaitEvent(lanes->panel, lanes->fork, 0) != cudaSuccess ||
+                          cudaStreamWaitEvent(lanes->trail, lanes->fork, 0) != cudaSuccess))
+      status = kCudaFailure;
+  }
+  if (status == kOk) status = factorize(m, n, d_a, lda, o, ws, di, sc, inf);
+  int aux = kOk;
+  if (lanes) {
+    // st waits for both lanes whatever happened, before the workspace is freed
+    cudaEventRecord(lanes->join, lanes->panel);
+    cudaStreamWaitEvent(st, lanes->join, 0);
+    cudaEventRecord(lanes->join, lanes->trail);
+    cudaStreamWaitEvent(st, lanes->join, 0);
+    if (status == kOk &&
+        cudaMemcpyAsync(&aux, ws.aux_status, sizeof(int), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess)
+      status = kCudaFailure;
+  }
   if (status == kOk) {
     if (cudaMemcpyAsync(ipiv, ws.d_ipiv, sizeof(int) * pivots, cudaMemcpyDeviceToHost, st) !=
             cudaSuccess ||
@@ -600,7 +822,14 @@ int getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* 
   }
   cudaFreeAsync(base, st);
   if (cudaStreamSynchronize(st) != cudaSuccess && status == kOk) status = kCudaFailure;
+  if (status == kOk && aux != kOk) status = aux;
   rec.flush(status == kOk);
+  rec2.flush(status == kOk);
+  if (tl_base) {
+    std::lock_guard<std::mutex> lock(g_stats_mutex);
+    ++g_timeline_calls;
+    event_put(tl_base);
+  }
   g_trace = nullptr;
   if (status != kOk) {
     cudaGetLastError();
@@ -726,7 +955,11 @@ int getrf_device_noalloc(int m, int n, double* d_a, int lda, int* ipiv, int* jpi
   int inf = pivots;
   Recorder rec(st);
   rec.on = false;  // no timing events on this path
-  if (status == kOk) status = factorize(m, n, d_a, lda, o, ws, di, st, inf, rec);
+  Schedule sc;  // one stream: no look-ahead
+  sc.s1 = st;
+  sc.r1 = &rec;
+  sc.r2 = &rec;
+  if (status == kOk) status = factorize(m, n, d_a, lda, o, ws, di, sc, inf);
   if (status == kOk) {
     if (cudaMemcpyAsync(ipiv, ws.d_ipiv, sizeof(int) * pivots, cudaMemcpyDeviceToHost, st) !=
             cudaSuccess ||

@@ -84,6 +84,88 @@ laswp_kernel(double* a, long long lda, int begin, int nblock, const int* swap_bl
   }
 }
 
+// The swap lists of consecutive panels applied in panel order: list p covers
+// the panel starting at row begin_p = q.base + width[0] + ... + width[p-1],
+// its block part at blk[begin_p - q.base] and its extra pairs at
+// ext[2 (begin_p - q.base)].  Each CTA compacts every list into shared memory
+// (list p at [s_lb[p], s_lb[p+1])); each warp then applies the lists to one
+// column in turn, gathering a list's sources before scattering it, so the
+// result equals launching laswp_kernel once per panel.
+__global__ void __launch_bounds__(kLaswpThreads)
+laswp_seq_kernel(double* a, long long lda, const int* blk, const int* ext, SwapSeq q, int c0,
+                 int c1, int c2, int c3) {
+  __shared__ int s_dst[kSwapSeqEntries];
+  __shared__ int s_src[kSwapSeqEntries];
+  __shared__ int s_lb[kSwapSeqLists + 1];
+  __shared__ int s_count;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    s_count = 0;
+    s_lb[0] = 0;
+  }
+  __syncthreads();
+  int off = 0;
+  for (int p = 0; p < q.lists; ++p) {
+    const int nblock = q.width[p], nextra = q.nextra[p];
+    for (int base = 0; base < nblock + nextra; base += blockDim.x) {
+      const int i = base + tid;
+      int d = 0, sr = 0;
+      bool keep = false;
+      if (i < nblock) {
+        d = q.base + off + i;
+        sr = blk[off + i];
+        keep = sr != d;
+      } else if (i < nblock + nextra) {
+        d = ext[2 * off + 2 * (i - nblock)];
+        sr = ext[2 * off + 2 * (i - nblock) + 1];
+        keep = sr != d;
+      }
+      const unsigned mask = __ballot_sync(0xffffffffu, keep);
+      int wbase = 0;
+      if ((tid & 31) == 0 && mask) wbase = atomicAdd(&s_count, __popc(mask));
+      wbase = __shfl_sync(0xffffffffu, wbase, 0);
+      if (keep) {
+        const int pos = wbase + __popc(mask & ((1u << (tid & 31)) - 1u));
+        s_dst[pos] = d;
+        s_src[pos] = sr;
+      }
+      __syncthreads();
+    }
+    // the list's last append is behind the barrier above; no thread appends
+    // to the next list before the boundary is read
+    if (tid == 0) s_lb[p + 1] = s_count;
+    __syncthreads();
+    off += nblock;
+  }
+  if (s_count == 0) return;
+
+  const int lane = tid & 31;
+  const int warps = blockDim.x >> 5;
+  const long long n1 = c1 - c0, ncols = n1 + (c3 - c2);
+  for (long long cid = (long long)blockIdx.x * warps + (tid >> 5); cid < ncols;
+       cid += (long long)gridDim.x * warps) {
+    const long long col = cid < n1 ? c0 + cid : c2 + (cid - n1);
+    double* ac = a + idx(0, col, lda);
+    for (int p = 0; p < q.lists; ++p) {
+      const int lo = s_lb[p], cnt = s_lb[p + 1] - lo;
+      if (cnt == 0) continue;
+      double v[kPerLane];
+#pragma unroll
+      for (int j = 0; j < kPerLane; ++j) {
+        const int i = lane + 32 * j;
+        if (i < cnt) v[j] = ac[s_src[lo + i]];
+      }
+      __syncwarp();
+#pragma unroll
+      for (int j = 0; j < kPerLane; ++j) {
+        const int i = lane + 32 * j;
+        if (i < cnt) ac[s_dst[lo + i]] = v[j];
+      }
+      __syncwarp();
+    }
+  }
+}
+
 __global__ void swap_row_kernel(double* a, long long lda, int n, int r1, int r2) {
   for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
        j += (long long)gridDim.x * blockDim.x) {
@@ -135,6 +217,41 @@ void launch_laswp(double* a, long long lda, int begin, int nblock, const int* sw
   dp::note_launch();
   laswp_kernel<<<grid, kLaswpThreads, 0, s>>>(a, lda, begin, nblock, swap_block, swap_extra,
                                               state, c0, c1, c2, c3);
+}
+
+int launch_laswp_seq(double* a, long long lda, const int* blk, const int* ext, int base,
+                     const int* widths, const int* nextra, int lists, int c0, int c1, int c2,
+                     int c3, cudaStream_t s) {
+  const long long ncols = (long long)(c1 - c0) + (c3 - c2);
+  if (ncols <= 0 || lists <= 0) return 0;
+  for (int i = 0; i < lists; ++i)  // a panel list: at most kMaxSwapEntries changed rows
+    if (widths[i] < 0 || nextra[i] < 0 || widths[i] + nextra[i] > kMaxSwapEntries) return -1;
+  const int warps = kLaswpThreads / 32;
+  const int grid = grid_for(ncols, warps, 148 * 16);
+  int launches = 0, p = 0, off = 0;
+  while (p < lists) {
+    // as many whole lists as fit the kernel's list and entry capacity
+    SwapSeq q;
+    q.base = base + off;
+    q.lists = 0;
+    int entries = 0, width = 0;
+    while (p < lists && q.lists < kSwapSeqLists &&
+           entries + widths[p] + nextra[p] <= kSwapSeqEntries) {
+      q.width[q.lists] = widths[p];
+      q.nextra[q.lists] = nextra[p];
+      entries += widths[p] + nextra[p];
+      width += widths[p];
+      ++q.lists;
+      ++p;
+    }
+    if (q.lists == 0) return -1;  // one list beyond the capacity: not a panel's list
+    dp::note_launch();
+    laswp_seq_kernel<<<grid, kLaswpThreads, 0, s>>>(a, lda, blk + off, ext + 2 * off, q, c0, c1,
+                                                    c2, c3);
+    ++launches;
+    off += width;
+  }
+  return launches;
 }
 
 void launch_swap_row(double* a, long long lda, int n, int r1, int r2, cudaStream_t s) {

@@ -29,7 +29,7 @@ class Options(ctypes.Structure):
         ("nb_outer", ctypes.c_int),
         ("panel_kernel", ctypes.c_int),
         ("precision", ctypes.c_int),
-        ("reserved", ctypes.c_int * 1),
+        ("lookahead", ctypes.c_int),
     ]
 
 
@@ -304,14 +304,16 @@ def delayed_getrf_cuda_status_string(status: int) -> str:
 
 def getrf_device_ex(m, n, d_a, lda, ipiv, jpiv, stream=None, nb=64, threshold=0.0,
                     policy=POLICY_FULL_PIVOT, panel_rows=0, nb_outer=0, panel_kernel=0,
-                    precision=PRECISION_FP64):
-    """dp_getrf_device_ex with explicit options.  Returns (status, info)."""
+                    precision=PRECISION_FP64, lookahead=0):
+    """dp_getrf_device_ex with explicit options.  Returns (status, info).
+    lookahead: 0 automatic, 1 on, 2 off (one stream, the unscheduled order)."""
     opt = Options()
     lib().dp_options_init(ctypes.byref(opt))
     opt.nb, opt.threshold, opt.policy, opt.panel_rows = nb, threshold, policy, panel_rows
     opt.nb_outer = nb_outer
     opt.panel_kernel = panel_kernel
     opt.precision = precision
+    opt.lookahead = lookahead
     info = ctypes.c_int(-1)
     st = lib().dp_getrf_device_ex(m, n, _dptr(d_a), lda, _iptr(ipiv), _iptr(jpiv),
                                   ctypes.byref(info), _stream(stream), ctypes.byref(opt))

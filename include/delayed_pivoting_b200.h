@@ -51,7 +51,9 @@ typedef struct dp_options {
   int panel_kernel;  /* 0 automatic (cluster panel when it fits), 1 cluster, 2 grid-wide */
   int precision;     /* DP_PRECISION_FP64 (reference arithmetic) or
                         DP_PRECISION_MIXED_BF16X3 (tensor-core trailing update) */
-  int reserved[1];
+  int lookahead;     /* 0 automatic (on beyond one outer block), 1 on, 2 off: the
+                        trailing update right of the next outer block runs on a
+                        second stream behind the next block's panels */
 } dp_options;
 
 void dp_options_init(dp_options *opt);

@@ -147,6 +147,49 @@ def test_repeat_calls_are_deterministic(built):
     np.testing.assert_array_equal(f1, f2)
 
 
+@pytest.mark.parametrize("name,nb,nb_outer", [
+    ("square_2000_zero20", 64, 256),   # fallback stops and restarts
+    ("square_2000_zero20", 16, 48),    # many blocks, restarts inside them
+    ("config1_n1024", 32, 96),         # delays at the end
+    ("tall_300x200", 8, 24),
+    ("wide_150x260", 8, 40),           # columns right of the pivots
+    ("square_517_lda520", 24, 64),
+])
+def test_lookahead_changes_no_bit(built, name, nb, nb_outer):
+    """The look-ahead schedule (two streams, deferred row swaps) gives every
+    element the same operations in the same order as the one-stream order."""
+    a, case = gc.load(name)
+    m, n = case["m"], case["n"]
+    kw = dict(nb=nb, nb_outer=nb_outer, policy=case["policy"])
+    f1, i1, j1, info1, st1 = run_device(a, m, n, lookahead=1, **kw)
+    f2, i2, j2, info2, st2 = run_device(a, m, n, lookahead=2, **kw)
+    assert st1 == 0 and st2 == 0 and info1 == info2 == case["info"]
+    np.testing.assert_array_equal(i1, case["ipiv"])
+    np.testing.assert_array_equal(j1, case["jpiv"])
+    np.testing.assert_array_equal(i1, i2)
+    np.testing.assert_array_equal(j1, j2)
+    np.testing.assert_array_equal(f1, f2)
+
+
+def test_lookahead_mixed_precision_records(built):
+    """Mixed precision: the next block's columns take their update in FP64
+    under look-ahead, so factors differ in rounding only; records do not."""
+    import oracle as orc
+
+    a, case = gc.load("square_2000_zero20")
+    kw = dict(nb=32, nb_outer=128, precision=2)
+    f1, i1, j1, info1, st1 = run_device(a, 2000, 2000, lookahead=1, **kw)
+    f2, i2, j2, info2, st2 = run_device(a, 2000, 2000, lookahead=2, **kw)
+    assert st1 == 0 and st2 == 0 and info1 == info2 == case["info"]
+    np.testing.assert_array_equal(i1, i2)
+    np.testing.assert_array_equal(j1, j2)
+    np.testing.assert_array_equal(i1, case["ipiv"])
+    r1, an = orc.residual(a, f1, 2000, 2000, info1, i1, j1)
+    r2, _ = orc.residual(a, f2, 2000, 2000, info2, i2, j2)
+    assert r1 / an <= 1e-4  # FP32-level products with FP32 accumulation
+    assert r1 <= 2.0 * r2  # FP64 on the next block's columns loses nothing
+
+
 @pytest.mark.slow
 def test_config2_n16384_records_bit_identical(built):
     """n = 16384, 16 tiny + 3 zero columns: records equal the reference's;
