@@ -28,6 +28,8 @@ struct PanelParams {
   double* rowk;               // [4][w_max + 1]
   int* swap_block;            // [end - begin]: source row of block row begin + i
   int* swap_extra;            // [2 * (end - begin)]: (dst, src) pairs below `end`
+  int gated;                  // cluster kernel: 1 -> do nothing when state->stop_k >= 0 (an
+                              // earlier panel of the same enqueued sequence stopped)
 };
 
 __global__ void panel_factor_kernel(PanelParams p);
@@ -40,10 +42,12 @@ constexpr int kPanelThreadsHost = 256;
 size_t panel_smem_bytes(int w, int rows_per_cta);
 
 // Applies the composite row permutation of one panel (swap list written by
-// panel_factor_kernel) to columns [c0, c1) and [c2, c3).
+// panel_factor_kernel) to columns [c0, c1) and [c2, c3).  gate_begin >= 0:
+// do nothing when state->stop_k is in [0, gate_begin) (a panel before this
+// one stopped; its own stop, at or after gate_begin, still applies).
 void launch_laswp(double* a, long long lda, int begin, int nblock, const int* swap_block,
                   const int* swap_extra, const State* state, int c0, int c1, int c2, int c3,
-                  cudaStream_t s);
+                  cudaStream_t s, int gate_begin = -1);
 
 // Swap lists of up to kSwapSeqLists consecutive panels (kSwapSeqEntries
 // entries in all) applied in order by one launch of laswp_seq_kernel.
@@ -53,33 +57,35 @@ struct SwapSeq {
   int lists;
   int base;  // first row of the first panel
   int width[kSwapSeqLists];
-  int nextra[kSwapSeqLists];
 };
 
 // Applies the swap lists of `lists` consecutive panels starting at row
 // `base` (panel p of width widths[p], its block part at blk[begin_p - base],
-// its nextra[p] extra pairs at ext[2 (begin_p - base)]) to the columns
-// [c0, c1) and [c2, c3), in panel order.  Returns the number of launches, or
-// -1 when a list exceeds a panel's size.
+// up to widths[p] extra pairs at ext[2 (begin_p - base)], the unused ones
+// holding a negative destination) to the columns [c0, c1) and [c2, c3), in
+// panel order.  Returns the number of launches, or -1 when a panel is wider
+// than the kernel's lists.
 int launch_laswp_seq(double* a, long long lda, const int* blk, const int* ext, int base,
-                     const int* widths, const int* nextra, int lists, int c0, int c1, int c2,
-                     int c3, cudaStream_t s);
+                     const int* widths, int lists, int c0, int c1, int c2, int c3,
+                     cudaStream_t s);
 
 // B(w x nc) <- L^{-1} B, L unit lower (w x w) at a(r0, r0), B at a(r0, c0);
-// w <= trsm_max_width().
+// w <= trsm_max_width().  A non-null `gate`: do nothing when *gate >= 0
+// (the stop word of an enqueued panel sequence, read when the kernel starts).
 int trsm_max_width();
 void launch_trsm_unit_lower(double* a, long long lda, int r0, int w, int c0, int nc,
-                            cudaStream_t s);
+                            cudaStream_t s, const int* gate = nullptr);
 // Same with separate operands; and B <- U^{-1} B for upper U with diagonal.
 void launch_trsm_lower_unit(const double* L, long long ldl, double* B, long long ldb, int w, int nc,
-                            cudaStream_t s);
+                            cudaStream_t s, const int* gate = nullptr);
 void launch_trsm_upper(const double* U, long long ldu, double* B, long long ldb, int w, int nc,
                        cudaStream_t s);
 
 // C(M x N) -= A(M x K) * B(K x N); all three inside the same column-major
-// matrix (or any column-major operands).
+// matrix (or any column-major operands).  `gate` as for the TRSM.
 void launch_gemm_minus(int M, int N, int K, const double* A, long long lda, const double* B,
-                       long long ldb, double* C, long long ldc, cudaStream_t s);
+                       long long ldb, double* C, long long ldc, cudaStream_t s,
+                       const int* gate = nullptr);
 
 // C(M x N) -= A(M x K) * B(K x N) on the tensor cores (BF16 split into
 // `terms` pieces: 2 -> three products, 3 -> six products; FP32 accumulation in

@@ -15,6 +15,9 @@
 // registers so shared-memory latency hides behind the previous k-step's MMAs.  The C tile is prefetched into L2 when
 // the CTA starts so the read-modify-write of the epilogue hits L2.
 // Accumulation is C - sum_k(a*b), the sum formed in FP64 by the tensor core.
+#include <atomic>
+
+#include "delayed_pivoting_b200.h"
 #include "dp_device.cuh"
 #include "dp_kernels.h"
 
@@ -64,7 +67,9 @@ struct Cfg {
 template <class C>
 __global__ void __launch_bounds__(C::THREADS, C::MINB)
 dgemm_minus_kernel(int M, int N, int K, const double* __restrict__ A, long long lda,
-                   const double* __restrict__ B, long long ldb, double* Cm, long long ldc) {
+                   const double* __restrict__ B, long long ldb, double* Cm, long long ldc,
+                   const int* gate) {
+  if (gate && *gate >= 0) return;  // an enqueued panel sequence stopped before this update
   extern __shared__ __align__(16) double gsm[];
   double* As = gsm;                         // [STAGES][BK][LDA_S]
   double* Bs = gsm + C::STAGES * C::A_STAGE;  // [STAGES][BN][LDB_S]
@@ -189,28 +194,59 @@ dgemm_minus_kernel(int M, int N, int K, const double* __restrict__ A, long long 
 
 template <class C>
 void launch(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
-            double* Cm, long long ldc, cudaStream_t s) {
+            double* Cm, long long ldc, cudaStream_t s, const int* gate) {
   dp::ensure_smem((const void*)dgemm_minus_kernel<C>, C::SMEM);
   dim3 grid((M + C::BM - 1) / C::BM, (N + C::BN - 1) / C::BN);
   dp::note_launch();
-  dgemm_minus_kernel<C><<<grid, C::THREADS, C::SMEM, s>>>(M, N, K, A, lda, B, ldb, Cm, ldc);
+  dgemm_minus_kernel<C><<<grid, C::THREADS, C::SMEM, s>>>(M, N, K, A, lda, B, ldb, Cm, ldc, gate);
 }
 
-// Production configuration: 128 x 128 tiles, 8 warps of 64 x 32.
+// 128 x 128 tiles, 8 warps of 64 x 32, one CTA per SM (212 KB of stages).
 using Big = Cfg<128, 128, 32, 3, 2, 4, 1>;
+// 128 x 64 tiles, 4 warps of 64 x 32, 16-deep k chunks in 4 stages (108 KB):
+// two CTAs per SM, so one CTA's pipeline fill and C read-modify-write overlap
+// the other's MMAs - with K = one outer block (256) those fixed costs are a
+// large part of a 128 x 128 tile's life.
+using Half = Cfg<128, 64, 16, 4, 2, 2, 2>;
 // Few columns (the refinement residual B - A X, N = right-hand sides): 64 x 32
 // tiles, 4 warps of 16 x 32, two CTAs per SM, so M / 64 CTAs stream A.
 using Skinny = Cfg<64, 32, 32, 4, 4, 1, 2>;
 
+std::atomic<int> g_tile{0};  // 0 automatic, 1 Big, 2 Half
+
 }  // namespace gemm
 
+// Every configuration accumulates each element over k in the same order
+// (k = 0, 1, ... in chunks of 4, one accumulator), so the choice of tile
+// changes no result bit.
 void launch_gemm_minus(int M, int N, int K, const double* A, long long lda, const double* B,
-                       long long ldb, double* C, long long ldc, cudaStream_t s) {
+                       long long ldb, double* C, long long ldc, cudaStream_t s, const int* gate) {
   if (M <= 0 || N <= 0 || K <= 0) return;
+  const int tile = gemm::g_tile.load(std::memory_order_relaxed);
   if (N <= 32)
-    gemm::launch<gemm::Skinny>(M, N, K, A, lda, B, ldb, C, ldc, s);
+    gemm::launch<gemm::Skinny>(M, N, K, A, lda, B, ldb, C, ldc, s, gate);
+  else if (tile == 1)
+    gemm::launch<gemm::Big>(M, N, K, A, lda, B, ldb, C, ldc, s, gate);
   else
-    gemm::launch<gemm::Big>(M, N, K, A, lda, B, ldb, C, ldc, s);
+    gemm::launch<gemm::Half>(M, N, K, A, lda, B, ldb, C, ldc, s, gate);
 }
 
 }  // namespace dp
+
+extern "C" {
+
+int dp_schur_update_device(int M, int N, int K, const double* A, int lda, const double* B,
+                           int ldb, double* C, int ldc, void* stream) {
+  if (M < 0 || N < 0 || K < 0) return dp::kInvalidArgument;
+  if (M == 0 || N == 0 || K == 0) return dp::kOk;
+  if (!A || !B || !C || lda < M || ldb < K || ldc < M) return dp::kInvalidArgument;
+  dp::launch_gemm_minus(M, N, K, A, lda, B, ldb, C, ldc, static_cast<cudaStream_t>(stream));
+  return cudaGetLastError() == cudaSuccess ? dp::kOk : dp::kCudaFailure;
+}
+
+int dp_gemm_tile(int tile) {
+  if (tile < 0 || tile > 2) return -1;
+  return dp::gemm::g_tile.exchange(tile);
+}
+
+}  // extern "C"

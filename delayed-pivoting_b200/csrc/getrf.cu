@@ -360,21 +360,22 @@ double panel_flops(int m, int begin, int w) {
 // most trsm_max_width() are solved by the TRSM kernel, the blocks below them
 // by the GEMM kernel.
 void trsm_blocked(double* a, long long lda, int r0, int W, int c0, int nc, cudaStream_t st,
-                  Recorder& rec) {
+                  Recorder& rec, const int* gate = nullptr) {
   if (W <= 1 || nc <= 0) return;
   const int tw = trsm_max_width();
   for (int b = 0; b < W; b += tw) {
     const int wb = std::min(tw, W - b);
     if (wb > 1) {
       rec.begin(DP_KFAM_TRSM);
-      launch_trsm_unit_lower(a, lda, r0 + b, wb, c0, nc, st);
+      launch_trsm_unit_lower(a, lda, r0 + b, wb, c0, nc, st, gate);
       rec.end((double)wb * (wb - 1) * nc, 8.0 * (0.5 * wb * wb + 2.0 * wb * nc), 1);
     }
     const int rows_below = W - b - wb;
     if (rows_below > 0) {
       rec.begin(DP_KFAM_GEMM);
       launch_gemm_minus(rows_below, nc, wb, a + idx(r0 + b + wb, r0 + b, lda), lda,
-                        a + idx(r0 + b, c0, lda), lda, a + idx(r0 + b + wb, c0, lda), lda, st);
+                        a + idx(r0 + b, c0, lda), lda, a + idx(r0 + b + wb, c0, lda), lda, st,
+                        gate);
       rec.end(2.0 * rows_below * (double)nc * wb,
               8.0 * ((double)rows_below * wb + (double)wb * nc + 2.0 * rows_below * (double)nc), 1);
     }
@@ -386,12 +387,13 @@ void trsm_blocked(double* a, long long lda, int r0, int W, int c0, int nc, cudaS
 // A(r_gemm:m, c0:n_end) -= L(r_gemm:m, s0:s0+W) * U(s0:s0+W, c0:n_end).
 // When `mixed_ws` is set the rank-W update runs on the tensor cores (BF16
 // split into `terms` pieces, FP32 accumulation); the TRSM always runs in FP64.
+// A non-null `gate` (FP64 only) makes the kernels do nothing once *gate >= 0.
 int update_columns(double* a, long long lda, int m, int s0, int W, int r_gemm, int c0, int n_end,
                    cudaStream_t st, Recorder& rec, void* mixed_ws = nullptr,
-                   int* status = nullptr, int terms = 2) {
+                   int* status = nullptr, int terms = 2, const int* gate = nullptr) {
   const int nc = n_end - c0;
   if (W <= 0 || nc <= 0) return kOk;
-  trsm_blocked(a, lda, s0, W, c0, nc, st, rec);
+  trsm_blocked(a, lda, s0, W, c0, nc, st, rec, gate);
   const int M = m - r_gemm;
   if (M <= 0) return kOk;
   const double fl = 2.0 * M * (double)nc * W;
@@ -406,7 +408,7 @@ int update_columns(double* a, long long lda, int m, int s0, int W, int r_gemm, i
   }
   rec.begin(DP_KFAM_GEMM);
   launch_gemm_minus(M, nc, W, a + idx(r_gemm, s0, lda), lda, a + idx(s0, c0, lda), lda,
-                    a + idx(r_gemm, c0, lda), lda, st);
+                    a + idx(r_gemm, c0, lda), lda, st, gate);
   rec.end(fl, by, 1);
   return kOk;
 }
@@ -465,21 +467,18 @@ struct Schedule {
 
 // Applies the deferred swap lists of the panels [B, B + sum widths) of an
 // outer block to the columns [c0, c1) and [c2, c3).
-int apply_deferred(double* a, long long lda, const Workspace& ws, const int* blk,
-                   const int* ext, int B, const std::vector<int>& widths,
-                   const std::vector<int>& extras, int c0, int c1, int c2, int c3,
+int apply_deferred(double* a, long long lda, const int* blk, const int* ext, int B,
+                   const std::vector<int>& widths, int c0, int c1, int c2, int c3,
                    cudaStream_t st, Recorder& rec) {
   const long long cols = (long long)std::max(0, c1 - c0) + std::max(0, c3 - c2);
   if (widths.empty() || cols <= 0) return kOk;
-  double moved = 0.0;
-  for (size_t i = 0; i < widths.size(); ++i) moved += (double)widths[i] + extras[i];
+  double moved = 0.0;  // at most: every block row and one row below it per step
+  for (int w : widths) moved += 2.0 * w;
   rec.begin(DP_KFAM_LASWP);
-  const int launches = launch_laswp_seq(a, lda, blk, ext, B, widths.data(), extras.data(),
-                                        (int)widths.size(), c0, c1, c2, c3, st);
+  const int launches = launch_laswp_seq(a, lda, blk, ext, B, widths.data(), (int)widths.size(),
+                                        c0, c1, c2, c3, st);
   rec.end(0.0, 16.0 * moved * (double)cols, std::max(launches, 0));
-  if (launches < 0) return kInvalidArgument;
-  (void)ws;
-  return kOk;
+  return launches < 0 ? kInvalidArgument : kOk;
 }
 
 // Two-level blocked delayed LU.  An outer block [B, E) of width NB is
@@ -507,6 +506,14 @@ int apply_deferred(double* a, long long lda, const Workspace& ws, const int* blk
 // restores the state of the unscheduled order before the materialize /
 // search logic runs.  Every element receives the same operations in the
 // same order either way, so the schedule changes no result.
+//
+// With look-ahead the cluster panels of a block are also enqueued without a
+// host round trip each: a panel that stops records stop_k, and every kernel
+// enqueued after it (later panels, their swaps, the in-block updates) reads
+// the word when it starts and does nothing.  The host reads the state once
+// per block, finds the stopped panel from stop_k, and proceeds exactly as if
+// it had stopped there.  (The grid-wide cooperative panel keeps a round trip
+// per panel, with s2 drained before it.)
 int factorize(int m, int n, double* a, long long lda, const Options& o, Workspace& ws,
               const DeviceInfo& di, const Schedule& sc, int& info) {
   cudaStream_t st = sc.s1;
@@ -524,19 +531,35 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
   const int NB = std::max(o.nb_outer, o.nb);
   const int terms = mixed_terms(o.precision);
   void* mixed_ws = terms ? ws.mixed : nullptr;
-  std::vector<int> widths, extras;  // the current block's panels (look-ahead)
+  int* const stop_word = &ws.state->stop_k;
+  std::vector<int> widths;  // the current block's panels (look-ahead)
+  if (la) DP_CHECK_CUDA(cudaMemsetAsync(stop_word, 0xFF, sizeof(int), st));  // stop_k = -1
   while (B < pivots) {
     const int E = std::min(pivots, B + NB);
     int* blk = la ? ws.defer_blk + (size_t)half * ws.defer_cap : ws.swap_block;
     int* ext = la ? ws.defer_ext + (size_t)2 * half * ws.defer_cap : ws.swap_extra;
+    // extra pairs are written from the front of each panel's region: the
+    // rest must read as "no pair" (destination -1)
+    if (la) DP_CHECK_CUDA(cudaMemsetAsync(ext, 0xFF, sizeof(int) * 2 * (size_t)(E - B), st));
     widths.clear();
-    extras.clear();
     int b = B, e = B, stop = -1;
+    bool unread = false;  // enqueued panels whose state the host has not read
     while (b < E) {
       int w = std::min(std::min(o.nb, ws.w_max), E - b);
       int G = 1, R = 1;
       const bool use_cluster = o.panel_kernel != 2 && plan_cluster(m - b, w, di, G, R);
       if (!use_cluster && !plan_panel(m - b, w, o.panel_rows, di, G, R)) return kInvalidArgument;
+      const bool enqueue = la && use_cluster;
+      if (!enqueue && unread) {
+        // a synchronous panel follows enqueued ones: settle them first
+        if (int err = read_state(hs, ws, st)) return err;
+        if (hs.status != kOk) return hs.status;
+        unread = false;
+        if (hs.stop_k >= 0) {
+          stop = hs.stop_k;
+          break;
+        }
+      }
       e = b + w;
       if (la && !use_cluster) {
         // the cooperative grid needs all its CTAs resident: s2 finishes first
@@ -563,6 +586,7 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       pp.rowk = ws.rowk;
       pp.swap_block = la ? blk + (b - B) : ws.swap_block;
       pp.swap_extra = la ? ext + 2 * (size_t)(b - B) : ws.swap_extra;
+      pp.gated = enqueue ? 1 : 0;
       rec.begin(DP_KFAM_PANEL);
       if (use_cluster) {
         cudaLaunchConfig_t cfg = {};
@@ -589,16 +613,28 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       }
       rec.end(panel_flops(m, b, w), 16.0 * (double)(m - b) * w, 1);
       positioned = false;
+      if (la) widths.push_back(w);
+
+      if (enqueue) {
+        // swaps inside the block, then the rest of the block: both skip
+        // themselves if this panel or an earlier one stopped (the swaps of
+        // the stopping panel itself still apply)
+        rec.begin(DP_KFAM_LASWP);
+        launch_laswp(a, lda, b, w, pp.swap_block, pp.swap_extra, ws.state, B, b, e, E, st, b);
+        rec.end(0.0, 16.0 * 2.0 * w * (double)(E - B - w), 1);
+        update_columns(a, lda, m, b, w, e, e, E, st, rec, nullptr, nullptr, 2, stop_word);
+        DP_CHECK_CUDA(cudaGetLastError());
+        unread = true;
+        b = e;
+        continue;
+      }
       if (int err = read_state(hs, ws, st)) return err;
       if (hs.status != kOk) return hs.status;
-
       const double moved = (double)(hs.block_changed + hs.swap_count);
       rec.begin(DP_KFAM_LASWP);
       if (la) {
         launch_laswp(a, lda, b, w, pp.swap_block, pp.swap_extra, ws.state, B, b, e, E, st);
         rec.end(0.0, 16.0 * moved * (double)(E - B - w), 1);
-        widths.push_back(w);
-        extras.push_back(hs.swap_count);
       } else {
         launch_laswp(a, lda, b, w, ws.swap_block, ws.swap_extra, ws.state, 0, b, e, n, st);
         rec.end(0.0, 16.0 * moved * (double)(n - w), 1);
@@ -610,6 +646,20 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       update_columns(a, lda, m, b, w, e, e, E, st, rec);  // rest of the outer block
       DP_CHECK_CUDA(cudaGetLastError());
       b = e;
+    }
+    if (unread) {
+      if (int err = read_state(hs, ws, st)) return err;
+      if (hs.status != kOk) return hs.status;
+      if (hs.stop_k >= 0) stop = hs.stop_k;
+    }
+    if (stop >= 0 && la) {
+      // the panel that stopped: the last whose first column is <= stop; the
+      // ones after it did nothing
+      size_t p = 0;
+      b = B;
+      while (p + 1 < widths.size() && b + widths[p] <= stop) b += widths[p++];
+      e = b + widths[p];
+      widths.resize(p + 1);
     }
     if (stop < 0 && !la) {
       // right of the outer block: the O(n^3) update
@@ -625,16 +675,14 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       const int NNE = std::min(pivots, NE + NB);  // the block after next
       // s1: the next block's columns, then on to its panels
       if (pending) DP_CHECK_CUDA(cudaStreamWaitEvent(st, sc.next, 0));
-      if (int err = apply_deferred(a, lda, ws, blk, ext, B, widths, extras, E, NE, NE, NE, st,
-                                   rec))
+      if (int err = apply_deferred(a, lda, blk, ext, B, widths, E, NE, NE, NE, st, rec))
         return err;
       update_columns(a, lda, m, B, E - B, E, E, NE, st, rec);
       DP_CHECK_CUDA(cudaGetLastError());
       DP_CHECK_CUDA(cudaEventRecord(sc.block, st));
       // s2: everything else, behind the block
       DP_CHECK_CUDA(cudaStreamWaitEvent(sc.s2, sc.block, 0));
-      if (int err = apply_deferred(a, lda, ws, blk, ext, B, widths, extras, 0, B, NE, n, sc.s2,
-                                   *sc.r2))
+      if (int err = apply_deferred(a, lda, blk, ext, B, widths, 0, B, NE, n, sc.s2, *sc.r2))
         return err;
       pending = false;
       if (NNE > NE) {
@@ -660,8 +708,7 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       DP_CHECK_CUDA(cudaEventRecord(sc.next, sc.s2));
       DP_CHECK_CUDA(cudaStreamWaitEvent(st, sc.next, 0));
       pending = false;
-      if (int err = apply_deferred(a, lda, ws, blk, ext, B, widths, extras, 0, B, E, n, st, rec))
-        return err;
+      if (int err = apply_deferred(a, lda, blk, ext, B, widths, 0, B, E, n, st, rec)) return err;
     }
     update_columns(a, lda, m, b, k - b, k, e, E, st, rec);  // rest of the outer block
     if (int err = update_columns(a, lda, m, B, k - B, k, E, n, st, rec, mixed_ws,
@@ -689,6 +736,7 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
     rec.end(0.0, 32.0 * ((c.row != k ? (double)n : 0.0) + (c.col != k ? (double)m : 0.0)),
             1 + (c.row != k) + (c.col != k));
     DP_CHECK_CUDA(cudaGetLastError());
+    if (la) DP_CHECK_CUDA(cudaMemsetAsync(stop_word, 0xFF, sizeof(int), st));  // re-arm
     B = k;
     positioned = true;
   }

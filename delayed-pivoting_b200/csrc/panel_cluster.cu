@@ -76,6 +76,9 @@ __device__ __forceinline__ LocalBest warp_lb(LocalBest v) {
 }  // namespace
 
 __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams p) {
+  // Every CTA reads the same word before any barrier or state write (a stop
+  // is recorded only by an earlier kernel), so all of them leave together.
+  if (p.gated && p.state->stop_k >= 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cg::cluster_group cluster = cg::this_cluster();
   const int C = (int)cluster.num_blocks();

@@ -24,10 +24,15 @@ constexpr int kPerLane = kMaxSwapEntries / 32;
 
 __global__ void __launch_bounds__(kLaswpThreads)
 laswp_kernel(double* a, long long lda, int begin, int nblock, const int* swap_block,
-             const int* swap_extra, const State* state, int c0, int c1, int c2, int c3) {
+             const int* swap_extra, const State* state, int c0, int c1, int c2, int c3,
+             int gate_begin) {
   __shared__ int s_dst[kMaxSwapEntries];
   __shared__ int s_src[kMaxSwapEntries];
   __shared__ int s_count;
+  if (gate_begin >= 0) {
+    const int sk = state->stop_k;
+    if (sk >= 0 && sk < gate_begin) return;  // an earlier panel stopped: this one never ran
+  }
   const int tid = threadIdx.x;
   const int nextra = min(state->swap_count, kMaxSwapEntries - nblock);
   if (tid == 0) s_count = 0;
@@ -86,8 +91,10 @@ laswp_kernel(double* a, long long lda, int begin, int nblock, const int* swap_bl
 
 // The swap lists of consecutive panels applied in panel order: list p covers
 // the panel starting at row begin_p = q.base + width[0] + ... + width[p-1],
-// its block part at blk[begin_p - q.base] and its extra pairs at
-// ext[2 (begin_p - q.base)].  Each CTA compacts every list into shared memory
+// its block part at blk[begin_p - q.base] and up to width[p] extra pairs at
+// ext[2 (begin_p - q.base)] (unused pairs have a negative destination: the
+// region is filled with -1 before the panel runs, and the panel writes its
+// pairs from the front).  Each CTA compacts every list into shared memory
 // (list p at [s_lb[p], s_lb[p+1])); each warp then applies the lists to one
 // column in turn, gathering a list's sources before scattering it, so the
 // result equals launching laswp_kernel once per panel.
@@ -106,7 +113,7 @@ laswp_seq_kernel(double* a, long long lda, const int* blk, const int* ext, SwapS
   __syncthreads();
   int off = 0;
   for (int p = 0; p < q.lists; ++p) {
-    const int nblock = q.width[p], nextra = q.nextra[p];
+    const int nblock = q.width[p], nextra = q.width[p];
     for (int base = 0; base < nblock + nextra; base += blockDim.x) {
       const int i = base + tid;
       int d = 0, sr = 0;
@@ -118,7 +125,7 @@ laswp_seq_kernel(double* a, long long lda, const int* blk, const int* ext, SwapS
       } else if (i < nblock + nextra) {
         d = ext[2 * off + 2 * (i - nblock)];
         sr = ext[2 * off + 2 * (i - nblock) + 1];
-        keep = sr != d;
+        keep = d >= 0 && sr != d;
       }
       const unsigned mask = __ballot_sync(0xffffffffu, keep);
       int wbase = 0;
@@ -209,23 +216,23 @@ int grid_for(long long work, int threads, int cap) {
 
 void launch_laswp(double* a, long long lda, int begin, int nblock, const int* swap_block,
                   const int* swap_extra, const State* state, int c0, int c1, int c2, int c3,
-                  cudaStream_t s) {
+                  cudaStream_t s, int gate_begin) {
   const long long ncols = (long long)(c1 - c0) + (c3 - c2);
   if (ncols <= 0 || nblock <= 0) return;
   const int warps = kLaswpThreads / 32;
   const int grid = grid_for(ncols, warps, 148 * 16);
   dp::note_launch();
   laswp_kernel<<<grid, kLaswpThreads, 0, s>>>(a, lda, begin, nblock, swap_block, swap_extra,
-                                              state, c0, c1, c2, c3);
+                                              state, c0, c1, c2, c3, gate_begin);
 }
 
 int launch_laswp_seq(double* a, long long lda, const int* blk, const int* ext, int base,
-                     const int* widths, const int* nextra, int lists, int c0, int c1, int c2,
-                     int c3, cudaStream_t s) {
+                     const int* widths, int lists, int c0, int c1, int c2, int c3,
+                     cudaStream_t s) {
   const long long ncols = (long long)(c1 - c0) + (c3 - c2);
   if (ncols <= 0 || lists <= 0) return 0;
   for (int i = 0; i < lists; ++i)  // a panel list: at most kMaxSwapEntries changed rows
-    if (widths[i] < 0 || nextra[i] < 0 || widths[i] + nextra[i] > kMaxSwapEntries) return -1;
+    if (widths[i] < 1 || 2 * widths[i] > kMaxSwapEntries) return -1;
   const int warps = kLaswpThreads / 32;
   const int grid = grid_for(ncols, warps, 148 * 16);
   int launches = 0, p = 0, off = 0;
@@ -235,11 +242,9 @@ int launch_laswp_seq(double* a, long long lda, const int* blk, const int* ext, i
     q.base = base + off;
     q.lists = 0;
     int entries = 0, width = 0;
-    while (p < lists && q.lists < kSwapSeqLists &&
-           entries + widths[p] + nextra[p] <= kSwapSeqEntries) {
+    while (p < lists && q.lists < kSwapSeqLists && entries + 2 * widths[p] <= kSwapSeqEntries) {
       q.width[q.lists] = widths[p];
-      q.nextra[q.lists] = nextra[p];
-      entries += widths[p] + nextra[p];
+      entries += 2 * widths[p];
       width += widths[p];
       ++q.lists;
       ++p;

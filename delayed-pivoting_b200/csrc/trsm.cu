@@ -46,7 +46,8 @@ __device__ __forceinline__ void stage_out(double* B, long long ldb, int w, int n
 // B (w x nc) <- L^{-1} B, L unit lower (w x w).
 __global__ void __launch_bounds__(kTrsmThreads)
 trsm_lower_unit_kernel(const double* __restrict__ L, long long ldl, double* B, long long ldb, int w,
-                       int nc) {
+                       int nc, const int* gate) {
+  if (gate && *gate >= 0) return;
   extern __shared__ __align__(16) double tsm[];
   double* Ls = tsm;                    // Ls[p * 64 + i] = L(i, p), zero outside the strict lower part
   double* Bt = tsm + kTrsmW * kTrsmW + kTrsmW;  // Bt[c * 65 + i] = B(i, c)
@@ -177,12 +178,12 @@ void configure() {
 int trsm_max_width() { return kTrsmW; }
 
 void launch_trsm_lower_unit(const double* L, long long ldl, double* B, long long ldb, int w, int nc,
-                            cudaStream_t s) {
+                            cudaStream_t s, const int* gate) {
   if (w <= 1 || nc <= 0) return;  // w == 1: unit diagonal, nothing to solve
   configure();
   const int grid = (nc + kTrsmCols - 1) / kTrsmCols;
   dp::note_launch();
-  trsm_lower_unit_kernel<<<grid, kTrsmThreads, kTrsmSmem, s>>>(L, ldl, B, ldb, w, nc);
+  trsm_lower_unit_kernel<<<grid, kTrsmThreads, kTrsmSmem, s>>>(L, ldl, B, ldb, w, nc, gate);
 }
 
 void launch_trsm_upper(const double* U, long long ldu, double* B, long long ldb, int w, int nc,
@@ -195,8 +196,8 @@ void launch_trsm_upper(const double* U, long long ldu, double* B, long long ldb,
 }
 
 void launch_trsm_unit_lower(double* a, long long lda, int r0, int w, int c0, int nc,
-                            cudaStream_t s) {
-  launch_trsm_lower_unit(a + idx(r0, r0, lda), lda, a + idx(r0, c0, lda), lda, w, nc, s);
+                            cudaStream_t s, const int* gate) {
+  launch_trsm_lower_unit(a + idx(r0, r0, lda), lda, a + idx(r0, c0, lda), lda, w, nc, s, gate);
 }
 
 }  // namespace dp

@@ -25,7 +25,7 @@ from .api import (  # noqa: F401
     PRECISION_FP64, PRECISION_MIXED_BF16X3, PRECISION_MIXED_BF16X6, getrf_device_noalloc,
     BATCH_MAX_N, BATCH_MAX_NB, BATCH_BUCKETS, BatchOptions, Batch, BatchError, batch_options,
     batch_autotune, batch_tune_save, batch_tune_load, Factor, Server, ServerOptions, Request,
-    RequestResult, ServerStats, server_options, server_clock,
+    RequestResult, ServerStats, server_options, server_clock, schur_update_device, gemm_tile,
 )
 from .inputs import (  # noqa: F401
     normal_matrix, plant_columns, mt64_nth, planted_matrix, uniform_stream, normal_vector,

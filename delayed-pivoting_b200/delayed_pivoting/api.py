@@ -326,6 +326,22 @@ def getrs_device(n, nrhs, d_lu, ldlu, ipiv, jpiv, d_b, ldb, stream=None):
                                  _dptr(d_b), ldb, _stream(stream))
 
 
+def schur_update_device(M, N, K, d_a, lda, d_b, ldb, d_c, ldc, stream=None):
+    """dp_schur_update_device: C -= A * B in FP64 on the DMMA kernel
+    (column-major operands; asynchronous on `stream`).  Returns the status."""
+    L = lib()
+    L.dp_schur_update_device.restype = ctypes.c_int
+    L.dp_schur_update_device.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p, ctypes.c_int] * 3 \
+        + [ctypes.c_void_p]
+    return L.dp_schur_update_device(M, N, K, _dptr(d_a), lda, _dptr(d_b), ldb, _dptr(d_c), ldc,
+                                    _stream(stream))
+
+
+def gemm_tile(tile: int) -> int:
+    """dp_gemm_tile: 0 automatic, 1 128 x 128, 2 128 x 64.  Returns the previous setting."""
+    return lib().dp_gemm_tile(int(tile))
+
+
 def gesv_ir_device(n, nrhs, d_a, lda, d_b, ldb, precision=PRECISION_MIXED_BF16X3, max_iter=10,
                    tol=1e-14, stream=None):
     """dp_gesv_ir_device: mixed-precision LU + FP64 iterative refinement.

@@ -308,6 +308,19 @@ void dp_stats_get(dp_kernel_stats *out);
  * stream and host thread (no reference counterpart). */
 long long dp_kernel_launches(void);
 
+/* The FP64 Schur-complement update of the factorisation, C -= A * B, on the
+ * DMMA tensor-core kernel (column-major M x K A, K x N B, M x N C; the
+ * trailing update that delayed_dgetrf_cuda.cu:205-209 hands to cublasDgemm
+ * with alpha = -1, beta = 1).  Asynchronous on `stream`; every element is
+ * accumulated over k in order, one FP64 accumulator. */
+int dp_schur_update_device(int M, int N, int K, const double *A, int lda, const double *B,
+                           int ldb, double *C, int ldc, void *stream);
+
+/* Tile of that kernel for N > 32 (tuning; no result bit depends on it):
+ * 0 automatic, 1 128 x 128 (one CTA per SM), 2 128 x 64 (two CTAs per SM).
+ * Returns the previous setting, or -1 for an invalid one. */
+int dp_gemm_tile(int tile);
+
 /* delayed_dgetrf_cuda.hpp:63 (delayed_getrf_cuda_status_string). */
 const char *dp_status_string(int status);
 

@@ -147,20 +147,23 @@ def test_repeat_calls_are_deterministic(built):
     np.testing.assert_array_equal(f1, f2)
 
 
-@pytest.mark.parametrize("name,nb,nb_outer", [
-    ("square_2000_zero20", 64, 256),   # fallback stops and restarts
-    ("square_2000_zero20", 16, 48),    # many blocks, restarts inside them
-    ("config1_n1024", 32, 96),         # delays at the end
-    ("tall_300x200", 8, 24),
-    ("wide_150x260", 8, 40),           # columns right of the pivots
-    ("square_517_lda520", 24, 64),
+@pytest.mark.parametrize("name,nb,nb_outer,panel", [
+    ("square_2000_zero20", 64, 256, 0),   # fallback stops and restarts
+    ("square_2000_zero20", 16, 48, 0),    # many blocks, restarts inside them
+    ("square_2000_zero20", 16, 48, 2),    # grid-wide panel: one round trip per panel
+    ("config1_n1024", 32, 96, 0),         # delays at the end
+    ("tall_300x200", 8, 24, 0),
+    ("wide_150x260", 8, 40, 0),           # columns right of the pivots
+    ("square_517_lda520", 24, 64, 0),
 ])
-def test_lookahead_changes_no_bit(built, name, nb, nb_outer):
-    """The look-ahead schedule (two streams, deferred row swaps) gives every
-    element the same operations in the same order as the one-stream order."""
+def test_lookahead_changes_no_bit(built, name, nb, nb_outer, panel):
+    """The look-ahead schedule (two streams, deferred row swaps, panels
+    enqueued without a round trip and skipped on the device after a stop)
+    gives every element the same operations in the same order as the
+    one-stream order."""
     a, case = gc.load(name)
     m, n = case["m"], case["n"]
-    kw = dict(nb=nb, nb_outer=nb_outer, policy=case["policy"])
+    kw = dict(nb=nb, nb_outer=nb_outer, policy=case["policy"], panel_kernel=panel)
     f1, i1, j1, info1, st1 = run_device(a, m, n, lookahead=1, **kw)
     f2, i2, j2, info2, st2 = run_device(a, m, n, lookahead=2, **kw)
     assert st1 == 0 and st2 == 0 and info1 == info2 == case["info"]
@@ -188,6 +191,37 @@ def test_lookahead_mixed_precision_records(built):
     r2, _ = orc.residual(a, f2, 2000, 2000, info2, i2, j2)
     assert r1 / an <= 1e-4  # FP32-level products with FP32 accumulation
     assert r1 <= 2.0 * r2  # FP64 on the next block's columns loses nothing
+
+
+@pytest.mark.parametrize("M,N,K", [(1000, 300, 256), (517, 33, 24), (129, 70, 5), (64, 20, 64)])
+def test_schur_update_against_torch(built, M, N, K):
+    """C -= A B on the DMMA kernel: within FP64 rounding of torch's product,
+    and bit-identical across tiles (each element accumulated in k order)."""
+    import delayed_pivoting as dp
+
+    torch = _torch()
+    g = torch.Generator(device="cuda").manual_seed(M * 7 + N)
+    lda, ldb, ldc = M + 3, K + 1, M + 5
+    A = torch.randn(K, lda, dtype=torch.float64, device="cuda", generator=g)  # column-major
+    B = torch.randn(N, ldb, dtype=torch.float64, device="cuda", generator=g)
+    C0 = torch.randn(N, ldc, dtype=torch.float64, device="cuda", generator=g)
+    ref = C0[:, :M].T - A[:, :M].T @ B[:, :K].T
+    outs = []
+    prev = dp.gemm_tile(0)
+    try:
+        for tile in (1, 2):
+            dp.gemm_tile(tile)
+            C = C0.clone()
+            torch.cuda.synchronize()
+            assert dp.schur_update_device(M, N, K, A, lda, B, ldb, C, ldc) == 0
+            torch.cuda.synchronize()
+            assert torch.equal(C[:, M:], C0[:, M:])  # rows beyond M untouched
+            outs.append(C[:, :M].T.clone())
+    finally:
+        dp.gemm_tile(prev)
+    err = (outs[0] - ref).abs().max().item()
+    assert err <= 1e-13 * K * max(1.0, ref.abs().max().item())
+    assert torch.equal(outs[0], outs[1])
 
 
 @pytest.mark.slow
