@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=16384)
     ap.add_argument("--nb", type=int, default=64)
+    ap.add_argument("--nb-outer", type=int, default=0,
+                    help="LU outer block width (0: the library's default)")
     ap.add_argument("--lookahead", type=int, default=0, choices=[0, 1, 2],
                     help="LU trailing-update schedule: 0 automatic, 1 two streams, 2 one stream")
     ap.add_argument("--seed", type=int, default=16384)
@@ -269,7 +271,8 @@ def run_lu(args):
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         st, info = dp.getrf_device_ex(n, n, work, n, ipiv, jpiv, stream=stream, nb=args.nb,
-                                      precision=prec, lookahead=args.lookahead)
+                                      nb_outer=args.nb_outer, precision=prec,
+                                      lookahead=args.lookahead)
         e1.record(stream)
         if st != 0:
             raise RuntimeError(dp.delayed_getrf_cuda_status_string(st))
@@ -285,9 +288,16 @@ def run_lu(args):
 
     import ctypes
 
+    # Timed steps record device time for the trailing-update GEMM family
+    # only (the roofline kernel); every family is timed in one extra step.
+    g = 7 if prec != dp.PRECISION_FP64 else 3  # DP_KFAM_GEMM_MIXED / DP_KFAM_GEMM
+    L.dp_stats_families.restype = ctypes.c_uint
+    L.dp_stats_families.argtypes = [ctypes.c_uint]
     L.dp_stats_reset()
+    L.dp_stats_families(1 << g)
     L.dp_stats_enable(1)
     events = []
+    l0 = L.dp_kernel_launches()
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         if dist:
@@ -297,6 +307,7 @@ def run_lu(args):
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
+    launches = L.dp_kernel_launches() - l0
     L.dp_stats_enable(0)
     ms = sum(e0.elapsed_time(e1) for e0, e1, _ in events)
     info = events[-1][2]
@@ -304,9 +315,15 @@ def run_lu(args):
         t = torch.tensor([ms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-
     stats = _stats(L)
-    launches_per_step = sum(stats["launches"]) / max(args.steps, 1)
+    launches_per_step = launches / max(args.steps, 1)
+    L.dp_stats_reset()
+    L.dp_stats_families(0xFFFFFFFF)
+    L.dp_stats_enable(1)
+    step()
+    torch.cuda.synchronize()
+    L.dp_stats_enable(0)
+    fam_stats = _stats(L)
 
     # e2e: host buffers through the host-memory entry point (H2D + LU + D2H).
     e2e = None
@@ -340,16 +357,26 @@ def run_lu(args):
 
     peaks = measured_peaks()
     fp64 = fp64_peak_tflops(torch, dev)
-    g = 3  # DP_KFAM_GEMM
     gemm_ms = stats["ms"][g]
     gemm_tf = stats["flops"][g] / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else 0.0
-    roofline = {"bound": "tensor", "kernel": "dgemm_minus_kernel (FP64 DMMA m16n8k4)",
-                "achieved": gemm_tf, "peak": fp64, "unit": "TFLOP/s",
-                "frac": gemm_tf / fp64 if fp64 else None,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured live (FP64 is not in MEASURED_PEAKS.json)",
-                "traffic": None,
-                "per_launch_flops": stats["flops"][g] / max(stats["launches"][g], 1),
-                "avg_launch_ms": gemm_ms / max(stats["launches"][g], 1)}
+    if g == 3:
+        roofline = {"bound": "tensor", "kernel": "dgemm_minus_kernel (FP64 DMMA m16n8k4)",
+                    "achieved": gemm_tf, "peak": fp64, "unit": "TFLOP/s",
+                    "frac": gemm_tf / fp64 if fp64 else None,
+                    "peak_source": "cuBLAS DGEMM 8192^3 measured live (FP64 is not in "
+                                   "MEASURED_PEAKS.json)"}
+    else:
+        terms = 6 if prec == dp.PRECISION_MIXED_BF16X6 else 3
+        bf16 = peaks.get("bf16_tflops_sustained") or peaks.get("bf16_tflops")
+        roofline = {"bound": "tensor", "kernel": f"gemm_bf16x3_kernel (tcgen05, {terms} products)",
+                    "achieved": terms * gemm_tf, "peak": bf16, "unit": "TFLOP/s",
+                    "frac": terms * gemm_tf / bf16 if bf16 else None,
+                    "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (measured)",
+                    "algorithmic_fp64_tflops": gemm_tf}
+    roofline.update({"traffic": None,
+                     "per_launch_flops": stats["flops"][g] / max(stats["launches"][g], 1),
+                     "avg_launch_ms": gemm_ms / max(stats["launches"][g], 1),
+                     "launches_timed": stats["launches"][g]})
 
     value = world * flops(n) * args.steps / (ms * 1e-3) / 1e9
     cpu = None
@@ -360,26 +387,30 @@ def run_lu(args):
                "sample": f"one delayed_getrf of n={args.cpu_n} (same generator, 0.1%/0.02% "
                          f"planted columns), {t_cpu:.2f} s, OpenBLAS {threads} threads"}
     if rank == 0:
+        # one extra step with every family timed (events on both streams:
+        # with look-ahead the families overlap, so shares add up past 1)
         fam = ["panel", "laswp", "trsm", "gemm", "search", "swap", "other", "gemm_mixed"]
         kern = {}
+        fs = fam_stats
         for i, nm in enumerate(fam):
-            if stats["launches"][i] == 0:
+            if fs["launches"][i] == 0:
                 continue
-            t = stats["ms"][i] / args.steps
-            kern[nm] = {"ms_per_step": t, "launches_per_step": stats["launches"][i] / args.steps,
-                        "share": stats["ms"][i] / max(ms / world, 1e-9)}
-            if stats["flops"][i]:
-                kern[nm]["tflops"] = stats["flops"][i] / (stats["ms"][i] * 1e-3) / 1e12
-            if stats["bytes"][i]:
-                kern[nm]["gbs"] = stats["bytes"][i] / (stats["ms"][i] * 1e-3) / 1e9
+            kern[nm] = {"ms_per_step": fs["ms"][i], "launches_per_step": fs["launches"][i],
+                        "share": fs["ms"][i] / max(ms / args.steps, 1e-9)}
+            if fs["flops"][i]:
+                kern[nm]["tflops"] = fs["flops"][i] / (fs["ms"][i] * 1e-3) / 1e12
+            if fs["bytes"][i]:
+                kern[nm]["gbs"] = fs["bytes"][i] / (fs["ms"][i] * 1e-3) / 1e9
         line = {
             "metric": lu_metric(n), "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": f"synthetic: N(0,1) MT19937-64 seeded per rank, {w['n_tiny']} tiny (x1e-18) + "
                     f"{w['n_zero']} zero columns",
-            "config": {"workload": f"delayed_getrf plain FP64 n={n} (single matrix)", "n": n,
-                       "nb": args.nb, "parallelism": f"replicas x{world}",
+            "config": {"workload": f"delayed_getrf {args.precision} n={n} (single matrix)", "n": n,
+                       "nb": args.nb, "nb_outer": args.nb_outer or 256,
+                       "lookahead": {0: "auto", 1: "on", 2: "off"}[args.lookahead],
+                       "parallelism": f"replicas x{world}",
                        "l2": f"input {8 * n * n / 2**30:.2f} GiB " + (
                            "> L2 (no flush needed)" if 8 * n * n > 126e6 else "<= L2"), "info": info},
             "roofline": roofline,

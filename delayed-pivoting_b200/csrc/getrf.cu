@@ -250,6 +250,7 @@ int read_state(State& hs, const Workspace& ws, cudaStream_t st) {
 std::mutex g_stats_mutex;
 dp_kernel_stats g_stats;
 bool g_stats_on = false;
+unsigned g_stats_mask = ~0u;  // kernel families recorded while enabled
 
 // Events are recycled across calls (creating them per launch costs more
 // host time than the launches themselves).  Guarded by g_stats_mutex.
@@ -292,6 +293,7 @@ struct Recorder {
     int launches;
   };
   bool on = false;
+  unsigned mask = ~0u;
   cudaStream_t st = nullptr;
   std::vector<Mark> marks;
   int cur = -1;
@@ -300,9 +302,11 @@ struct Recorder {
   explicit Recorder(cudaStream_t s) : st(s) {
     std::lock_guard<std::mutex> lock(g_stats_mutex);
     on = g_stats_on;
+    mask = g_stats_mask;
   }
   void begin(int fam) {
-    if (!on) return;
+    cur = -1;
+    if (!on || !(mask >> fam & 1u)) return;
     Mark mk{fam, nullptr, nullptr, 0.0, 0.0, 0};
     mk.e0 = event_get();
     mk.e1 = event_get();
@@ -1075,6 +1079,13 @@ int dp_getrf_hybrid_host(int m, int n, double* a, int lda, int* ipiv, int* jpiv,
 void dp_stats_enable(int on) {
   std::lock_guard<std::mutex> lock(dp::g_stats_mutex);
   dp::g_stats_on = on != 0;
+}
+
+unsigned dp_stats_families(unsigned mask) {
+  std::lock_guard<std::mutex> lock(dp::g_stats_mutex);
+  const unsigned prev = dp::g_stats_mask;
+  dp::g_stats_mask = mask;
+  return prev;
 }
 
 void dp_stats_reset(void) {

@@ -301,6 +301,10 @@ typedef struct dp_kernel_stats {
   long long calls;
 } dp_kernel_stats;
 void dp_stats_enable(int on);
+/* Families recorded while enabled: bit DP_KFAM_x set (default all, ~0u);
+ * fewer families mean fewer timing events inside the timed work.  Returns
+ * the previous mask. */
+unsigned dp_stats_families(unsigned mask);
 void dp_stats_reset(void);
 void dp_stats_get(dp_kernel_stats *out);
 
