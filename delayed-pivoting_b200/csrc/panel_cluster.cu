@@ -36,6 +36,8 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kSub = 8;  // sub-panel width
+constexpr int kMaxW = 128;  // widest panel (the TRSM's limit)
+constexpr int kPushPer = (kMaxW + 1 + 31) / 32;  // pushed row elements per lane
 
 struct __align__(16) CandSlot {
   double val;
@@ -64,6 +66,16 @@ __device__ __forceinline__ void warp_best(double v, int row, double& bv, int& br
   const int key = (hi == mhi && lo == mlo) ? row : 0x7fffffff;
   brow = __reduce_min_sync(0xffffffffu, key);
   bv = __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
+}
+
+// 8-byte asynchronous global -> shared copy (L1-allocating), and the wait
+// for every copy this thread issued.
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 __device__ __forceinline__ LocalBest warp_lb(LocalBest v) {
@@ -105,11 +117,13 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
   int* orig = reinterpret_cast<int*>(psave + (size_t)kSub * W1);
   __shared__ LocalBest red[kThreads / 32];
 
+  // the slice arrives by asynchronous copies, all in flight at once
   for (int c = 0; c < w; ++c) {
     const double* src = p.a + idx(row0, p.begin + c, p.lda);
-    for (int r = tid; r < rows_here; r += blockDim.x) sm[(size_t)c * RP + r] = src[r];
+    for (int r = tid; r < rows_here; r += blockDim.x) cp_async8(sm + (size_t)c * RP + r, src + r);
   }
   for (int r = tid; r < rows_here; r += blockDim.x) orig[r] = (int)(row0 + r);
+  cp_async_wait_all();
   if (rank == 0 && tid == 0) {
     p.state->stop_k = -1;
     p.state->swap_count = 0;
@@ -130,52 +144,65 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
   }
 
   // End of a sub-panel that executed kd steps at [base, base + kd): solve its
-  // pivot rows for the columns [send, w) and update the rows below; then
-  // the candidate of column send (unless the panel stopped).
+  // pivot rows for the columns [send, w), give them to the pivot rows held
+  // here and update the rows below; each updating thread also finds its
+  // candidate of column send (the next step's search, rows below the last
+  // pivot only).  Called with kd = 0 only when the panel stops.
   auto sub_panel_end = [&](int kd, int base, int send) {
     __syncthreads();  // psave complete, this CTA's rows updated
-    if (kd > 0) {
-      for (int c = send + tid; c < w; c += blockDim.x)
-        for (int j = 1; j < kd; ++j) {
-          double u = psave[(size_t)j * W1 + c];
-          for (int t = 0; t < j; ++t)
-            u -= psave[(size_t)j * W1 + base + t] * psave[(size_t)t * W1 + c];
-          psave[(size_t)j * W1 + c] = u;
-        }
-      __syncthreads();
-      const long long first = (long long)p.begin + base;  // global row of the first pivot
-      for (int r = tid; r < rows_here; r += blockDim.x) {
-        const long long g = row0 + r;
-        double* __restrict__ row = sm + r;
-        if (g < first) continue;
-        if (g < first + kd) {
-          const double* u = psave + (size_t)(g - first) * W1;
-          for (int c = send; c < w; ++c) row[(size_t)c * RP] = u[c];
-          continue;
-        }
-        double l[kSub];
+    mine = LocalBest{0.0, -1, 0};
+    if (kd == 0) return;
+    // U12 = L11^{-1} A12 of the sub-panel, one column per thread, in registers
+    for (int c = send + tid; c < w; c += blockDim.x) {
+      double u[kSub];
 #pragma unroll
-        for (int t = 0; t < kSub; ++t) l[t] = t < kd ? row[(size_t)(base + t) * RP] : 0.0;
-        for (int c = send; c < w; ++c) {
-          double x = row[(size_t)c * RP];
+      for (int j = 0; j < kSub; ++j) u[j] = j < kd ? psave[(size_t)j * W1 + c] : 0.0;
 #pragma unroll
-          for (int t = 0; t < kSub; ++t)
-            if (t < kd) x = fma(-l[t], psave[(size_t)t * W1 + c], x);
-          row[(size_t)c * RP] = x;
+      for (int j = 1; j < kSub; ++j) {
+        if (j < kd) {
+#pragma unroll
+          for (int t = 0; t < j; ++t) u[j] = fma(-psave[(size_t)j * W1 + base + t], u[t], u[j]);
+          psave[(size_t)j * W1 + c] = u[j];
         }
       }
     }
     __syncthreads();
-    mine = LocalBest{0.0, -1, 0};
-    if (send < w) {
-      const long long last = (long long)p.begin + base + kd - 1;  // last pivot row
-      for (int r = tid; r < rows_here; r += blockDim.x) {
-        if (row0 + r <= last) continue;
-        const double v = fabs(sm[(size_t)send * RP + r]);
-        if (v > mine.val) {
-          mine.val = v;
+    const long long first = (long long)p.begin + base;  // global row of the first pivot
+    const int ncol = w - send;
+    // the solved rows to the pivot rows of this CTA, spread over the threads
+    for (int e = tid; e < kd * ncol; e += blockDim.x) {
+      const int j = e / ncol, c = send + (e - j * ncol);
+      const long long g = first + j;
+      if (g >= row0 && g < row0 + rows_here) sm[(size_t)c * RP + (g - row0)] = psave[(size_t)j * W1 + c];
+    }
+    const double* __restrict__ ps = psave;
+    for (int r = tid; r < rows_here; r += blockDim.x) {
+      const long long g = row0 + r;
+      if (g < first + kd) continue;
+      double* __restrict__ row = sm + r;
+      double l[kSub];
+#pragma unroll
+      for (int t = 0; t < kSub; ++t) l[t] = t < kd ? row[(size_t)(base + t) * RP] : 0.0;
+      {
+        // column send first: the next step's candidate
+        double x = row[(size_t)send * RP];
+#pragma unroll
+        for (int t = 0; t < kSub; ++t)
+          if (t < kd) x = fma(-l[t], ps[(size_t)t * W1 + send], x);
+        row[(size_t)send * RP] = x;
+        const double av = fabs(x);
+        if (av > mine.val) {
+          mine.val = av;
           mine.row = r;
         }
+      }
+#pragma unroll 4
+      for (int c = send + 1; c < w; ++c) {
+        double x = row[(size_t)c * RP];
+#pragma unroll
+        for (int t = 0; t < kSub; ++t)
+          if (t < kd) x = fma(-l[t], ps[(size_t)t * W1 + c], x);
+        row[(size_t)c * RP] = x;
       }
     }
   };
@@ -202,18 +229,29 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
       double* my_stc = stc + ((size_t)par * 16 + rank) * W1;
       double* my_stk = stk + (size_t)par * W1;
       // warp w pushes to CTAs w, w + nwarps, ...; its lanes walk the row
-      if (cb.row >= 0 || own_k) {
-        for (int dest = warp; dest < C; dest += nwarps)
-          for (int j = lane; j < W1; j += 32) {
-            if (cb.row >= 0) {
-              const double v = j < w ? sm[(size_t)j * RP + cb.row] : (double)orig[cb.row];
-              *cluster.map_shared_rank(my_stc + j, dest) = v;
-            }
-            if (own_k) {
-              const double v = j < w ? sm[(size_t)j * RP + kl] : (double)orig[kl];
-              *cluster.map_shared_rank(my_stk + j, dest) = v;
+      // each lane reads its elements of both rows once, then stores them
+      // to every destination of its warp
+      if (warp < C && (cb.row >= 0 || own_k)) {
+        double cv[kPushPer], kv[kPushPer];
+#pragma unroll
+        for (int u = 0; u < kPushPer; ++u) {
+          const int j = lane + 32 * u;
+          cv[u] = (cb.row >= 0 && j < W1) ? (j < w ? sm[(size_t)j * RP + cb.row] : (double)orig[cb.row])
+                                          : 0.0;
+          kv[u] = (own_k && j < W1) ? (j < w ? sm[(size_t)j * RP + kl] : (double)orig[kl]) : 0.0;
+        }
+        for (int dest = warp; dest < C; dest += nwarps) {
+          double* rc = cluster.map_shared_rank(my_stc, dest);
+          double* rk = cluster.map_shared_rank(my_stk, dest);
+#pragma unroll
+          for (int u = 0; u < kPushPer; ++u) {
+            const int j = lane + 32 * u;
+            if (j < W1) {
+              if (cb.row >= 0) rc[j] = cv[u];
+              if (own_k) rk[j] = kv[u];
             }
           }
+        }
       }
       if (tid < C) {
         CandSlot cs;
@@ -260,31 +298,51 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
     const int base = (s / kSub) * kSub, send = min(base + kSub, w);
     for (int j = tid; j < W1; j += blockDim.x) psave[(size_t)(s - base) * W1 + j] = pr[j];
 
-    // 4. Swap, scale, update own rows; next column's candidate on the way.
+    // 4. Row k takes the pivot row and row pl row k's old content (columns
+    //    outside [s, send): the updating thread writes those), spread over
+    //    the threads; then every thread swaps, scales and updates its own
+    //    rows, reading row pl's old values from the pushed row k.  The next
+    //    column's candidate is on the way.
+    if (own_k)
+      for (int j = tid; j < W1; j += blockDim.x) {
+        if (j < w) sm[(size_t)j * RP + kl] = pr[j];
+        else orig[kl] = (int)pr[w];
+      }
+    if (swap_p)
+      for (int j = tid; j < W1; j += blockDim.x) {
+        if (j < w) {
+          if (j < s || j >= send) sm[(size_t)j * RP + pl] = kr[j];
+        } else {
+          orig[pl] = (int)kr[w];
+        }
+      }
     const double inv = win.inv;
+    double pv[kSub];  // pivot row over the sub-panel's columns [s, send)
+    pv[0] = 0.0;
+#pragma unroll
+    for (int t = 1; t < kSub; ++t) pv[t] = s + t < send ? pr[s + t] : 0.0;
     mine = LocalBest{0.0, -1, 0};
-    for (int r = max(0, kl) + tid; r < rows_here; r += blockDim.x) {
+    for (int r = max(0, kl + 1) + tid; r < rows_here; r += blockDim.x) {
       double* __restrict__ row = sm + r;
-      if (r == kl) {
-        for (int j = 0; j < w; ++j) row[(size_t)j * RP] = pr[j];
-        orig[r] = (int)pr[w];
-        continue;
-      }
-      if (swap_p && r == pl) {
-        for (int j = 0; j < w; ++j) row[(size_t)j * RP] = kr[j];
-        orig[r] = (int)kr[w];
-      }
-      const double l = row[(size_t)s * RP] * inv;
+      const bool from_k = swap_p && r == pl;
+      double x[kSub];
+#pragma unroll
+      for (int t = 0; t < kSub; ++t)
+        x[t] = s + t < send ? (from_k ? kr[s + t] : row[(size_t)(s + t) * RP]) : 0.0;
+      const double l = x[0] * inv;
       row[(size_t)s * RP] = l;
-      if (s + 1 < send) {  // columns past the sub-panel wait for its rank-kSub update
-        const double v = row[(size_t)(s + 1) * RP] - l * pr[s + 1];
-        row[(size_t)(s + 1) * RP] = v;
-        const double av = fabs(v);
+#pragma unroll
+      for (int t = 1; t < kSub; ++t)
+        if (s + t < send) {  // columns past the sub-panel wait for its rank-kSub update
+          x[t] = fma(-l, pv[t], x[t]);
+          row[(size_t)(s + t) * RP] = x[t];
+        }
+      if (s + 1 < send) {
+        const double av = fabs(x[1]);
         if (av > mine.val) {
           mine.val = av;
           mine.row = r;
         }
-        for (int j = s + 2; j < send; ++j) row[(size_t)j * RP] -= l * pr[j];
       }
     }
     if (s + 1 == send && send < w) sub_panel_end(s + 1 - base, base, send);
@@ -293,22 +351,36 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
   // back, and no CTA may exit while a peer could still push into it.
   cluster.sync();
 
+#pragma unroll 4
   for (int c = 0; c < w; ++c) {
     double* dst = p.a + idx(row0, p.begin + c, p.lda);
     for (int r = tid; r < rows_here; r += blockDim.x) dst[r] = sm[(size_t)c * RP + r];
   }
-  for (int r = tid; r < rows_here; r += blockDim.x) {
+  // Swap lists: whole warps walk the rows together, so that the moved rows
+  // below the block take their slots with one atomic per warp.
+  int changed = 0;
+  for (int r0w = warp * 32; r0w < rows_here; r0w += blockDim.x) {
+    const int r = r0w + lane;
     const long long g = row0 + r;
-    const int src = orig[r];
-    if (g < p.end) {
+    const int src = r < rows_here ? orig[r] : (int)g;
+    if (r < rows_here && g < p.end) {
       p.swap_block[g - p.begin] = src;
-      if (src != (int)g) atomicAdd(&p.state->block_changed, 1);
-    } else if (src != (int)g) {
-      const int slot = atomicAdd(&p.state->swap_count, 1);
-      p.swap_extra[2 * slot + 0] = (int)g;
-      p.swap_extra[2 * slot + 1] = src;
+      changed += src != (int)g;
+    }
+    const bool moved = r < rows_here && g >= p.end && src != (int)g;
+    const unsigned bal = __ballot_sync(0xffffffffu, moved);
+    if (bal) {
+      int slot = 0;
+      if (lane == 0) slot = atomicAdd(&p.state->swap_count, __popc(bal));
+      slot = __shfl_sync(0xffffffffu, slot, 0) + __popc(bal & ((1u << lane) - 1u));
+      if (moved) {
+        p.swap_extra[2 * slot + 0] = (int)g;
+        p.swap_extra[2 * slot + 1] = src;
+      }
     }
   }
+  changed = __reduce_add_sync(0xffffffffu, changed);
+  if (lane == 0 && changed) atomicAdd(&p.state->block_changed, changed);
 }
 
 size_t panel_cluster_smem_bytes(int w, int rows_per_cta) {
