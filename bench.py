@@ -103,6 +103,12 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi's start-up (NVML initialisation) can hold driver
+            # locks for ~100 ms: let it reach its first sample before the
+            # caller's timed region begins
+            deadline = time.time() + 3.0
+            while not self.lines and time.time() < deadline and self.proc.poll() is None:
+                time.sleep(0.01)
         except OSError:
             self.proc = None
         return self

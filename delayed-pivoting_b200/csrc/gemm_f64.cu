@@ -212,7 +212,18 @@ using Half = Cfg<128, 64, 16, 4, 2, 2, 2>;
 // tiles, 4 warps of 16 x 32, two CTAs per SM, so M / 64 CTAs stream A.
 using Skinny = Cfg<64, 32, 32, 4, 4, 1, 2>;
 
-std::atomic<int> g_tile{0};  // 0 automatic, 1 Big, 2 Half
+// 64 x 64 tiles, 4 warps of 32 x 32, three CTAs per SM (57 KB of stages).
+using Small = Cfg<64, 64, 16, 3, 2, 2, 3>;
+// The same tile with two stages and four CTAs per SM (at most 128
+// registers; 16 warps per SM hide the shallow pipeline): the fastest
+// measured on B200 at every update shape of the LU, so the automatic choice.
+// 16384 x 16384 updates: 29.6 TF/s at K = 256 and 24.2 at K = 64 (three-
+// stage 64 x 64: 29.1 / 21.8; 128 x 64: 26.4 / 18.3; cuBLAS DGEMM 32.7 / 20.8).
+using Small4 = Cfg<64, 64, 16, 2, 2, 2, 4>;
+// 128 x 64 tiles as Half with 8 warps of 32 x 32: 16 warps per SM.
+using HalfW8 = Cfg<128, 64, 16, 4, 4, 2, 2>;
+
+std::atomic<int> g_tile{0};  // 0 automatic (Small4), 1 Big, 2 Half, 3 Small, 4 HalfW8, 5 Small4
 
 }  // namespace gemm
 
@@ -227,8 +238,14 @@ void launch_gemm_minus(int M, int N, int K, const double* A, long long lda, cons
     gemm::launch<gemm::Skinny>(M, N, K, A, lda, B, ldb, C, ldc, s, gate);
   else if (tile == 1)
     gemm::launch<gemm::Big>(M, N, K, A, lda, B, ldb, C, ldc, s, gate);
-  else
+  else if (tile == 2)
     gemm::launch<gemm::Half>(M, N, K, A, lda, B, ldb, C, ldc, s, gate);
+  else if (tile == 3)
+    gemm::launch<gemm::Small>(M, N, K, A, lda, B, ldb, C, ldc, s, gate);
+  else if (tile == 4)
+    gemm::launch<gemm::HalfW8>(M, N, K, A, lda, B, ldb, C, ldc, s, gate);
+  else
+    gemm::launch<gemm::Small4>(M, N, K, A, lda, B, ldb, C, ldc, s, gate);
 }
 
 }  // namespace dp
@@ -245,7 +262,7 @@ int dp_schur_update_device(int M, int N, int K, const double* A, int lda, const 
 }
 
 int dp_gemm_tile(int tile) {
-  if (tile < 0 || tile > 2) return -1;
+  if (tile < 0 || tile > 5) return -1;
   return dp::gemm::g_tile.exchange(tile);
 }
 

@@ -338,7 +338,10 @@ def schur_update_device(M, N, K, d_a, lda, d_b, ldb, d_c, ldc, stream=None):
 
 
 def gemm_tile(tile: int) -> int:
-    """dp_gemm_tile: 0 automatic, 1 128 x 128, 2 128 x 64.  Returns the previous setting."""
+    """dp_gemm_tile: 0 automatic (= 5), 1 128 x 128, 2 128 x 64, 3 64 x 64, 4 128 x 64
+    (8 warps), 5 64 x 64 (two stages).
+
+    Returns the previous setting."""
     return lib().dp_gemm_tile(int(tile))
 
 

@@ -216,7 +216,9 @@ int dp_batch_tune_load(const char *path, dp_batch_options *opt);
 typedef struct dp_server_options {
   unsigned long long budget_bytes; /* HBM admission budget (0: 160 GB) */
   int precision;       /* DP_PRECISION_* of the blocked factorisations (default: MIXED_BF16X6) */
-  int large_workers;   /* concurrent blocked factorisations (streams); 0: 6 */
+  int large_workers;   /* concurrent blocked factorisations (streams); 0: automatic -
+                          14 for the mixed precisions (refinement solves gain from
+                          more overlap), 6 for FP64 (more contend in the updates) */
   int small_max_n;     /* orders up to this take the batched path (<= DP_BATCH_MAX_N); 0: 512,
                           -1: none */
   int small_max_batch; /* requests per batched launch; 0: 2048 */
@@ -321,7 +323,9 @@ int dp_schur_update_device(int M, int N, int K, const double *A, int lda, const 
                            int ldb, double *C, int ldc, void *stream);
 
 /* Tile of that kernel for N > 32 (tuning; no result bit depends on it):
- * 0 automatic, 1 128 x 128 (one CTA per SM), 2 128 x 64 (two CTAs per SM).
+ * 0 automatic (= 5), 1 128 x 128 (one CTA per SM), 2 128 x 64 (two CTAs per
+ * SM), 3 64 x 64 (three CTAs per SM), 4 128 x 64 with eight warps, 5 64 x 64
+ * with two stages (four CTAs per SM).
  * Returns the previous setting, or -1 for an invalid one. */
 int dp_gemm_tile(int tile);
 

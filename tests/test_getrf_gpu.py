@@ -209,7 +209,7 @@ def test_schur_update_against_torch(built, M, N, K):
     outs = []
     prev = dp.gemm_tile(0)
     try:
-        for tile in (1, 2):
+        for tile in (1, 2, 3, 4, 5):
             dp.gemm_tile(tile)
             C = C0.clone()
             torch.cuda.synchronize()
@@ -221,7 +221,8 @@ def test_schur_update_against_torch(built, M, N, K):
         dp.gemm_tile(prev)
     err = (outs[0] - ref).abs().max().item()
     assert err <= 1e-13 * K * max(1.0, ref.abs().max().item())
-    assert torch.equal(outs[0], outs[1])
+    for o in outs[1:]:
+        assert torch.equal(outs[0], o)
 
 
 @pytest.mark.slow
