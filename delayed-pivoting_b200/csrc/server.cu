@@ -625,7 +625,7 @@ void dp_server_options_init(dp_server_options* o) {
   std::memset(o, 0, sizeof(*o));
   o->budget_bytes = 160ull << 30;
   o->precision = DP_PRECISION_MIXED_BF16X6;
-  o->large_workers = 0;  // automatic: decided by the precision at creation
+  o->large_workers = 6;
   o->small_max_n = DP_BATCH_MAX_N;
   o->small_max_batch = 2048;
   o->max_iter = 10;
@@ -647,13 +647,7 @@ int dp_server_create(dp_server** out, const dp_server_options* opt) {
     if (o.max_iter == 0) o.max_iter = 10;
     if (o.tol == 0.0) o.tol = 1e-14;
   }
-  if (o.large_workers == 0) {
-    // Measured on B200, 400-request stream of orders 64..8192: the mixed
-    // server gains up to 14 workers (218 -> 259 solves/s from 6 to 14: its
-    // refinement solves are latency bound and overlap), the FP64 server
-    // loses beyond 6 (470 -> 391: concurrent updates contend).
-    o.large_workers = o.precision == DP_PRECISION_FP64 ? 6 : 14;
-  }
+  if (o.large_workers == 0) o.large_workers = 6;
   if (!dp::valid_precision(o.precision) ||
       o.large_workers < 1 || o.large_workers > 64 || o.small_max_n > DP_BATCH_MAX_N ||
       o.small_max_batch < 1 || o.max_iter < 0 || !(o.tol > 0.0))

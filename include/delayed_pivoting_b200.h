@@ -216,9 +216,7 @@ int dp_batch_tune_load(const char *path, dp_batch_options *opt);
 typedef struct dp_server_options {
   unsigned long long budget_bytes; /* HBM admission budget (0: 160 GB) */
   int precision;       /* DP_PRECISION_* of the blocked factorisations (default: MIXED_BF16X6) */
-  int large_workers;   /* concurrent blocked factorisations (streams); 0: automatic -
-                          14 for the mixed precisions (refinement solves gain from
-                          more overlap), 6 for FP64 (more contend in the updates) */
+  int large_workers;   /* concurrent blocked factorisations (streams); 0: 6 */
   int small_max_n;     /* orders up to this take the batched path (<= DP_BATCH_MAX_N); 0: 512,
                           -1: none */
   int small_max_batch; /* requests per batched launch; 0: 2048 */
