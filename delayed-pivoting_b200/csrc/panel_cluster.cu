@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
   // the slice arrives by asynchronous copies, all in flight at once
   for (int c = 0; c < w; ++c) {
     const double* src = p.a + idx(row0, p.begin + c, p.lda);
-    for (int r = tid; r < rows_here; r += blockDim.x) cp_async8(sm + (size_t)c * RP + r, src + r);
+    for (int r = tid; r < rows_here; r += blockDim.x) cp_async8(sm + c * RP + r, src + r);
   }
   for (int r = tid; r < rows_here; r += blockDim.x) orig[r] = (int)(row0 + r);
   cp_async_wait_all();
@@ -156,13 +156,13 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
     for (int c = send + tid; c < w; c += blockDim.x) {
       double u[kSub];
 #pragma unroll
-      for (int j = 0; j < kSub; ++j) u[j] = j < kd ? psave[(size_t)j * W1 + c] : 0.0;
+      for (int j = 0; j < kSub; ++j) u[j] = j < kd ? psave[j * W1 + c] : 0.0;
 #pragma unroll
       for (int j = 1; j < kSub; ++j) {
         if (j < kd) {
 #pragma unroll
-          for (int t = 0; t < j; ++t) u[j] = fma(-psave[(size_t)j * W1 + base + t], u[t], u[j]);
-          psave[(size_t)j * W1 + c] = u[j];
+          for (int t = 0; t < j; ++t) u[j] = fma(-psave[j * W1 + base + t], u[t], u[j]);
+          psave[j * W1 + c] = u[j];
         }
       }
     }
@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
     for (int e = tid; e < kd * ncol; e += blockDim.x) {
       const int j = e / ncol, c = send + (e - j * ncol);
       const long long g = first + j;
-      if (g >= row0 && g < row0 + rows_here) sm[(size_t)c * RP + (g - row0)] = psave[(size_t)j * W1 + c];
+      if (g >= row0 && g < row0 + rows_here) sm[c * RP + (int)(g - row0)] = psave[j * W1 + c];
     }
     const double* __restrict__ ps = psave;
     for (int r = tid; r < rows_here; r += blockDim.x) {
@@ -182,14 +182,14 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
       double* __restrict__ row = sm + r;
       double l[kSub];
 #pragma unroll
-      for (int t = 0; t < kSub; ++t) l[t] = t < kd ? row[(size_t)(base + t) * RP] : 0.0;
+      for (int t = 0; t < kSub; ++t) l[t] = t < kd ? row[(base + t) * RP] : 0.0;
       {
         // column send first: the next step's candidate
-        double x = row[(size_t)send * RP];
+        double x = row[send * RP];
 #pragma unroll
         for (int t = 0; t < kSub; ++t)
-          if (t < kd) x = fma(-l[t], ps[(size_t)t * W1 + send], x);
-        row[(size_t)send * RP] = x;
+          if (t < kd) x = fma(-l[t], ps[t * W1 + send], x);
+        row[send * RP] = x;
         const double av = fabs(x);
         if (av > mine.val) {
           mine.val = av;
@@ -198,11 +198,11 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
       }
 #pragma unroll 4
       for (int c = send + 1; c < w; ++c) {
-        double x = row[(size_t)c * RP];
+        double x = row[c * RP];
 #pragma unroll
         for (int t = 0; t < kSub; ++t)
-          if (t < kd) x = fma(-l[t], ps[(size_t)t * W1 + c], x);
-        row[(size_t)c * RP] = x;
+          if (t < kd) x = fma(-l[t], ps[t * W1 + c], x);
+        row[c * RP] = x;
       }
     }
   };
@@ -226,8 +226,8 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
 
     // 2. Push (value, row), the candidate row and row k into every CTA.
     {
-      double* my_stc = stc + ((size_t)par * 16 + rank) * W1;
-      double* my_stk = stk + (size_t)par * W1;
+      double* my_stc = stc + (par * 16 + rank) * W1;
+      double* my_stk = stk + par * W1;
       // warp w pushes to CTAs w, w + nwarps, ...; its lanes walk the row
       // each lane reads its elements of both rows once, then stores them
       // to every destination of its warp
@@ -236,9 +236,9 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
 #pragma unroll
         for (int u = 0; u < kPushPer; ++u) {
           const int j = lane + 32 * u;
-          cv[u] = (cb.row >= 0 && j < W1) ? (j < w ? sm[(size_t)j * RP + cb.row] : (double)orig[cb.row])
+          cv[u] = (cb.row >= 0 && j < W1) ? (j < w ? sm[j * RP + cb.row] : (double)orig[cb.row])
                                           : 0.0;
-          kv[u] = (own_k && j < W1) ? (j < w ? sm[(size_t)j * RP + kl] : (double)orig[kl]) : 0.0;
+          kv[u] = (own_k && j < W1) ? (j < w ? sm[j * RP + kl] : (double)orig[kl]) : 0.0;
         }
         for (int dest = warp; dest < C; dest += nwarps) {
           double* rc = cluster.map_shared_rank(my_stc, dest);
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
         cs.val = cb.row >= 0 ? cb.val : 0.0;
         cs.row = cb.row >= 0 ? (int)(row0 + cb.row) : -1;
         cs.pad = 0;
-        cs.inv = cb.row >= 0 ? 1.0 / sm[(size_t)s * RP + cb.row] : 0.0;
+        cs.inv = cb.row >= 0 ? 1.0 / sm[s * RP + cb.row] : 0.0;
         cs.pad2 = 0.0;
         *cluster.map_shared_rank(cands + par * 16 + rank, tid) = cs;
       }
@@ -289,14 +289,14 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
       break;
     }
     const long long prow_g = win.row;
-    const int owner_p = (int)((prow_g - p.begin) / R);
-    const double* __restrict__ pr = stc + ((size_t)par * 16 + owner_p) * W1;
-    const double* __restrict__ kr = stk + (size_t)par * W1;
+    const int owner_p = (int)(prow_g - p.begin) / R;
+    const double* __restrict__ pr = stc + (par * 16 + owner_p) * W1;
+    const double* __restrict__ kr = stk + par * W1;
     const int pl = (int)(prow_g - row0);
     const bool swap_p = pl >= 0 && pl < rows_here && prow_g != k;
     if (rank == 0 && tid == 0 && !positioned) p.ipiv[k] = (int)prow_g;
     const int base = (s / kSub) * kSub, send = min(base + kSub, w);
-    for (int j = tid; j < W1; j += blockDim.x) psave[(size_t)(s - base) * W1 + j] = pr[j];
+    for (int j = tid; j < W1; j += blockDim.x) psave[(s - base) * W1 + j] = pr[j];
 
     // 4. Row k takes the pivot row and row pl row k's old content (columns
     //    outside [s, send): the updating thread writes those), spread over
@@ -305,13 +305,13 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
     //    column's candidate is on the way.
     if (own_k)
       for (int j = tid; j < W1; j += blockDim.x) {
-        if (j < w) sm[(size_t)j * RP + kl] = pr[j];
+        if (j < w) sm[j * RP + kl] = pr[j];
         else orig[kl] = (int)pr[w];
       }
     if (swap_p)
       for (int j = tid; j < W1; j += blockDim.x) {
         if (j < w) {
-          if (j < s || j >= send) sm[(size_t)j * RP + pl] = kr[j];
+          if (j < s || j >= send) sm[j * RP + pl] = kr[j];
         } else {
           orig[pl] = (int)kr[w];
         }
@@ -322,20 +322,23 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
 #pragma unroll
     for (int t = 1; t < kSub; ++t) pv[t] = s + t < send ? pr[s + t] : 0.0;
     mine = LocalBest{0.0, -1, 0};
+#pragma unroll 2
     for (int r = max(0, kl + 1) + tid; r < rows_here; r += blockDim.x) {
       double* __restrict__ row = sm + r;
       const bool from_k = swap_p && r == pl;
+      // row pl's old values are the pushed row k: one load per element either way
+      const double* __restrict__ xs = from_k ? kr + s : row + s * RP;
+      const int xstride = from_k ? 1 : RP;
       double x[kSub];
 #pragma unroll
-      for (int t = 0; t < kSub; ++t)
-        x[t] = s + t < send ? (from_k ? kr[s + t] : row[(size_t)(s + t) * RP]) : 0.0;
+      for (int t = 0; t < kSub; ++t) x[t] = s + t < send ? xs[t * xstride] : 0.0;
       const double l = x[0] * inv;
-      row[(size_t)s * RP] = l;
+      row[s * RP] = l;
 #pragma unroll
       for (int t = 1; t < kSub; ++t)
         if (s + t < send) {  // columns past the sub-panel wait for its rank-kSub update
           x[t] = fma(-l, pv[t], x[t]);
-          row[(size_t)(s + t) * RP] = x[t];
+          row[(s + t) * RP] = x[t];
         }
       if (s + 1 < send) {
         const double av = fabs(x[1]);
@@ -354,7 +357,7 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
 #pragma unroll 4
   for (int c = 0; c < w; ++c) {
     double* dst = p.a + idx(row0, p.begin + c, p.lda);
-    for (int r = tid; r < rows_here; r += blockDim.x) dst[r] = sm[(size_t)c * RP + r];
+    for (int r = tid; r < rows_here; r += blockDim.x) dst[r] = sm[c * RP + r];
   }
   // Swap lists: whole warps walk the rows together, so that the moved rows
   // below the block take their slots with one atomic per warp.
