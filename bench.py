@@ -196,6 +196,25 @@ def cpu_reference_gflops(n, seed, threads, repeats=1):
     return flops(n) / best / 1e9, best, kind, info
 
 
+def cpu_lapack_gflops(n, seed, threads):
+    """LAPACK dgetrf (OpenBLAS) through the reference's own wrapper
+    (delayed_lu/lapack_dgetrf.cpp) on the same matrix, on the host cores:
+    the partial-pivoting factorisation the delayed LU is compared with.
+    None when the reference's CPU build is absent."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import delayed_pivoting as dp
+    import oracle as orc
+
+    if not orc.ref_available():
+        return None
+    w = workload(n)
+    f = dp.planted_matrix(n, n, seed, w["n_tiny"], w["n_zero"]).copy(order="F")
+    t0 = time.perf_counter()
+    orc.ref_lapack_getrf(f, threads=threads)
+    t = time.perf_counter() - t0
+    return flops(n) / t / 1e9, t
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -398,6 +417,11 @@ def run_lu(args):
         cpu = {"value": g_cpu, "unit": UNIT, "cores": threads, "kind": kind,
                "sample": f"one delayed_getrf of n={args.cpu_n} (same generator, 0.1%/0.02% "
                          f"planted columns), {t_cpu:.2f} s, OpenBLAS {threads} threads"}
+        lap = cpu_lapack_gflops(args.cpu_n, args.seed, threads)
+        if lap is not None:
+            cpu["lapack_dgetrf"] = {"value": lap[0], "unit": UNIT, "cores": threads,
+                                    "sample": f"LAPACK dgetrf (OpenBLAS) of the same n={args.cpu_n} "
+                                              f"matrix, {lap[1]:.2f} s"}
     if rank == 0:
         # one extra step with every family timed (events on both streams:
         # with look-ahead the families overlap, so shares add up past 1)
