@@ -131,3 +131,30 @@ def test_empty_matrix(built):
     a = np.zeros((1, 1), order="F")
     _, _, info = orc.oracle_getrf(a, 0, 0)
     assert info == 0
+
+
+@pytest.mark.parametrize("seed", range(10))
+def test_oracle_matches_reference_on_exact_ties_and_rank_deficiency(built, seed):
+    """Small-integer matrices: eliminations stay exact, so columns tie in
+    magnitude (the first row wins, delayed_dgetrf.cpp:164-176 through idamax)
+    and become exactly zero part-way (the full-pivot fallback and the delayed
+    suffix, :183-218); duplicated columns force rank deficiency."""
+    import oracle as orc
+
+    if not orc.ref_available():
+        pytest.skip("reference CPU build not present")
+    rng = np.random.default_rng(500 + seed)
+    m = int(rng.integers(2, 40))
+    n = int(rng.integers(2, 40))
+    a = np.asfortranarray(rng.integers(-2, 3, size=(m, n)).astype(np.float64))
+    for _ in range(int(rng.integers(0, 3))):  # duplicated columns
+        a[:, int(rng.integers(0, n))] = a[:, int(rng.integers(0, n))]
+    for policy in (0, 1):
+        r = a.copy(order="F")
+        o = a.copy(order="F")
+        fn = orc.ref_getrf if policy == 0 else orc.ref_getrf_column
+        ri, rj, rinfo = fn(r, m, n)
+        oi, oj, oinfo = orc.oracle_getrf(o, m, n, policy=policy)  # the reference's nb = 64
+        assert rinfo == oinfo
+        np.testing.assert_array_equal(ri, oi)
+        np.testing.assert_array_equal(rj, oj)
