@@ -422,6 +422,15 @@ def run_lu(args):
             cpu["lapack_dgetrf"] = {"value": lap[0], "unit": UNIT, "cores": threads,
                                     "sample": f"LAPACK dgetrf (OpenBLAS) of the same n={args.cpu_n} "
                                               f"matrix, {lap[1]:.2f} s"}
+        # one host thread, on a sample of half the order (same generator)
+        n1 = max(256, args.cpu_n // 2)
+        g1, t1, kind1, _ = cpu_reference_gflops(n1, args.seed, 1)
+        cpu["one_thread"] = {"value": g1, "unit": UNIT, "cores": 1, "kind": kind1,
+                             "sample": f"one delayed_getrf of n={n1}, {t1:.2f} s"}
+        lap1 = cpu_lapack_gflops(n1, args.seed, 1)
+        if lap1 is not None:
+            cpu["one_thread"]["lapack_dgetrf"] = {"value": lap1[0], "unit": UNIT, "cores": 1,
+                                                  "sample": f"n={n1}, {lap1[1]:.2f} s"}
     if rank == 0:
         # one extra step with every family timed (events on both streams:
         # with look-ahead the families overlap, so shares add up past 1)
