@@ -45,6 +45,11 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "delayed-pivoting_b200"))
 
+# ncu on B200: DRAM bytes (read + write) of one dgemm_minus_kernel launch on
+# an 8192 x 8192 x 256 update per algorithmic byte (16 M N + 8 K (M + N)).
+DMMA_DRAM_PER_ALGORITHMIC_BYTE = 1060.07e6 / 1107.30e6
+
+
 def lu_metric(n):
     return f"plain FP64 delayed_getrf GFLOP/s (2/3 n^3), n={n}, 0.1% tiny + 0.02% zero columns"
 UNIT = "GFLOP/s"
@@ -404,7 +409,17 @@ def run_lu(args):
                     "frac": terms * gemm_tf / bf16 if bf16 else None,
                     "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (measured)",
                     "algorithmic_fp64_tflops": gemm_tf}
-    roofline.update({"traffic": None,
+    alg_bytes = stats["bytes"][g] / max(stats["launches"][g], 1)
+    traffic = None
+    if g == 3:
+        # DRAM bytes per launch scaled from one ncu capture of the same kernel
+        # (8192 x 8192 x 256 update: 1060.1 MB read + written against 1107.3 MB
+        # algorithmic): traffic grows with the algorithmic bytes of a launch
+        traffic = alg_bytes * DMMA_DRAM_PER_ALGORITHMIC_BYTE
+    roofline.update({"traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
+                     "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of an "
+                                        "8192^2 x 256 update, scaled by algorithmic bytes"
+                                        if traffic is not None else None),
                      "per_launch_flops": stats["flops"][g] / max(stats["launches"][g], 1),
                      "avg_launch_ms": gemm_ms / max(stats["launches"][g], 1),
                      "launches_timed": stats["launches"][g]})
