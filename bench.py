@@ -511,6 +511,9 @@ def run_ir(args):
     world, rank, local, dev, dist = _dist_setup(torch)
     n = args.n
     cur = torch.cuda.current_stream()
+    L = dp.lib()
+    L.dp_kernel_launches.restype = ctypes_longlong()
+    launches = 0  # this library's kernels in the timed repetitions
 
     def ev():
         return torch.cuda.Event(enable_timing=True)
@@ -533,6 +536,7 @@ def run_ir(args):
             rec = None
             for it in range(args.warmup + args.steps):
                 torch.cuda.synchronize()
+                l0 = L.dp_kernel_launches()
                 e0, e1 = ev(), ev()
                 e0.record(cur)
                 f = dp.Factor(n, dA, n, precision=prec)
@@ -550,6 +554,7 @@ def run_ir(args):
                 f.close()
                 if it < args.warmup:
                     continue
+                launches += L.dp_kernel_launches() - l0
                 fms = e0.elapsed_time(e1)
                 r = {"factor_ms": fms}
                 for k, (X, res, s0, s1) in sol.items():
@@ -584,7 +589,7 @@ def run_ir(args):
             "config": {"workload": f"gesv with refinement n={n}, kappa {list(IR_KAPPAS)}, 1 and 64 RHS",
                        "n": n, "max_iter": 10, "tol": 1e-14, "l2": "inputs > L2 (no flush needed)"},
             "cpu_baseline": None, "e2e": None, "clocks": clk.summary(),
-            "kappas": rows,
+            "gpu_launches": int(launches), "kappas": rows,
         }
         print(json.dumps(line), flush=True)
     return 0
