@@ -90,3 +90,4 @@ def test_reference_arm_prints_on_rank_zero_only(rank, prints):
         assert line["impl"] == "reference" and "unavailable" in line
     else:
         assert lines == []
+
