@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--cpu-n", type=int, default=8192, help="CPU baseline sample size")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-lu-key", action="store_true",
+                    help="serve: skip the n=16384 plain-LU key of the line")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "mixed3"],
                     help="trailing-update arithmetic of the lu workload: FP64, BF16x6, BF16x3")
     ap.add_argument("--workload", default="serve", choices=["serve", "lu", "batched", "ir"])
@@ -653,33 +655,214 @@ def _serve_summary(reqs, results):
             "refactored_below_1e10": refac_other}
 
 
-def _cpu_serve_baseline(pool, reqs, budget_flops=6e11):
+def _cpu_serve_baseline(reqs, seed, orders=None, lapack=True):
     """The reference's CPU delayed_getrf (oracle/_ref, OpenBLAS on every host
-    core) on the leading requests of the stream, up to budget_flops of
-    factorisation work; each request's solves are counted as served by its
-    factorisation (the reference has no solve), so this overstates the CPU."""
+    core) on the whole stream: one factorisation of a matrix of every
+    distinct order the stream uses, timed, then the stream's CPU time is the
+    sum over ALL its requests of the time of their order.  A nonsingular
+    matrix without exact-zero columns costs delayed_getrf the same work
+    whatever its entries or condition number (the same idamax / dswap /
+    dscal / dger / dtrsm / dgemm calls; no fallback search fires), so one
+    seeded N(0,1) matrix per order stands for every request of that order;
+    info == n is checked.  The reference has no solve (delayed_getrf only
+    factors): each request's solves are counted as served by its
+    factorisation, which overstates the CPU.  With `lapack`, LAPACK dgetrf
+    through the reference's wrapper is timed the same way.  `orders` limits
+    the timed orders (warm-up passes); the value then covers only them."""
     sys.path.insert(0, str(ROOT / "oracle"))
+    import delayed_pivoting as dp
     import oracle as orc
 
     kind, fn = ("reference", orc.ref_getrf) if orc.ref_available() else ("port", orc.oracle_getrf)
     threads = os.cpu_count() or 1
     if kind == "reference":
         orc.ref_lib().ref_set_threads(threads)
-    t_tot, solves, used, count = 0.0, 0, 0.0, 0
-    for q in reqs:
-        f = 2.0 / 3.0 * q.n ** 3
-        if count > 0 and used + f > budget_flops:
-            continue
-        a = np.asfortranarray(pool[(q.n, q.kappa)].cpu().numpy().T)
+    todo = sorted({q.n for q in reqs} if orders is None else set(orders))
+    t_n, t_lap = {}, {}
+    for n in todo:
+        a = dp.planted_matrix(n, n, seed + n)
+        f = a.copy(order="F")
         t0 = time.perf_counter()
-        fn(a)
-        t_tot += time.perf_counter() - t0
-        solves += len(q.solves)
-        used += f
-        count += 1
-    return {"value": solves / t_tot, "unit": "solves/s", "cores": threads, "kind": kind,
-            "sample": f"{count} requests of the stream ({solves} solves, {used:.3g} factorisation "
-                      f"flops) factored by delayed_getrf in {t_tot:.1f} s; solves not timed"}
+        _, _, info = fn(f)
+        t_n[n] = time.perf_counter() - t0
+        if info != n:
+            raise RuntimeError(f"CPU baseline: info {info} != {n}")
+        if lapack and kind == "reference":
+            f = a.copy(order="F")
+            t0 = time.perf_counter()
+            orc.ref_lapack_getrf(f)
+            t_lap[n] = time.perf_counter() - t0
+    sub = [q for q in reqs if q.n in t_n]
+    solves = sum(len(q.solves) for q in sub)
+    stream_s = sum(t_n[q.n] for q in sub)
+    out = {"value": solves / stream_s, "unit": "solves/s", "cores": threads, "kind": kind,
+           "sample": f"delayed_getrf timed once per distinct order ({len(t_n)} orders, "
+                     f"{sum(t_n.values()):.1f} s of CPU work, seeded N(0,1) matrices), weighted by "
+                     f"the stream's {len(sub)} requests ({solves} solves): {stream_s:.1f} s of CPU "
+                     f"time for the stream; solves counted as free",
+           "stream_cpu_s": stream_s, "requests": len(sub), "solves": solves,
+           "per_order_s": {str(n): round(t, 5) for n, t in t_n.items()}}
+    if t_lap:
+        lap_s = sum(t_lap[q.n] for q in sub)
+        out["lapack_dgetrf"] = {"value": solves / lap_s, "unit": "solves/s", "cores": threads,
+                                "stream_cpu_s": lap_s,
+                                "sample": "LAPACK dgetrf (OpenBLAS) through the reference's "
+                                          "wrapper, timed the same way"}
+    return out
+
+
+FAMILY_KERNELS = {0: "panel_cluster_kernel / panel_single_kernel (panel factorisation)",
+                  1: "laswp_kernel (row permutation outside the panel)",
+                  2: "trsm_lower_unit_kernel (U12 = L11^-1 A12)",
+                  3: "dgemm_minus_kernel (FP64 DMMA m16n8k4)",
+                  7: "gemm_bf16x3_kernel<3> (tcgen05 kind::f16, 6 products, incl. operand split)"}
+
+
+def _family_roofline(stats, i, peaks):
+    """Roofline of one kernel family from the library's per-family CUDA events
+    (dp_stats_*: events on the launching stream around every launch group):
+    achieved = algorithmic bytes (and flops) per launch / average launch
+    duration.  In the served burst a launch's event interval includes the
+    time it waits for SMs behind other requests' kernels."""
+    ms, launches = stats["ms"][i], max(stats["launches"][i], 1)
+    if not stats["launches"][i] or ms <= 0:
+        return None
+    avg_s = ms * 1e-3 / launches
+    by = stats["bytes"][i] / launches
+    fl = stats["flops"][i] / launches
+    hbm = peaks.get("hbm_gbs")
+    gbs = by / avg_s / 1e9
+    r = {"kernel": FAMILY_KERNELS.get(i, f"family {i}"), "avg_launch_ms": avg_s * 1e3,
+         "launches": stats["launches"][i], "algorithmic_bytes_per_launch": by,
+         "algorithmic_flops_per_launch": fl, "hbm_gbs": gbs, "hbm_peak_gbs": hbm,
+         "hbm_frac": gbs / hbm if hbm else None, "traffic": None,
+         "peak_source": "MEASURED_PEAKS.json (measured)" if not peaks.get("fallback")
+         else "fallback figures (MEASURED_PEAKS.json absent)"}
+    if i == 7:
+        bf16 = peaks.get("bf16_tflops_sustained") or peaks.get("bf16_tflops")
+        tf = 6 * fl / avg_s / 1e12
+        r.update({"bound": "tensor", "achieved": tf, "peak": bf16, "unit": "TFLOP/s",
+                  "frac": tf / bf16 if bf16 else None, "algorithmic_fp64_tflops": fl / avg_s / 1e12,
+                  "tensor_frac": tf / bf16 if bf16 else None})
+    else:
+        r.update({"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s",
+                  "frac": gbs / hbm if hbm else None, "tflops": fl / avg_s / 1e12})
+    return r
+
+
+def _serve_e2e(torch, dp, sv, dist, dev, pool, rhs, reqs, warm):
+    """solves/s of the mixed server on the full stream `reqs` with every input
+    in pinned host memory (see run_serve)."""
+    keys = sorted({(q.n, q.kappa) for q in reqs})
+    hostA = {k: pool[k].cpu().pin_memory() for k in keys}
+    hostB = {s.rid: rhs.src[s.rid].cpu().pin_memory() for q in reqs for s in q.solves}
+    hostX = {k: torch.empty_like(v).pin_memory() for k, v in hostB.items()}
+    devA = [torch.empty_like(pool[(q.n, q.kappa)]) for q in reqs]
+    srv = dp.Server(precision=dp.PRECISION_MIXED_BF16X6)
+    rhs.reset(torch)
+    sv.replay(srv, pool, rhs, warm)  # the same warm-up as the bursts' server
+    rhs.reset(torch)
+    cs = torch.cuda.Stream()
+    h2d = sum(8 * q.n * q.n for q in reqs) + sum(v.numel() * 8 for v in hostB.values())
+    d2h = sum(v.numel() * 8 for v in hostB.values())
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(cs)
+    results = {}
+    for q, dA in zip(reqs, devA):
+        with torch.cuda.stream(cs):
+            dA.copy_(hostA[(q.n, q.kappa)], non_blocking=True)
+            for s_ in q.solves:
+                rhs.work[s_.rid].copy_(hostB[s_.rid], non_blocking=True)
+        cs.synchronize()
+        for s_ in q.solves:
+            b = rhs.work[s_.rid]
+            if s_.factor_id == 0:
+                st = srv.submit(s_.rid, q.n, dA, q.n, b, q.n, s_.nrhs,
+                                followups=len(q.solves) - 1)
+            else:
+                st = srv.submit(s_.rid, q.n, None, q.n, b, q.n, s_.nrhs, factor_id=s_.factor_id)
+            assert st == 0
+        for r in srv.poll(1024, 0):
+            results[r.id] = r
+    total = sum(len(q.solves) for q in reqs)
+    while len(results) < total:
+        for r in srv.poll(1024, 20):
+            results[r.id] = r
+    with torch.cuda.stream(cs):
+        for k_, v in hostX.items():
+            v.copy_(rhs.work[k_], non_blocking=True)
+    e1.record(cs)
+    e1.synchronize()
+    srv.close()
+    e_ms = _max_over_ranks(torch, dist, dev, e0.elapsed_time(e1))
+    bad = sum(1 for r in results.values() if r.status != 0 or not (r.backward_error <= 1e-14))
+    del devA, hostA, hostB, hostX
+    torch.cuda.empty_cache()
+    return {"value": _sum_over_ranks(torch, dist, dev, total) / (e_ms * 1e-3),
+            "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "ms_per_step": e_ms, "requests": len(reqs), "solves": total,
+            "api": "dp_server_submit / dp_server_poll (mixed), inputs from pinned host memory",
+            "backward_error_max": max(r.backward_error for r in results.values()),
+            "violations": bad}
+
+
+def lu_key(torch, dp, dev, L, n=16384, warmup=2, steps=3):
+    """Config-2 check carried by the default line: plain FP64 delayed_getrf of
+    the n = 16384 planted matrix (seed 16384, 16 tiny + 3 zero columns), time
+    per factorisation (CUDA events), GFLOP/s against the FP64 peaks measured
+    live (cuBLAS DGEMM), the kernel families, and whether the records equal
+    the reference's (tests/golden/config2_n16384.npz, written by the
+    reference's own delayed_getrf)."""
+    gold = ROOT / "tests" / "golden" / f"config2_n{n}.npz"
+    w = workload(n)
+    a = dp.planted_matrix(n, n, n, w["n_tiny"], w["n_zero"])
+    orig = torch.from_numpy(a.T.copy()).to(dev)
+    del a
+    work = torch.empty_like(orig)
+    ipiv = np.zeros(n, dtype=np.int32)
+    jpiv = np.zeros(n, dtype=np.int32)
+    stream = torch.cuda.current_stream(dev)
+    ms, info = [], None
+    for i in range(warmup + steps + 1):
+        work.copy_(orig)
+        last = i == warmup + steps
+        if last:
+            L.dp_stats_reset()
+            L.dp_stats_enable(1)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st, info = dp.getrf_device_ex(n, n, work, n, ipiv, jpiv, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        if st != 0:
+            raise RuntimeError(dp.delayed_getrf_cuda_status_string(st))
+        if last:
+            L.dp_stats_enable(0)
+        elif i >= warmup:
+            ms.append(e0.elapsed_time(e1))
+    stats = _stats(L)
+    L.dp_stats_reset()
+    del orig, work
+    torch.cuda.empty_cache()
+    fp64 = fp64_peak_tflops(torch, dev)
+    gf = flops(n) / (statistics.mean(ms) * 1e-3) / 1e9
+    fam = ["panel", "laswp", "trsm", "gemm", "search", "swap", "other", "gemm_mixed"]
+    kern = {nm: {"ms": round(stats["ms"][i], 3), "launches": stats["launches"][i]}
+            for i, nm in enumerate(fam) if stats["launches"][i]}
+    out = {"n": n, "gflops": gf, "ms_per_factorisation": statistics.mean(ms),
+           "step_ms": [round(x, 3) for x in ms], "info": info,
+           "fp64_peak_tflops_cublas_dgemm": fp64, "frac_of_fp64_peak": gf / 1e3 / fp64,
+           "target_frac": 0.70, "kernels_one_step": kern,
+           "panel_roofline": _family_roofline(stats, 0, measured_peaks())}
+    if gold.exists():
+        with np.load(gold) as z:
+            out["records_match_reference"] = bool(
+                np.array_equal(z["ipiv"], ipiv) and np.array_equal(z["jpiv"], jpiv)
+                and int(z["info"]) == info)
+    return out
 
 
 def run_serve(args):
@@ -747,83 +930,39 @@ def run_serve(args):
         out[mode]["server"].close()
         out[mode]["server"] = None
 
-    # e2e: requests whose matrices and right-hand sides start in pinned host
-    # memory; H2D copies, serving and the D2H of every X inside the timed region
+    # e2e: the same requests as `value`, but every matrix and right-hand side
+    # starts in pinned host memory: per request the H2D copies of its matrix
+    # (its own device buffer) and right-hand sides, then its submission; the
+    # D2H of every solution after the last result.  All inside the timed
+    # region, on a server warmed like the bursts' one.
     e2e = None
     if not args.no_e2e:
-        ereqs = reqs[:max(10, R // 4)]
-        hostA = {}
-        for q in ereqs:
-            if (q.n, q.kappa) not in hostA:
-                hostA[(q.n, q.kappa)] = pool[(q.n, q.kappa)].cpu().pin_memory()
-        hostB = {s.rid: rhs.src[s.rid].cpu().pin_memory() for q in ereqs for s in q.solves}
-        hostX = {k: torch.empty_like(v).pin_memory() for k, v in hostB.items()}
-        devA = [torch.empty_like(pool[(q.n, q.kappa)]) for q in ereqs]
-        srv = dp.Server(precision=dp.PRECISION_MIXED_BF16X6)
-        cs = torch.cuda.Stream()
-        h2d = sum(8 * q.n * q.n for q in ereqs) + sum(v.numel() * 8 for v in hostB.values())
-        d2h = sum(v.numel() * 8 for v in hostB.values())
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(cs)
-        results = {}
-        for q, dA in zip(ereqs, devA):
-            with torch.cuda.stream(cs):
-                dA.copy_(hostA[(q.n, q.kappa)], non_blocking=True)
-                for s_ in q.solves:
-                    rhs.work[s_.rid].copy_(hostB[s_.rid], non_blocking=True)
-            cs.synchronize()
-            for s_ in q.solves:
-                b = rhs.work[s_.rid]
-                if s_.factor_id == 0:
-                    st = srv.submit(s_.rid, q.n, dA, q.n, b, q.n, s_.nrhs,
-                                    followups=len(q.solves) - 1)
-                else:
-                    st = srv.submit(s_.rid, q.n, None, q.n, b, q.n, s_.nrhs,
-                                    factor_id=s_.factor_id)
-                assert st == 0
-            for r in srv.poll(1024, 0):
-                results[r.id] = r
-        total = sum(len(q.solves) for q in ereqs)
-        while len(results) < total:
-            for r in srv.poll(1024, 20):
-                results[r.id] = r
-        with torch.cuda.stream(cs):
-            for k_, v in hostX.items():
-                v.copy_(rhs.work[k_], non_blocking=True)
-        e1.record(cs)
-        e1.synchronize()
-        srv.close()
-        e_ms = _max_over_ranks(torch, dist, dev, e0.elapsed_time(e1))
-        e2e = {"value": _sum_over_ranks(torch, dist, dev, total) / (e_ms * 1e-3),
-               "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "ms_per_step": e_ms, "requests": len(ereqs),
-               "api": "dp_server_submit / dp_server_poll (mixed), inputs from pinned host memory",
-               "backward_error_max": max(r.backward_error for r in results.values())}
-        del devA, hostA, hostB, hostX
+        e2e = _serve_e2e(torch, dp, sv, dist, dev, pool, rhs, reqs, warm)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        cpu = _cpu_serve_baseline(pool, reqs)
+        cpu = _cpu_serve_baseline(reqs, seed)
+
+    pool_gb = pool.bytes / 1e9
+    lu = None
+    if not args.no_lu_key:
+        del pool, rhs
+        torch.cuda.empty_cache()
+        lu = lu_key(torch, dp, dev, L)
 
     peaks = measured_peaks()
-    g = 7  # DP_KFAM_GEMM_MIXED
-    gm_ms = stats["ms"][g]
-    algo_tf = stats["flops"][g] / (gm_ms * 1e-3) / 1e12 if gm_ms > 0 else 0.0
-    bf16 = peaks.get("bf16_tflops_sustained") or peaks.get("bf16_tflops")
-    roofline = {"bound": "tensor", "kernel": "gemm_bf16x3_kernel<3> (tcgen05 kind::f16, 6 products)",
-                "achieved": 6 * algo_tf, "peak": bf16, "unit": "TFLOP/s",
-                "frac": 6 * algo_tf / bf16 if bf16 else None,
-                "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (measured)",
-                "traffic": None, "algorithmic_fp64_tflops": algo_tf,
-                "per_launch_flops": stats["flops"][g] / max(stats["launches"][g], 1),
-                "avg_launch_ms": gm_ms / max(stats["launches"][g], 1)}
     fam = ["panel", "laswp", "trsm", "gemm", "search", "swap", "other", "gemm_mixed"]
     kern = {nm: {"ms": stats["ms"][i], "launches": stats["launches"][i],
+                 "avg_launch_us": 1e3 * stats["ms"][i] / stats["launches"][i],
                  "tflops": (stats["flops"][i] / (stats["ms"][i] * 1e-3) / 1e12
-                            if stats["flops"][i] and stats["ms"][i] else None)}
+                            if stats["flops"][i] and stats["ms"][i] else None),
+                 "gbs": (stats["bytes"][i] / (stats["ms"][i] * 1e-3) / 1e9
+                         if stats["bytes"][i] and stats["ms"][i] else None)}
             for i, nm in enumerate(fam) if stats["launches"][i]}
+    # the dominant kernel family of the burst (largest event time)
+    top = max(kern, key=lambda k: kern[k]["ms"])
+    roofline = _family_roofline(stats, fam.index(top), peaks)
+    roofline_gemm = _family_roofline(stats, 7, peaks)
     if rank == 0:
         m, pl = out["mixed"], out["plain"]
         line = {
@@ -833,7 +972,7 @@ def run_serve(args):
             "data": "synthetic: seeded QR-conditioned matrices, seeded Poisson stream",
             "config": {"workload": SERVE_WORKLOAD, "requests_per_step": R, "max_n": args.max_n,
                        "solves_per_step": solves_per_step, "precision": "mixed BF16x6 (six-product BF16 split, FP32 accumulation) + FP64 IR",
-                       "pool_gb": pool.bytes / 1e9, "parallelism": f"replicas x{world}",
+                       "pool_gb": pool_gb, "parallelism": f"replicas x{world}",
                        "l2": "inputs per step >> L2 (no flush needed)"},
             "p99_ms": m["open"]["p99_ms"], "p50_ms": m["open"]["p50_ms"],
             "open_loop": {"rate_rps": rate, "load": args.load, "mixed": m["open"],
@@ -843,11 +982,13 @@ def run_serve(args):
                            "p50_ms": pl["open"]["p50_ms"], "p99_ms": pl["open"]["p99_ms"],
                            "mixed_over_plain": m["capacity"] / pl["capacity"]},
             "roofline": roofline,
+            "roofline_gemm_mixed": roofline_gemm,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(m["launches"]),
             "clocks": m["clocks"],
             "kernels_mixed_burst": kern,
+            "lu_n16384": lu,
         }
         print(json.dumps(line), flush=True)
     if dist:
@@ -857,44 +998,38 @@ def run_serve(args):
 
 
 def serve_reference_arm(args):
-    """The reference's CPU delayed_getrf on a bounded sample of the same stream
-    per step (each request's solves counted as served by its factorisation)."""
-    import torch
+    """The reference's CPU delayed_getrf on the same stream as the GPU arm's
+    `value` (the same seed, all --requests requests): every step times one
+    factorisation per distinct order and weights it by the stream's counts
+    (_cpu_serve_baseline); the step's solves/s are the stream's solves over
+    the stream's CPU time.  Warm-up steps time the orders up to 1024 only
+    (they warm OpenBLAS's thread pool and the caches)."""
     from delayed_pivoting import serving as sv
 
     reqs = sv.make_stream(args.requests, args.seed, hi=args.max_n)
-    vals, cpu = [], None
-    sample = reqs[:64]
-
-    class HostPool:
-        def __init__(self):
-            self.cache = {}
-
-        def __getitem__(self, key):
-            if key not in self.cache:
-                n, kappa = key
-                g = torch.Generator().manual_seed(args.seed * 100003 + n)
-                u, _ = torch.linalg.qr(torch.randn(n, n, dtype=torch.float64, generator=g))
-                v, _ = torch.linalg.qr(torch.randn(n, n, dtype=torch.float64, generator=g))
-                s = torch.logspace(0, -np.log10(kappa), n, dtype=torch.float64)
-                self.cache[key] = ((u * s) @ v.T).T.contiguous()
-            return self.cache[key]
-
-    pool = HostPool()
-    t_all = 0.0
+    small = [n for n in sorted({q.n for q in reqs}) if n <= 1024]
+    stream_s, solves, cpu, t_all = 0.0, 0, None, 0.0
     for i in range(args.warmup + args.steps):
+        if i < args.warmup:
+            _cpu_serve_baseline(reqs, args.seed, orders=small, lapack=False)
+            continue
         t0 = time.perf_counter()
-        cpu = _cpu_serve_baseline(pool, sample, budget_flops=2e11)
-        if i >= args.warmup:
-            vals.append(cpu["value"])
-            t_all += time.perf_counter() - t0
-    value = float(np.mean(vals))
+        cpu = _cpu_serve_baseline(reqs, args.seed, lapack=(i == args.warmup + args.steps - 1))
+        t_all += time.perf_counter() - t0
+        stream_s += cpu["stream_cpu_s"]
+        solves += cpu["solves"]
+    value = solves / stream_s
     line = {"impl": "reference", "metric": SERVE_METRIC, "value": value, "unit": "solves/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_all / max(args.steps, 1) * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic: seeded QR-conditioned matrices (host), seeded stream",
-            "config": {"workload": SERVE_WORKLOAD, "requests_per_step": args.requests},
+            "data": "synthetic: the GPU arm's seeded stream; seeded N(0,1) matrices per order",
+            "step": "one timing pass: delayed_getrf once per distinct order of the stream "
+                    "(ms_per_step is its wall time); value = the stream's solves over the "
+                    "stream's CPU time (the per-order times weighted by the stream's counts)",
+            "stream_cpu_s_per_step": stream_s / max(args.steps, 1),
+            "config": {"workload": SERVE_WORKLOAD, "requests_per_step": args.requests,
+                       "max_n": args.max_n, "solves_per_step": cpu["solves"]},
             "cpu_baseline": dict(cpu, value=value),
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}

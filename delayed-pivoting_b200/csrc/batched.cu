@@ -80,6 +80,8 @@ struct Params {
   int* ipiv;
   int* jpiv;
   int* info;
+  unsigned long long* ties;      // near-tie detector: decisions checked, order-sensitive
+                                 // ones, bits of the largest runner-up / winner ratio
   double threshold;
   int nb_bucket[DP_BATCH_BUCKETS];
   int pr;                        // column stride of the shared panel
@@ -101,11 +103,13 @@ struct Smem {
                                    // reciprocal of its pivot entry, by step parity
   double rval[2][kWarps];          // each warp's best magnitude (>= 0) and logical row
   int rkey[2][kWarps];
+  double rsec[2][kWarps];          // each warp's runner-up magnitude (near-tie detector)
   double psave[kSb][kLdsave];      // the current sub-panel's pivot rows, whole window
   short mv_dst[2 * kMaxNb];        // the panel's composite row permutation:
   short mv_src[2 * kMaxNb];        // panel row mv_src[j] moves to mv_dst[j]
   int mv_count;
   double fval[kWarps];             // fallback search
+  double fsec[kWarps];
   int frow[kWarps];
   int fcol[kWarps];
   int slot;
@@ -138,6 +142,38 @@ __device__ __forceinline__ void warp_best(double v, int key, double& bv, int& bk
   bv = __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
 }
 
+// Largest of the lanes' non-negative magnitudes (bit-pattern order).
+__device__ __forceinline__ double warp_max_pos(double v) {
+  const unsigned long long u = (unsigned long long)__double_as_longlong(v);
+  const unsigned hi = (unsigned)(u >> 32), lo = (unsigned)u;
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+  return __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
+}
+
+// Offers candidate (v, key) to a running best (cv, ck) with runner-up cs:
+// the magnitude that does not win becomes a runner-up candidate.
+__device__ __forceinline__ bool offer(double v, int key, double& cv, int& ck, double& cs) {
+  if (beats(v, key, cv, ck)) {
+    cs = fmax(cs, cv);
+    cv = v;
+    ck = key;
+    return true;
+  }
+  cs = fmax(cs, v);
+  return false;
+}
+
+// Counts one pivot decision of step k in the batch's near-tie counters.
+__device__ __forceinline__ void note_tie(unsigned long long* ties, int k, double best,
+                                         double second) {
+  atomicAdd(ties, 1ull);
+  if (best > 0.0) {
+    if (best - second <= kNearTieC * (double)(k + 1) * 0x1p-53 * best) atomicAdd(ties + 1, 1ull);
+    atomicMax(ties + 2, (unsigned long long)__double_as_longlong(second / best));
+  }
+}
+
 // Factor panel columns [b, b + w) of the n x n matrix A (rows b..n-1).
 // Returns the first step without an acceptable pivot (-1: all w steps done).
 // Writes the panel back in logical row order to A and to P (column stride
@@ -153,7 +189,7 @@ __device__ __forceinline__ void warp_best(double v, int key, double& bv, int& bk
 // shifts by kSb.  The compiled step body is one sub-panel long.
 __device__ __forceinline__ int panel_regs(double* A, int n, int lda, int b, int w,
                                           bool positioned, double thr, double* P, int pr,
-                                          Smem& s, int* ipiv) {
+                                          Smem& s, int* ipiv, unsigned long long* ties) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int rows = n - b;
   double x[kRpt][kMaxNb];
@@ -171,7 +207,7 @@ __device__ __forceinline__ int panel_regs(double* A, int n, int lda, int b, int 
   // the winning lane pushes its sub-panel columns j.., the reciprocal of its
   // entry in column j (computed by every lane ahead of the reductions, off
   // the path after the barrier) and the warp's result
-  auto push = [&](int j, int par, double cv, int ck, int ci) {
+  auto push = [&](int j, int par, double cv, int ck, int ci, double cs) {
     double pv = 0.0;
 #pragma unroll
     for (int c = 0; c < kSb; ++c)
@@ -180,6 +216,8 @@ __device__ __forceinline__ int panel_regs(double* A, int n, int lda, int b, int 
     double wv;
     int wk;
     warp_best(cv, ck, wv, wk);
+    // the warp's runner-up: the winner lane's runner-up, every other lane's best
+    const double ws = warp_max_pos((wk != kNone && ck == wk) ? cs : (ck != kNone ? cv : cs));
     if (wk != kNone ? ck == wk : lane == 0) {
       if (wk != kNone) {
 #pragma unroll
@@ -189,11 +227,12 @@ __device__ __forceinline__ int panel_regs(double* A, int n, int lda, int b, int 
       }
       s.rval[par][warp] = wv;
       s.rkey[par][warp] = wk;
+      s.rsec[par][warp] = ws;
     }
   };
   // candidate of window column 0 among the rows at logical positions >= first
   auto first_candidate = [&](int first, bool placed) {
-    double cv = 0.0;
+    double cv = 0.0, cs = 0.0;
     int ck = kNone, ci = 0;
 #pragma unroll
     for (int i = 0; i < kRpt; ++i) {
@@ -201,13 +240,9 @@ __device__ __forceinline__ int panel_regs(double* A, int n, int lda, int b, int 
       // a placed pivot (after a fallback) is the only candidate of its step
       if (placed && lp[i] != first) continue;
       const double v = placed ? INFINITY : fabs(x[i][0]);
-      if (beats(v, lp[i], cv, ck)) {
-        cv = v;
-        ck = lp[i];
-        ci = i;
-      }
+      if (offer(v, lp[i], cv, ck, cs)) ci = i;
     }
-    push(0, first & 1, cv, ck, ci);
+    push(0, first & 1, cv, ck, ci, cs);
   };
 
   first_candidate(0, positioned);
@@ -230,6 +265,15 @@ __device__ __forceinline__ int panel_regs(double* A, int n, int lda, int b, int 
       const int bw = max(0, __ffs(__ballot_sync(0xffffffffu, lane < kWarps && bk != kNone &&
                                                                 s.rkey[par][lane] == bk)) - 1);
       const bool placed = positioned && st == 0;
+      if (!placed) {
+        // runner-up over the warps (lanes >= kWarps repeat lanes < kWarps)
+        const int q = lane & (kWarps - 1);
+        const double bs = warp_max_pos((bk != kNone && s.rkey[par][q] == bk)
+                                           ? s.rsec[par][q]
+                                           : (s.rkey[par][q] != kNone ? s.rval[par][q]
+                                                                      : s.rsec[par][q]));
+        if (tid == 0) note_tie(ties, b + st, bk != kNone ? bv : 0.0, bs);
+      }
       if (!placed && !(bv > thr)) {
         stop = st;
         kd = j;
@@ -239,7 +283,7 @@ __device__ __forceinline__ int panel_regs(double* A, int n, int lda, int b, int 
       const int p = bk;  // logical position of the pivot row before the swap
       if (tid == 0 && !placed) ipiv[b + st] = b + p;
       const double inv = prow[kSb];
-      double cv = 0.0;
+      double cv = 0.0, cs = 0.0;
       int ck = kNone, ci = 0;
 #pragma unroll
       for (int i = 0; i < kRpt; ++i) {
@@ -261,15 +305,11 @@ __device__ __forceinline__ int panel_regs(double* A, int n, int lda, int b, int 
         for (int c = j + 1; c < kSb; ++c) x[i][c] = fma(-l, prow[c], x[i][c]);
         if (j + 1 < kSb) {
           const double v = fabs(x[i][j + 1 < kSb ? j + 1 : 0]);
-          if (beats(v, lp[i], cv, ck)) {
-            cv = v;
-            ck = lp[i];
-            ci = i;
-          }
+          if (offer(v, lp[i], cv, ck, cs)) ci = i;
         }
       }
       if (j + 1 < sw) {
-        push(j + 1, par ^ 1, cv, ck, ci);
+        push(j + 1, par ^ 1, cv, ck, ci, cs);
         __syncthreads();
       }
     }
@@ -506,52 +546,64 @@ __device__ __forceinline__ bool better2(double va, int ca, int ra, double vb, in
 // 2-D argmax over the active block A(k:n, k:n): larger magnitude, then the
 // smaller column, then the smaller row; NaN never wins.
 __device__ __forceinline__ void active_argmax(const double* A, int lda, int n, int k, Smem& s,
-                                              double& bv, int& br, int& bc) {
+                                              double& bv, int& br, int& bc, double& bs) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  double v0 = -1.0;
+  double v0 = -1.0, s0 = 0.0;  // best, runner-up (largest of the other magnitudes)
   int r0 = INT_MAX, c0 = INT_MAX;
   const int rows = n - k;
   for (int c = k; c < n; ++c)
     for (int r = tid; r < rows; r += kThreads) {
       const double v = fabs(A[idx(k + r, c, lda)]);
       if (v > v0) {  // (column, row) increase along this thread's scan
+        s0 = fmax(s0, v0);
         v0 = v;
         r0 = k + r;
         c0 = c;
+      } else {
+        s0 = fmax(s0, v);
       }
     }
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
     const double ov = __shfl_xor_sync(0xffffffffu, v0, off);
+    const double os = __shfl_xor_sync(0xffffffffu, s0, off);
     const int orr = __shfl_xor_sync(0xffffffffu, r0, off);
     const int oc = __shfl_xor_sync(0xffffffffu, c0, off);
     if (better2(ov, oc, orr, v0, c0, r0)) {
+      s0 = fmax(os, v0);
       v0 = ov;
       r0 = orr;
       c0 = oc;
+    } else {
+      s0 = fmax(s0, ov);
     }
   }
   __syncthreads();
   if (lane == 0) {
     s.fval[warp] = v0;
+    s.fsec[warp] = s0;
     s.frow[warp] = r0;
     s.fcol[warp] = c0;
   }
   __syncthreads();
   bv = s.fval[0];
+  bs = s.fsec[0];
   br = s.frow[0];
   bc = s.fcol[0];
   for (int q = 1; q < kWarps; ++q)
     if (better2(s.fval[q], s.fcol[q], s.frow[q], bv, bc, br)) {
+      bs = fmax(s.fsec[q], bv);
       bv = s.fval[q];
       br = s.frow[q];
       bc = s.fcol[q];
+    } else {
+      bs = fmax(bs, s.fval[q]);
     }
 }
 
 __device__ __forceinline__ void getrf_one(double* A, int n, int* ipiv, int* jpiv, int* info,
                                           int nb, double thr, double* P, int pr, double* Bs,
-                                          Smem& s) {
+                                          Smem& s, unsigned long long* ties) {
   const int tid = threadIdx.x;
   const int lda = n;
   for (int i = tid; i < n; i += kThreads) ipiv[i] = jpiv[i] = i;
@@ -561,7 +613,7 @@ __device__ __forceinline__ void getrf_one(double* A, int n, int* ipiv, int* jpiv
   while (b < n) {
     const int w = min(nb, n - b), e = b + w;
     __syncthreads();  // P, Bs, the move list and the records are settled
-    const int stop = panel_regs(A, n, lda, b, w, positioned, thr, P, pr, s, ipiv);
+    const int stop = panel_regs(A, n, lda, b, w, positioned, thr, P, pr, s, ipiv, ties);
     positioned = false;
     __syncthreads();  // panel written back, move list complete
     permute_outside(A, lda, n, b, w, s);
@@ -575,9 +627,10 @@ __device__ __forceinline__ void getrf_one(double* A, int n, int* ipiv, int* jpiv
     const int k = b + stop;
     if (e < n && stop > 0) trailing_update(A, lda, n, b, stop, e, P, pr, Bs);
     __syncthreads();
-    double bv;
+    double bv, bs;
     int br, bc;
-    active_argmax(A, lda, n, k, s, bv, br, bc);
+    active_argmax(A, lda, n, k, s, bv, br, bc, bs);
+    if (tid == 0) note_tie(ties, k, bv > 0.0 ? bv : 0.0, bv > 0.0 ? bs : 0.0);
     if (!(bv > thr)) {
       if (tid == 0) *info = k;
       return;
@@ -621,7 +674,7 @@ __global__ void __launch_bounds__(kThreads, 1) batched_getrf_kernel(Params p) {
     const int nb = bk == 0 ? p.nb_bucket[0] : bk == 1 ? p.nb_bucket[1] : bk == 2 ? p.nb_bucket[2]
                                                                                  : p.nb_bucket[3];
     getrf_one(p.base + p.offsets[i], n, p.ipiv + p.rec_offsets[i], p.jpiv + p.rec_offsets[i],
-              p.info + i, nb, p.threshold, P, p.pr, Bs, s);
+              p.info + i, nb, p.threshold, P, p.pr, Bs, s, p.ties);
   }
 }
 
@@ -701,7 +754,8 @@ namespace batch {
 // The batched launch on caller-managed device arrays (the server's small-
 // request path, which allocates from the stream-ordered pool): d_n, d_off,
 // d_rec, d_order describe `count` matrices as in a dp_batch plan, d_queue is
-// one int of scratch.
+// kQueueBytes of 8-byte aligned scratch (the work counter, then the launch's
+// near-tie counters), cleared here before the launch.
 int launch_raw(int count, int max_n, int sms, const int* d_n, const long long* d_off,
                const long long* d_rec, const int* d_order, int* d_queue, double* base, int* ipiv,
                int* jpiv, int* info, const dp_batch_options& opt, cudaStream_t st) {
@@ -718,6 +772,7 @@ int launch_raw(int count, int max_n, int sms, const int* d_n, const long long* d
   p.ipiv = ipiv;
   p.jpiv = jpiv;
   p.info = info;
+  p.ties = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(d_queue) + 8);
   p.threshold = opt.threshold;
   for (int i = 0; i < DP_BATCH_BUCKETS; ++i) p.nb_bucket[i] = opt.nb_bucket[i];
   p.pr = panel_ld(max_n);
@@ -726,7 +781,7 @@ int launch_raw(int count, int max_n, int sms, const int* d_n, const long long* d
   const int per_sm = dp::occupancy_once((const void*)batched_getrf_kernel, kThreads, smem);
   if (per_sm < 1) return DP_CUDA_FAILURE;
   const int grid = std::max(1, std::min(count, sms * per_sm));
-  if (cudaMemsetAsync(d_queue, 0, sizeof(int), st) != cudaSuccess) return DP_CUDA_FAILURE;
+  if (cudaMemsetAsync(d_queue, 0, kQueueBytes, st) != cudaSuccess) return DP_CUDA_FAILURE;
   dp::note_launch();
   batched_getrf_kernel<<<grid, kThreads, smem, st>>>(p);
   return cudaGetLastError() == cudaSuccess ? DP_SUCCESS : DP_CUDA_FAILURE;
@@ -801,7 +856,7 @@ int dp_batch_create(dp_batch** out, int count, const int* n, const long long* of
       cudaMalloc(&bp->d_offsets, c * sizeof(long long)) != cudaSuccess ||
       cudaMalloc(&bp->d_rec, c * sizeof(long long)) != cudaSuccess ||
       cudaMalloc(&bp->d_order, c * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&bp->d_queue, sizeof(int)) != cudaSuccess) {
+      cudaMalloc(&bp->d_queue, dp::batch::kQueueBytes) != cudaSuccess) {
     dp_batch_destroy(bp);
     return DP_ALLOCATION_FAILED;
   }
@@ -886,6 +941,22 @@ int dp_batch_getrf_graph(dp_batch* bp, double* d_base, int* d_ipiv, int* d_jpiv,
   dp::note_launch();  // the graph holds one kernel (after the queue reset)
   return cudaGraphLaunch(bp->exec, (cudaStream_t)stream) == cudaSuccess ? DP_SUCCESS
                                                                         : DP_CUDA_FAILURE;
+}
+
+int dp_batch_last_report(dp_batch* bp, dp_getrf_report* out) {
+  if (!bp || !out) return DP_INVALID_ARGUMENT;
+  unsigned long long t[3] = {0, 0, 0};
+  if (bp->count > 0 &&
+      (cudaDeviceSynchronize() != cudaSuccess ||
+       cudaMemcpy(t, reinterpret_cast<char*>(bp->d_queue) + 8, sizeof(t),
+                  cudaMemcpyDeviceToHost) != cudaSuccess))
+    return DP_CUDA_FAILURE;
+  std::memset(out, 0, sizeof(*out));
+  out->decisions = (long long)t[0];
+  out->near_ties = (long long)t[1];
+  std::memcpy(&out->max_closeness, &t[2], sizeof(double));
+  out->info = bp->count;
+  return DP_SUCCESS;
 }
 
 void dp_batch_destroy(dp_batch* bp) {

@@ -93,6 +93,7 @@ struct Cand {
   double val;
   int row;
   int col;
+  double sec;  // runner-up: the largest other magnitude seen (near-tie detector)
 };
 
 __device__ __forceinline__ bool cand_better(const Cand& a, const Cand& b) {
@@ -103,6 +104,15 @@ __device__ __forceinline__ bool cand_better(const Cand& a, const Cand& b) {
     return a.row < b.row;
   }
   return false;
+}
+
+// Merges two candidates over disjoint element sets (winner by cand_better,
+// runner-up the largest magnitude that did not win; NaN is never taken).
+__device__ __forceinline__ Cand cand_merge(const Cand& a, const Cand& b) {
+  Cand r = cand_better(b, a) ? b : a;
+  const Cand& lose = cand_better(b, a) ? a : b;
+  r.sec = fmax(r.sec, fmax(lose.val, lose.sec));
+  return r;
 }
 
 // Device-resident state of one factorisation.  Written by kernels, read by
@@ -116,7 +126,31 @@ struct State {
   unsigned int search_done;  // last-block-done counter of the search kernels
   unsigned int barrier_exit; // exit counter of the panel kernel
   int pad1[2];
+  // Near-tie detector: every pivot decision (column search of a panel step,
+  // fallback search) also reduces the runner-up magnitude; a decision whose
+  // winner beats the runner-up by at most kNearTieC (k + 1) u |winner| (u =
+  // 2^-53, k the step) could change under another summation order and is
+  // counted as order-sensitive.  Decisions on a zero winner (delay / stop)
+  // are exact and never count.
+  unsigned long long ties_checked;  // decisions whose runner-up was compared
+  unsigned long long near_ties;     // order-sensitive decisions among them
+  unsigned long long closeness;     // bits of max(second / best) over the checked decisions
 };
+
+constexpr double kNearTieC = 4.0;
+
+// Records one pivot decision of step k with winner magnitude `best` and
+// runner-up `second` (both >= 0; NaN never reaches here).  Called by one
+// thread per decision.
+__device__ __forceinline__ void note_decision(State* st, long long k, double best, double second) {
+  st->ties_checked += 1;
+  if (best > 0.0) {
+    const double ratio = second / best;
+    if (best - second <= kNearTieC * (double)(k + 1) * 0x1p-53 * best) st->near_ties += 1;
+    const unsigned long long bits = (unsigned long long)__double_as_longlong(ratio);
+    if (bits > st->closeness) st->closeness = bits;
+  }
+}
 
 // Bounded wait: every spin in this library gives up after kSpinLimitNs of
 // wall time, records kDeviceTimeout in the state and lets the caller return.

@@ -207,6 +207,21 @@ bool plan_cluster(int rows, int& w, const DeviceInfo& di, int& C, int& R) {
   return true;
 }
 
+// Near-tie report of the calling thread's last factorisation (every entry
+// point is synchronous, so "last" is well defined per host thread).
+thread_local dp_getrf_report g_report = {0, 0, 0.0, -1, {0, 0, 0}};
+
+void set_report(const State& s, int info) {
+  g_report.decisions = (long long)s.ties_checked;
+  g_report.near_ties = (long long)s.near_ties;
+  double c = 0.0;
+  std::memcpy(&c, &s.closeness, sizeof(c));
+  g_report.max_closeness = c;
+  g_report.info = info;
+}
+
+void clear_report() { g_report = dp_getrf_report{0, 0, 0.0, -1, {0, 0, 0}}; }
+
 #define DP_CHECK_CUDA(call)                       \
   do {                                            \
     if ((call) != cudaSuccess) return kCudaFailure; \
@@ -552,6 +567,10 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       int w = std::min(std::min(o.nb, ws.w_max), E - b);
       int G = 1, R = 1;
       const bool use_cluster = o.panel_kernel != 2 && plan_cluster(m - b, w, di, G, R);
+      // panel_kernel 1 is the cluster panel or nothing: the grid panel's
+      // mailboxes may not exist in the workspace (the allocation-free path
+      // lays them out with zero size)
+      if (!use_cluster && o.panel_kernel == 1) return kInvalidArgument;
       if (!use_cluster && !plan_panel(m - b, w, o.panel_rows, di, G, R)) return kInvalidArgument;
       const bool enqueue = la && use_cluster;
       if (!enqueue && unread) {
@@ -791,6 +810,7 @@ bool resolve_options(const dp_options* in, Options& o) {
 
 int getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* info,
                  cudaStream_t st, const dp_options* opt) {
+  clear_report();
   if (info == nullptr) return kInvalidArgument;
   *info = -1;
   Options o;
@@ -799,7 +819,10 @@ int getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* 
   const int pivots = std::min(m, n);
   *info = pivots;
   for (int k = 0; k < pivots; ++k) ipiv[k] = jpiv[k] = k;
-  if (pivots == 0) return kOk;
+  if (pivots == 0) {
+    g_report.info = 0;
+    return kOk;
+  }
 
   DeviceInfo di;
   if (device_info(di) != kOk) {
@@ -865,11 +888,13 @@ int getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* 
             cudaSuccess)
       status = kCudaFailure;
   }
+  State fin{};
   if (status == kOk) {
     if (cudaMemcpyAsync(ipiv, ws.d_ipiv, sizeof(int) * pivots, cudaMemcpyDeviceToHost, st) !=
             cudaSuccess ||
         cudaMemcpyAsync(jpiv, ws.d_jpiv, sizeof(int) * pivots, cudaMemcpyDeviceToHost, st) !=
-            cudaSuccess)
+            cudaSuccess ||
+        cudaMemcpyAsync(&fin, ws.state, sizeof(State), cudaMemcpyDeviceToHost, st) != cudaSuccess)
       status = kCudaFailure;
   }
   cudaFreeAsync(base, st);
@@ -889,17 +914,20 @@ int getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* 
     return status;
   }
   *info = inf;
+  set_report(fin, inf);
   return kOk;
 }
 
 int getrf_host(int m, int n, double* a, int lda, int* ipiv, int* jpiv, int* info,
                cudaStream_t st, const dp_options* opt) {
+  clear_report();
   if (info == nullptr) return kInvalidArgument;
   *info = -1;
   if (!valid_arguments(m, n, a, lda, ipiv, jpiv)) return kInvalidArgument;
   const int pivots = std::min(m, n);
   if (pivots == 0) {  // delayed_dgetrf_cuda.cu:456-460
     *info = 0;
+    g_report.info = 0;
     return kOk;
   }
   size_t bytes = 0;
@@ -917,6 +945,7 @@ int getrf_host(int m, int n, double* a, int lda, int* ipiv, int* jpiv, int* info
         cudaStreamSynchronize(st) != cudaSuccess) {
       *info = -1;
       status = kCudaFailure;
+      clear_report();
     }
   }
   cudaFreeAsync(d_a, st);
@@ -948,8 +977,9 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratch
 // Device address of g_noalloc_scratch per device, looked up once (the host
 // name of a __device__ array is only a host-side handle, never a device
 // address).  The lookup is a host-side query and allocates nothing; it runs
-// on the first call on each device, which must therefore come before any
-// stream capture that contains the call.
+// on the first call on each device.  The entry point reads the pivot state
+// from the device during the call and synchronises its stream before it
+// returns, as every getrf entry point does.
 std::mutex g_noalloc_mutex;
 void* g_noalloc_ptr[64] = {};
 
@@ -971,6 +1001,7 @@ int noalloc_scratch(void** out) {
 
 int getrf_device_noalloc(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* info,
                          cudaStream_t st) {
+  clear_report();
   if (info == nullptr) return kInvalidArgument;
   *info = -1;
   if (!valid_arguments(m, n, d_a, lda, ipiv, jpiv)) return kInvalidArgument;
@@ -987,7 +1018,10 @@ int getrf_device_noalloc(int m, int n, double* d_a, int lda, int* ipiv, int* jpi
   }
   *info = pivots;
   for (int k = 0; k < pivots; ++k) ipiv[k] = jpiv[k] = k;
-  if (pivots == 0) return kOk;
+  if (pivots == 0) {
+    g_report.info = 0;
+    return kOk;
+  }
 
   void* scratch = nullptr;
   if (noalloc_scratch(&scratch) != kOk) {
@@ -1012,11 +1046,13 @@ int getrf_device_noalloc(int m, int n, double* d_a, int lda, int* ipiv, int* jpi
   sc.r1 = &rec;
   sc.r2 = &rec;
   if (status == kOk) status = factorize(m, n, d_a, lda, o, ws, di, sc, inf);
+  State fin{};
   if (status == kOk) {
     if (cudaMemcpyAsync(ipiv, ws.d_ipiv, sizeof(int) * pivots, cudaMemcpyDeviceToHost, st) !=
             cudaSuccess ||
         cudaMemcpyAsync(jpiv, ws.d_jpiv, sizeof(int) * pivots, cudaMemcpyDeviceToHost, st) !=
-            cudaSuccess)
+            cudaSuccess ||
+        cudaMemcpyAsync(&fin, ws.state, sizeof(State), cudaMemcpyDeviceToHost, st) != cudaSuccess)
       status = kCudaFailure;
   }
   if (cudaStreamSynchronize(st) != cudaSuccess && status == kOk) status = kCudaFailure;
@@ -1026,6 +1062,7 @@ int getrf_device_noalloc(int m, int n, double* d_a, int lda, int* ipiv, int* jpi
     return status;
   }
   *info = inf;
+  set_report(fin, inf);
   return kOk;
 }
 
@@ -1074,6 +1111,12 @@ int dp_getrf_hybrid_device(int m, int n, double* d_a, int lda, int* ipiv, int* j
 int dp_getrf_hybrid_host(int m, int n, double* a, int lda, int* ipiv, int* jpiv, int* info,
                          void* stream) {
   return dp_getrf_host(m, n, a, lda, ipiv, jpiv, info, stream);
+}
+
+int dp_getrf_last_report(dp_getrf_report* out) {
+  if (!out) return DP_INVALID_ARGUMENT;
+  *out = dp::g_report;
+  return DP_SUCCESS;
 }
 
 void dp_stats_enable(int on) {

@@ -44,14 +44,37 @@ struct __align__(16) CandSlot {
   int row;     // global row, -1 when the CTA has no candidate
   int pad;
   double inv;  // reciprocal of the candidate's entry in the current column
-  double pad2;
+  double sec;  // runner-up magnitude among the CTA's rows (near-tie detector)
 };
 
 struct __align__(16) LocalBest {
   double val;
-  int row;  // local row, -1 when none
+  int row;     // local row, -1 when none
   int pad;
+  double sec;  // largest magnitude among the other rows seen
 };
+
+// Offers magnitude v of local row r to a running (best, runner-up) pair.
+// Equal magnitudes keep the earlier row (rows arrive in increasing order per
+// thread) and make the runner-up equal to the best: an exact tie.
+__device__ __forceinline__ void offer(LocalBest& b, double v, int r) {
+  if (v > b.val) {
+    b.sec = b.val;
+    b.val = v;
+    b.row = r;
+  } else if (v > b.sec) {
+    b.sec = v;
+  }
+}
+
+// Largest of the lanes' non-negative magnitudes (bit-pattern order).
+__device__ __forceinline__ double warp_max_pos(double v) {
+  const unsigned long long u = (unsigned long long)__double_as_longlong(v);
+  const unsigned hi = (unsigned)(u >> 32), lo = (unsigned)u;
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+  return __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
+}
 
 // Best (largest magnitude, then smallest row) over the warp's lanes, every
 // lane getting the result.  Magnitudes are >= 0 and a missing candidate
@@ -78,11 +101,15 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// Best of the warp's (best, runner-up) pairs; the runner-up of the union is
+// the largest of the winner lane's runner-up and every other lane's best.
 __device__ __forceinline__ LocalBest warp_lb(LocalBest v) {
   double bv;
   int br;
   warp_best(v.row >= 0 ? v.val : 0.0, v.row >= 0 ? v.row : 0x7fffffff, bv, br);
-  return LocalBest{br == 0x7fffffff ? 0.0 : bv, br == 0x7fffffff ? -1 : br, 0};
+  const bool win = v.row >= 0 && v.row == br;
+  const double sec = warp_max_pos(win ? v.sec : (v.row >= 0 ? v.val : v.sec));
+  return LocalBest{br == 0x7fffffff ? 0.0 : bv, br == 0x7fffffff ? -1 : br, 0, sec};
 }
 
 }  // namespace
@@ -131,16 +158,10 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
   }
   __syncthreads();
 
-  LocalBest mine{0.0, -1, 0};
+  LocalBest mine{0.0, -1, 0, 0.0};
   {
     const int kl0 = (int)((long long)p.begin - row0);
-    for (int r = max(0, kl0) + tid; r < rows_here; r += blockDim.x) {
-      const double v = fabs(sm[r]);
-      if (v > mine.val) {
-        mine.val = v;
-        mine.row = r;
-      }
-    }
+    for (int r = max(0, kl0) + tid; r < rows_here; r += blockDim.x) offer(mine, fabs(sm[r]), r);
   }
 
   // End of a sub-panel that executed kd steps at [base, base + kd): solve its
@@ -150,7 +171,7 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
   // pivot only).  Called with kd = 0 only when the panel stops.
   auto sub_panel_end = [&](int kd, int base, int send) {
     __syncthreads();  // psave complete, this CTA's rows updated
-    mine = LocalBest{0.0, -1, 0};
+    mine = LocalBest{0.0, -1, 0, 0.0};
     if (kd == 0) return;
     // U12 = L11^{-1} A12 of the sub-panel, one column per thread, in registers
     for (int c = send + tid; c < w; c += blockDim.x) {
@@ -190,11 +211,7 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
         for (int t = 0; t < kSub; ++t)
           if (t < kd) x = fma(-l[t], ps[t * W1 + send], x);
         row[send * RP] = x;
-        const double av = fabs(x);
-        if (av > mine.val) {
-          mine.val = av;
-          mine.row = r;
-        }
+        offer(mine, fabs(x), r);
       }
 #pragma unroll 4
       for (int c = send + 1; c < w; ++c) {
@@ -216,13 +233,14 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
 
     // 1. CTA candidate (every thread reduces the per-warp results itself).
     if (positioned) {
-      mine = LocalBest{0.0, -1, 0};
-      if (own_k && tid == 0) mine = LocalBest{__longlong_as_double(0x7ff0000000000000ll), kl, 0};
+      mine = LocalBest{0.0, -1, 0, 0.0};
+      if (own_k && tid == 0)
+        mine = LocalBest{__longlong_as_double(0x7ff0000000000000ll), kl, 0, 0.0};
     }
     mine = warp_lb(mine);
     if (lane == 0) red[warp] = mine;
     __syncthreads();
-    const LocalBest cb = warp_lb(lane < nwarps ? red[lane] : LocalBest{0.0, -1, 0});
+    const LocalBest cb = warp_lb(lane < nwarps ? red[lane] : LocalBest{0.0, -1, 0, 0.0});
 
     // 2. Push (value, row), the candidate row and row k into every CTA.
     {
@@ -259,7 +277,7 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
         cs.row = cb.row >= 0 ? (int)(row0 + cb.row) : -1;
         cs.pad = 0;
         cs.inv = cb.row >= 0 ? 1.0 / sm[s * RP + cb.row] : 0.0;
-        cs.pad2 = 0.0;
+        cs.sec = cb.sec;
         *cluster.map_shared_rank(cands + par * 16 + rank, tid) = cs;
       }
     }
@@ -272,6 +290,9 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
       double bv;
       int brow;
       warp_best(c.row >= 0 ? c.val : 0.0, c.row >= 0 ? c.row : 0x7fffffff, bv, brow);
+      // runner-up over the cluster: the winner slot's runner-up, every other slot's best
+      win.sec = warp_max_pos((c.row >= 0 && c.row == brow) ? c.sec
+                                                           : (c.row >= 0 ? c.val : c.sec));
       if (brow != 0x7fffffff) {
         // the slot holding the winner (global rows are unique)
         const int src = __ffs(__ballot_sync(0xffffffffu, c.row == brow && lane < C)) - 1;
@@ -280,6 +301,7 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
         win.inv = __shfl_sync(0xffffffffu, c.inv, max(src, 0));
       }
     }
+    if (rank == 0 && tid == 0 && !positioned) note_decision(p.state, k, win.val, win.sec);
     const bool stop = !positioned && !(win.row >= 0 && win.val > p.threshold);
     if (stop) {
       if (rank == 0 && tid == 0) p.state->stop_k = (int)k;
@@ -321,7 +343,7 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
     pv[0] = 0.0;
 #pragma unroll
     for (int t = 1; t < kSub; ++t) pv[t] = s + t < send ? pr[s + t] : 0.0;
-    mine = LocalBest{0.0, -1, 0};
+    mine = LocalBest{0.0, -1, 0, 0.0};
 #pragma unroll 2
     for (int r = max(0, kl + 1) + tid; r < rows_here; r += blockDim.x) {
       double* __restrict__ row = sm + r;
@@ -340,13 +362,7 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
           x[t] = fma(-l, pv[t], x[t]);
           row[(s + t) * RP] = x[t];
         }
-      if (s + 1 < send) {
-        const double av = fabs(x[1]);
-        if (av > mine.val) {
-          mine.val = av;
-          mine.row = r;
-        }
-      }
+      if (s + 1 < send) offer(mine, fabs(x[1]), r);
     }
     if (s + 1 == send && send < w) sub_panel_end(s + 1 - base, base, send);
   }

@@ -20,6 +20,7 @@ namespace {
 
 constexpr int kSearchThreads = 256;
 
+// Lane 0 gets the warp's best candidate and runner-up.
 __device__ __forceinline__ Cand warp_best_cand(Cand v) {
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
@@ -27,7 +28,8 @@ __device__ __forceinline__ Cand warp_best_cand(Cand v) {
     o.val = __shfl_down_sync(0xffffffffu, v.val, off);
     o.row = __shfl_down_sync(0xffffffffu, v.row, off);
     o.col = __shfl_down_sync(0xffffffffu, v.col, off);
-    if (cand_better(o, v)) v = o;
+    o.sec = __shfl_down_sync(0xffffffffu, v.sec, off);
+    v = cand_merge(v, o);
   }
   return v;
 }
@@ -38,7 +40,7 @@ __device__ Cand block_best(Cand v, Cand* red) {
   if (lane == 0) red[warp] = v;
   __syncthreads();
   if (warp == 0) {
-    Cand x = lane < (int)(blockDim.x >> 5) ? red[lane] : Cand{0.0, 0x7fffffff, 0x7fffffff};
+    Cand x = lane < (int)(blockDim.x >> 5) ? red[lane] : Cand{0.0, 0x7fffffff, 0x7fffffff, 0.0};
     x = warp_best_cand(x);
     if (lane == 0) red[0] = x;
   }
@@ -56,13 +58,13 @@ search_active_kernel(const double* a, long long lda, int m, int n, int k, State*
   const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   // Start from (0, k, k): a zero or NaN never replaces it, so an all-zero
   // active block reports magnitude 0 at (k, k).
-  Cand best{0.0, k, k};
+  Cand best{0.0, k, k, 0.0};
   for (long long j = k + gw; j < n; j += warps_total) {
     const double* col = a + idx(0, j, lda);
     for (long long r = k + lane; r < m; r += 32) {
       const double v = fabs(col[r]);
-      const Cand c{v, (int)r, (int)j};
-      if (cand_better(c, best)) best = c;
+      const Cand c{v, (int)r, (int)j, 0.0};
+      best = cand_merge(best, c);
     }
   }
   best = block_best(best, red);
@@ -75,15 +77,13 @@ search_active_kernel(const double* a, long long lda, int m, int n, int k, State*
   __syncthreads();
   if (!last) return;
   __threadfence();
-  Cand v{0.0, k, k};
-  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
-    const Cand c = block_cands[i];
-    if (cand_better(c, v)) v = c;
-  }
+  Cand v{0.0, k, k, 0.0};
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) v = cand_merge(v, block_cands[i]);
   v = block_best(v, red);
   if (threadIdx.x == 0) {
     state->fallback = v;
     state->search_done = 0;
+    note_decision(state, k, v.val, v.sec);
   }
 }
 
@@ -119,24 +119,24 @@ search_nonzero_column_kernel(const double* a, long long lda, int m, int n, int k
   if (!last) return;
   __threadfence();
   const int j = *(volatile int*)&state->fallback.col;
-  Cand v{0.0, k, k};
+  Cand v{0.0, k, k, 0.0};
   if (j > k) {
     const double* col = a + idx(0, j, lda);
-    for (long long r = k + threadIdx.x; r < m; r += blockDim.x) {
-      const Cand c{fabs(col[r]), (int)r, j};
-      if (cand_better(c, v)) v = c;
-    }
+    for (long long r = k + threadIdx.x; r < m; r += blockDim.x)
+      v = cand_merge(v, Cand{fabs(col[r]), (int)r, j, 0.0});
   }
   v = block_best(v, red);
   if (threadIdx.x == 0) {
-    if (j <= k) v = Cand{0.0, k, k};
+    if (j <= k) v = Cand{0.0, k, k, 0.0};
     state->fallback = v;
     state->search_done = 0;
+    // the column is chosen exactly (nonzero or not); its row is an argmax
+    note_decision(state, k, v.val, v.sec);
   }
 }
 
 __global__ void reset_fallback_kernel(State* state, int k) {
-  state->fallback = Cand{0.0, k, -1};
+  state->fallback = Cand{0.0, k, -1, 0.0};
   state->search_done = 0;
 }
 

@@ -8,6 +8,10 @@
 
 namespace dp {
 namespace batch {
+// Bytes of the scratch `d_queue` of launch_raw: the work counter and the
+// launch's near-tie counters (decisions checked, order-sensitive decisions,
+// largest runner-up / winner ratio as bits) at byte 8.
+constexpr size_t kQueueBytes = 32;
 // The batched factorisation on caller-managed device arrays (batched.cu).
 int launch_raw(int count, int max_n, int sms, const int* d_n, const long long* d_off,
                const long long* d_rec, const int* d_order, int* d_queue, double* base, int* ipiv,

@@ -186,6 +186,8 @@ int getrs_device(int n, int nrhs, const double* lu, int ldlu, const int* ipiv, c
       cudaSuccess) {
     cudaGetLastError();
     cudaFreeAsync(d_perm, st);
+    cudaFreeAsync(flags, st);
+    cudaFreeAsync(inv, st);
     return kAllocationFailed;
   }
   int status = kOk;

@@ -47,6 +47,22 @@ class IRResult(ctypes.Structure):
     ]
 
 
+class GetrfReport(ctypes.Structure):
+    """dp_getrf_report: pivot decisions checked by the near-tie detector."""
+
+    _fields_ = [
+        ("decisions", ctypes.c_longlong),
+        ("near_ties", ctypes.c_longlong),
+        ("max_closeness", ctypes.c_double),
+        ("info", ctypes.c_int),
+        ("reserved", ctypes.c_int * 3),
+    ]
+
+    def as_dict(self):
+        return {"decisions": int(self.decisions), "near_ties": int(self.near_ties),
+                "max_closeness": float(self.max_closeness), "info": int(self.info)}
+
+
 class BatchOptions(ctypes.Structure):
     """dp_batch_options: threshold, precision, panel width per order bucket."""
 
@@ -320,6 +336,19 @@ def getrf_device_ex(m, n, d_a, lda, ipiv, jpiv, stream=None, nb=64, threshold=0.
     return st, info.value
 
 
+def getrf_last_report() -> dict:
+    """dp_getrf_last_report: the near-tie report of this thread's last
+    dp_getrf_* call (decisions, near_ties, max_closeness, info)."""
+    L = lib()
+    L.dp_getrf_last_report.restype = ctypes.c_int
+    L.dp_getrf_last_report.argtypes = [ctypes.POINTER(GetrfReport)]
+    r = GetrfReport()
+    st = L.dp_getrf_last_report(ctypes.byref(r))
+    if st != SUCCESS:
+        raise RuntimeError(f"dp_getrf_last_report: status {st}")
+    return r.as_dict()
+
+
 def getrs_device(n, nrhs, d_lu, ldlu, ipiv, jpiv, d_b, ldb, stream=None):
     """dp_getrs_device: solve with the factors of getrf; d_b overwritten."""
     return lib().dp_getrs_device(n, nrhs, _dptr(d_lu), ldlu, _iptr(ipiv), _iptr(jpiv),
@@ -418,6 +447,18 @@ class Batch:
     def getrf_graph(self, d_base, d_ipiv, d_jpiv, d_info, stream=None) -> int:
         return lib().dp_batch_getrf_graph(self._h, _dptr(d_base), _dptr(d_ipiv), _dptr(d_jpiv),
                                           _dptr(d_info), _stream(stream))
+
+    def last_report(self) -> dict:
+        """dp_batch_last_report: near-tie counts summed over the last launch
+        (synchronises the device)."""
+        L = lib()
+        L.dp_batch_last_report.restype = ctypes.c_int
+        L.dp_batch_last_report.argtypes = [ctypes.c_void_p, ctypes.POINTER(GetrfReport)]
+        r = GetrfReport()
+        st = L.dp_batch_last_report(self._h, ctypes.byref(r))
+        if st != SUCCESS:
+            raise BatchError(st, "dp_batch_last_report")
+        return r.as_dict()
 
     def close(self):
         if getattr(self, "_h", None):

@@ -90,8 +90,9 @@ int dp_getrf_hybrid_host(int m, int n, double *a, int lda, int *ipiv, int *jpiv,
  * kernel; larger inputs return DP_INVALID_ARGUMENT with info = -1.  All calls
  * share the array: calls that overlap on the GPU (other threads, other
  * streams) race and must be serialised by the caller.  The first call on a
- * device looks the array's device address up; make it before capturing a
- * stream that contains the call. */
+ * device looks the array's device address up once (a host-side query that
+ * allocates nothing).  Like every dp_getrf_* entry point it reads the pivot
+ * state during the call and synchronises `stream` before returning. */
 int dp_getrf_device_noalloc(int m, int n, double *d_a, int lda, int *ipiv, int *jpiv, int *info,
                             void *stream);
 
@@ -99,6 +100,29 @@ int dp_getrf_device_noalloc(int m, int n, double *d_a, int lda, int *ipiv, int *
  * column-fallback policy of delayed_lu/delayed_dgetrf_column.hpp:18. */
 int dp_getrf_device_ex(int m, int n, double *d_a, int lda, int *ipiv, int *jpiv, int *info,
                        void *stream, const dp_options *opt);
+
+/* Near-tie report (no reference counterpart; the reference decides every
+ * pivot by a bare argmax, delayed_lu/delayed_dgetrf.cpp:170-178 and :32-47,
+ * delayed_lu_cuda/delayed_dgetrf_cuda.cu:13-20).  Every pivot decision of a
+ * factorisation - the column search of each panel step and each fallback
+ * search - also finds the runner-up magnitude.  A decision is order-sensitive
+ * when (best - second) <= 4 (k + 1) u best (u = 2^-53, k the step): the
+ * rounding of another summation order could swap the two, so a records match
+ * with the reference is only meaningful where near_ties == 0.  Decisions on a
+ * zero winner (stop / delay) are exact and never count.  Not covered: the
+ * grid-wide panel kernel (dp_options.panel_kernel = 2, or panels too tall for
+ * a 16-CTA cluster), whose steps are not counted in `decisions`. */
+typedef struct dp_getrf_report {
+  long long decisions;  /* pivot decisions whose runner-up was compared */
+  long long near_ties;  /* order-sensitive decisions among them */
+  double max_closeness; /* largest second / best over those decisions (1: an exact tie) */
+  int info;             /* info of the call (-1: the call failed) */
+  int reserved[3];
+} dp_getrf_report;
+
+/* The report of the calling host thread's last dp_getrf_* call (device, host,
+ * _ex, _noalloc; C++ delayed_getrf_cuda_* alike). */
+int dp_getrf_last_report(dp_getrf_report *report);
 
 /* Solve A X = B with the factors of dp_getrf_device (no reference
  * counterpart: the reference stops at the factorisation).  P*A*Q = L*U from
@@ -193,6 +217,10 @@ int dp_batch_getrf_async(dp_batch *plan, double *d_base, int *d_ipiv, int *d_jpi
 int dp_batch_getrf_graph(dp_batch *plan, double *d_base, int *d_ipiv, int *d_jpiv, int *d_info,
                          void *stream);
 void dp_batch_destroy(dp_batch *plan);
+/* Near-tie report (see dp_getrf_report) summed over every matrix of the
+ * plan's last launch; `info` holds the number of matrices.  Synchronises the
+ * device (cudaDeviceSynchronize) before it reads the plan's counters. */
+int dp_batch_last_report(dp_batch *plan, dp_getrf_report *report);
 
 /* Autotuner: for each bucket, times every candidate panel width on `samples`
  * seeded N(0,1) matrices whose orders spread log-uniformly over the bucket,

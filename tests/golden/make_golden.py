@@ -4,7 +4,8 @@ delayed_dgetrf_column.cpp, compiled unmodified into oracle/_ref/ against
 OpenBLAS).  Run from the repository root:
 
     python tests/golden/make_golden.py            # all cases except n=16384
-    python tests/golden/make_golden.py --large    # also the n=16384 case
+    python tests/golden/make_golden.py --large    # also the n=16384 and n=32768 cases
+    python tests/golden/make_golden.py --only config2_n32768   # one generated case
 
 It also writes tests/golden/batch/config4_subset64.npz: the reference's
 records for a seeded 64-matrix subset of the batched workload (orders
@@ -47,7 +48,8 @@ GENERATED = [
     ("row_1x6", 1, 6, 1, 5, 0, 0, 0),
     ("all_zero_9x9", 9, 9, 9, 6, 0, 9, 0),
 ]
-LARGE = [("config2_n16384", 16384, 16384, 16384, 16384, 16, 3, 0)]
+LARGE = [("config2_n16384", 16384, 16384, 16384, 16384, 16, 3, 0),
+         ("config2_n32768", 32768, 32768, 32768, 32768, 32, 6, 0)]
 BATCH_SUBSET = ("config4_subset64", 64, 8192)  # (name, count, seed)
 
 
@@ -90,8 +92,15 @@ def run_reference(a, m, n, policy):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--large", action="store_true")
+    ap.add_argument("--only", default=None, help="write only this generated case")
     args = ap.parse_args()
     orc.build(ref=True)
+    if args.only:
+        for case in GENERATED + LARGE:
+            if case[0] == args.only:
+                write_generated(*case)
+                return
+        raise SystemExit(f"no generated case {args.only}")
     for name, a, expect in reference_known_answer():
         m, n = a.shape
         ipiv, jpiv, info, res = run_reference(a, m, n, 0)
@@ -99,16 +108,20 @@ def main():
         np.savez_compressed(OUT / f"{name}.npz", kind="literal", matrix=a, m=m, n=n, lda=m,
                             policy=0, ipiv=ipiv, jpiv=jpiv, info=info, scaled_residual=res)
         print(f"{name}: info={info} scaled_residual={res:.3g}")
-    cases = GENERATED + (LARGE if args.large else [])
-    for name, m, n, lda, seed, nt, nz, policy in cases:
-        a = dp.planted_matrix(m, n, seed, nt, nz, lda=lda)
-        ipiv, jpiv, info, res = run_reference(a, m, n, policy)
-        np.savez_compressed(OUT / f"{name}.npz", kind="generated", m=m, n=n, lda=lda, seed=seed,
-                            n_tiny=nt, n_zero=nz, policy=policy, ipiv=ipiv, jpiv=jpiv, info=info,
-                            scaled_residual=res)
-        swaps = int((jpiv != np.arange(len(jpiv))).sum())
-        print(f"{name}: info={info} column_swaps={swaps} scaled_residual={res:.3g}")
+    for case in GENERATED + (LARGE if args.large else []):
+        write_generated(*case)
     batch_subset()
+
+
+def write_generated(name, m, n, lda, seed, nt, nz, policy):
+    a = dp.planted_matrix(m, n, seed, nt, nz, lda=lda)
+    ipiv, jpiv, info, res = run_reference(a, m, n, policy)
+    del a
+    np.savez_compressed(OUT / f"{name}.npz", kind="generated", m=m, n=n, lda=lda, seed=seed,
+                        n_tiny=nt, n_zero=nz, policy=policy, ipiv=ipiv, jpiv=jpiv, info=info,
+                        scaled_residual=res)
+    swaps = int((jpiv != np.arange(len(jpiv))).sum())
+    print(f"{name}: info={info} column_swaps={swaps} scaled_residual={res:.3g}")
 
 
 def batch_subset():

@@ -157,6 +157,10 @@ def test_batched_records_equal_reference_subset(built, graph):
     assert np.array_equal(info, f["info"])
     assert np.array_equal(ipiv, f["ipiv"])
     assert np.array_equal(jpiv, f["jpiv"])
+    # no pivot decision of the launch was order-sensitive (near-tie detector)
+    rep = b.last_report()
+    assert rep["near_ties"] == 0 and rep["decisions"] >= int(info.sum()), rep
+    assert rep["info"] == len(ns)
     check_residuals(b, host, fac, ns, ipiv, jpiv, info)
 
 
@@ -171,6 +175,7 @@ def test_batched_panel_width_does_not_change_records(built, nb):
                                                options=dp.batch_options(nb_bucket=nb))
     assert np.array_equal(info, f["info"])
     assert np.array_equal(ipiv, f["ipiv"]) and np.array_equal(jpiv, f["jpiv"])
+    assert b.last_report()["near_ties"] == 0
     check_residuals(b, host, fac, ns, ipiv, jpiv, info, every=3)
 
 
@@ -322,3 +327,34 @@ def test_batched_empty_batch(built):
     i = torch.zeros(1, dtype=torch.int32, device="cuda")
     assert b.getrf_async(x, i, i, i) == 0
     assert b.getrf_graph(x, i, i, i) == 0
+
+
+@pytest.mark.gpu
+def test_batched_near_tie_detector_counts_planted_ties(built):
+    """Two matrices of one launch carry a planted exact tie (step 0 column
+    search; 2-D fallback search), one does not: the launch's report counts
+    the two ties, and the records still follow the reference's tie rule."""
+    import delayed_pivoting as dp
+    import oracle as orc
+
+    mats = []
+    for seed, kind in ((11, "col"), (12, "none"), (13, "fallback")):
+        a = dp.planted_matrix(200, 200, seed)
+        a[:, 0] *= 0.1
+        if kind == "col":
+            a[5, 0], a[9, 0] = 10.0, -10.0
+        elif kind == "fallback":
+            a[:, 0] = 0.0
+            a[:, 2:5] *= 0.1
+            a[3, 4], a[6, 2] = 7.0, -7.0
+        mats.append(a)
+    ns = np.array([200, 200, 200], dtype=np.int32)
+    b, host, fac, ipiv, jpiv, info = run_batch(ns, None, 0, matrices=mats)
+    ip, jp = split_records(ipiv, ns), split_records(jpiv, ns)
+    for i, a in enumerate(mats):
+        oi, oj, oinfo = orc.oracle_getrf(a.copy(order="F"))
+        assert info[i] == oinfo
+        assert np.array_equal(ip[i], oi) and np.array_equal(jp[i], oj)
+    rep = b.last_report()
+    assert rep["near_ties"] == 2, rep
+    assert rep["max_closeness"] == 1.0 and rep["info"] == 3

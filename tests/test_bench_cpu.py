@@ -23,3 +23,27 @@ def test_cpu_baselines_time_the_reference_and_lapack(built):
         assert lap is not None and lap[0] > 0 and lap[1] > 0
     else:
         assert lap is None
+
+
+def test_serve_cpu_baseline_covers_the_whole_stream(built):
+    """The serve CPU leg and the reference arm share one function: every
+    distinct order of the stream is factored once, and the stream's CPU time
+    weights those times by the counts of ALL the stream's requests (no request
+    is skipped), so both report the same solves/s for the same stream."""
+    for p in (str(ROOT), str(ROOT / "delayed-pivoting_b200"), str(ROOT / "oracle")):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    import bench
+    from delayed_pivoting import serving as sv
+
+    reqs = sv.make_stream(40, 5, hi=256)
+    out = bench._cpu_serve_baseline(reqs, 5, lapack=False)
+    orders = sorted({q.n for q in reqs})
+    assert out["requests"] == len(reqs)
+    assert out["solves"] == sum(len(q.solves) for q in reqs)
+    assert sorted(int(k) for k in out["per_order_s"]) == orders
+    expect = sum(out["per_order_s"][str(q.n)] for q in reqs)
+    assert abs(out["stream_cpu_s"] - expect) <= 1e-3 * expect + 1e-4
+    assert out["value"] > 0 and out["cores"] >= 1
+    part = bench._cpu_serve_baseline(reqs, 5, orders=orders[:2], lapack=False)
+    assert part["requests"] == sum(1 for q in reqs if q.n in orders[:2])

@@ -21,6 +21,19 @@ def _torch():
     return torch
 
 
+def assert_no_near_ties(info):
+    """The near-tie detector saw every pivot decision of the last call and
+    none of them was order-sensitive, so a records match is not luck."""
+    import delayed_pivoting as dp
+
+    rep = dp.getrf_last_report()
+    assert rep["info"] == info
+    assert rep["near_ties"] == 0, rep
+    assert rep["decisions"] >= info, rep
+    assert 0.0 <= rep["max_closeness"] < 1.0 or info == 0, rep
+    return rep
+
+
 def run_device(a, m, n, **opts):
     """Factors a (host Fortran array) on the GPU through dp_getrf_device[_ex];
     returns (factor (host), ipiv, jpiv, info, status)."""
@@ -54,6 +67,7 @@ def test_records_match_reference(built, name):
     assert info == case["info"]
     np.testing.assert_array_equal(ipiv, case["ipiv"])
     np.testing.assert_array_equal(jpiv, case["jpiv"])
+    assert_no_near_ties(info)
     assert orc.scaled_residual(a, fac, m, n, info, ipiv, jpiv) <= 10.0
     if case["lda"] > m:  # padding rows below m are never touched
         np.testing.assert_array_equal(fac[m:, :], a[m:, :])
@@ -75,6 +89,7 @@ def test_panel_width_does_not_change_records(built, nb):
     assert st == 0 and info == case["info"]
     np.testing.assert_array_equal(ipiv, case["ipiv"])
     np.testing.assert_array_equal(jpiv, case["jpiv"])
+    assert_no_near_ties(info)
     assert orc.scaled_residual(a, fac, 2000, 2000, info, ipiv, jpiv) <= 10.0
 
 
@@ -226,17 +241,21 @@ def test_schur_update_against_torch(built, M, N, K):
 
 
 @pytest.mark.slow
-def test_config2_n16384_records_bit_identical(built):
-    """n = 16384, 16 tiny + 3 zero columns: records equal the reference's;
-    the residual is checked on the GPU (float64 products in torch)."""
+@pytest.mark.parametrize("n", [16384, 32768])
+def test_config2_records_bit_identical(built, n):
+    """n = 16384 (16 tiny + 3 zero columns) and n = 32768 (32 tiny + 6 zero
+    columns, 8.6 GB): records equal the reference's, with no order-sensitive
+    pivot decision; the residual is checked on the GPU (float64 products in
+    torch)."""
     import delayed_pivoting as dp
 
     torch = _torch()
-    if "config2_n16384" not in gc.names():
-        pytest.skip("n=16384 fixture not generated")
-    a, case = gc.load("config2_n16384")
-    n = 16384
-    d = torch.from_numpy(a.T.copy()).cuda()
+    name = f"config2_n{n}"
+    if name not in gc.names():
+        pytest.skip(f"{name} fixture not generated")
+    a, case = gc.load(name)
+    d = torch.from_numpy(np.ascontiguousarray(a.T)).cuda()
+    del a
     orig = d.clone()
     ipiv = np.zeros(n, dtype=np.int32)
     jpiv = np.zeros(n, dtype=np.int32)
@@ -245,7 +264,10 @@ def test_config2_n16384_records_bit_identical(built):
     assert st == 0 and info == case["info"]
     np.testing.assert_array_equal(ipiv, case["ipiv"])
     np.testing.assert_array_equal(jpiv, case["jpiv"])
+    assert_no_near_ties(info)
     assert scaled_residual_gpu(torch, orig, d, n, info, ipiv, jpiv) <= 10.0
+    del d, orig
+    torch.cuda.empty_cache()
 
 
 def scaled_residual_gpu(torch, orig_t, fac_t, n, info, ipiv, jpiv):
@@ -266,3 +288,67 @@ def scaled_residual_gpu(torch, orig_t, fac_t, n, info, ipiv, jpiv):
     U[info:, info:] = F[info:, info:]
     R = PAQ - L @ U
     return float(torch.linalg.norm(R) / (torch.linalg.norm(A) * n * 2.0**-53))
+
+
+def _tie_matrix(kind):
+    """300 x 300 N(0,1) with a planted decision at step 0: an exact tie
+    (+10 / -10), a near-tie one ulp apart, or a clear gap; or, with column 0
+    zero, an exact tie of the 2-D fallback search (+7 at column 4, -7 at
+    column 2: the smaller column wins)."""
+    import delayed_pivoting as dp
+
+    a = dp.planted_matrix(300, 300, 606)
+    a[:, 0] *= 0.1
+    if kind == "exact":
+        a[5, 0], a[9, 0] = 10.0, -10.0
+    elif kind == "ulp":
+        a[5, 0], a[9, 0] = 10.0, np.nextafter(10.0, 0.0)
+    elif kind == "clear":
+        a[5, 0], a[9, 0] = 10.0, 9.99
+    else:  # fallback search tie
+        a[:, 0] = 0.0
+        a[:, 2:5] *= 0.1
+        a[3, 4], a[6, 2] = 7.0, -7.0
+    return a
+
+
+@pytest.mark.parametrize("kind,flagged", [("exact", True), ("ulp", True), ("clear", False),
+                                          ("fallback", True)])
+def test_near_tie_detector_flags_planted_ties(built, kind, flagged):
+    """The detector counts a planted tie (and only it); the decision itself
+    still follows the reference's rule (first row; smaller column, then
+    smaller row), so the records equal the oracle's."""
+    import delayed_pivoting as dp
+    import oracle as orc
+
+    a = _tie_matrix(kind)
+    o = a.copy(order="F")
+    oi, oj, oinfo = orc.oracle_getrf(o)
+    fac, ipiv, jpiv, info, st = run_device(a, 300, 300)
+    assert st == 0 and info == oinfo
+    np.testing.assert_array_equal(ipiv, oi)
+    np.testing.assert_array_equal(jpiv, oj)
+    rep = dp.getrf_last_report()
+    assert rep["info"] == info and rep["decisions"] >= info
+    if flagged:
+        assert rep["near_ties"] >= 1, rep
+        assert rep["max_closeness"] >= 1.0 - 2.0**-50, rep
+    else:
+        assert rep["near_ties"] == 0, rep
+    if kind == "exact":
+        assert ipiv[0] == 5
+    if kind == "fallback":
+        assert ipiv[0] == 6 and jpiv[0] == 2
+
+
+def test_near_tie_report_of_failed_call(built):
+    """A rejected call leaves a report with info = -1 and no decisions."""
+    import delayed_pivoting as dp
+
+    _torch()
+    ipiv = np.zeros(4, dtype=np.int32)
+    jpiv = np.zeros(4, dtype=np.int32)
+    st, info = dp.delayed_getrf_cuda_device(4, 4, None, 4, ipiv, jpiv)
+    assert st == dp.INVALID_ARGUMENT and info == -1
+    rep = dp.getrf_last_report()
+    assert rep["info"] == -1 and rep["decisions"] == 0 and rep["near_ties"] == 0
