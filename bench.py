@@ -808,6 +808,41 @@ def _serve_e2e(torch, dp, sv, dist, dev, pool, rhs, reqs, warm):
             "violations": bad}
 
 
+def reference_cuda_figures(n, repeats=1, timeout=600):
+    """The reference's own cuBLAS GPU build timed by its own harness
+    (delayed_lu_cuda/benchmark.cu:38-72: best-of-repeats wall time around the
+    device call, 2/3 n^3 GFLOP/s, diagonally dominant U(-1,1) + n I input
+    from mt19937_64(20260807)), and the same unmodified harness linked against
+    this library (oracle/_ref/benchmark_on_b200, the drop-in build).  Each
+    line of the harness: "<name> best=<s> s, <GFLOP/s> GFLOP/s"."""
+    import re
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+
+    out = {}
+    for key, name in (("reference_cublas", "ref_cuda_benchmark"),
+                      ("this_library_via_reference_harness", "benchmark_on_b200")):
+        p = orc.ref_binary(name)
+        if p is None:
+            out[key] = {"unavailable": f"oracle/_ref/{name} not built"}
+            continue
+        try:
+            r = subprocess.run([str(p), str(n), str(repeats)], capture_output=True, text=True,
+                               timeout=timeout)
+        except subprocess.TimeoutExpired:
+            out[key] = {"unavailable": f"{name} {n} {repeats} exceeded {timeout} s"}
+            continue
+        rows = {}
+        for ln in r.stdout.splitlines():
+            m = re.match(r"(\S+)\s+best=\s*([0-9.eE+-]+) s,\s*([0-9.eE+-]+) GFLOP/s", ln.strip())
+            if m:
+                rows[m.group(1)] = {"seconds": float(m.group(2)), "gflops": float(m.group(3))}
+        out[key] = {"rc": r.returncode, "n": n, "repeats": repeats, "paths": rows,
+                    "harness": "delayed_lu_cuda/benchmark.cu (unmodified)"}
+    return out
+
+
 def lu_key(torch, dp, dev, L, n=16384, warmup=2, steps=3):
     """Config-2 check carried by the default line: plain FP64 delayed_getrf of
     the n = 16384 planted matrix (seed 16384, 16 tiny + 3 zero columns), time

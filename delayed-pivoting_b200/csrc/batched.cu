@@ -48,6 +48,7 @@
 
 #include "delayed_pivoting_b200.h"
 #include "dp_device.cuh"
+#include "dp_kernels.h"
 #include "serve_kernels.h"
 
 namespace dp {
@@ -678,6 +679,58 @@ __global__ void __launch_bounds__(kThreads, 1) batched_getrf_kernel(Params p) {
   }
 }
 
+// One panel of the blocked LU (PanelParams, the same contract as
+// panel_cluster_kernel) on ONE CTA, for panels of at most kMaxN rows and
+// kMaxNb columns: the rows stay in registers and the pivot decisions,
+// swaps (as relabelled row positions), scalings and rank-1 updates run with
+// one CTA barrier per step and no cluster exchange (panel_regs, the batched
+// kernel's panel).  Afterwards the composite row permutation is written as
+// the swap lists the laswp kernel applies outside the panel.
+__global__ void __launch_bounds__(kThreads, 1) panel_small_kernel(PanelParams p) {
+  // every thread reads the same word before any barrier or state write
+  if (p.gated && p.state->stop_k >= 0) return;
+  extern __shared__ __align__(16) double dsm[];
+  __shared__ Smem s;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int b = p.begin, w = p.end - p.begin;
+  const int pr = panel_ld(p.m - b);
+  if (tid == 0) {
+    p.state->stop_k = -1;
+    p.state->swap_count = 0;
+    p.state->block_changed = 0;
+  }
+  const int stop = panel_regs(p.a, p.m, (int)p.lda, b, w, p.positioned != 0, p.threshold, dsm, pr,
+                              s, p.ipiv, &p.state->ties_checked);
+  __syncthreads();  // rows written back, move list complete
+  for (int i = tid; i < w; i += kThreads) p.swap_block[i] = b + i;
+  __syncthreads();
+  const int cnt = s.mv_count;
+  int changed = 0;
+  for (int j0 = 0; j0 < cnt; j0 += kThreads) {  // whole warps: one atomic per warp
+    const int j = j0 + tid;
+    const bool on = j < cnt;
+    const int dst = on ? s.mv_dst[j] : 0, src = on ? s.mv_src[j] : 0;
+    if (on && dst < w) {
+      p.swap_block[dst] = b + src;
+      ++changed;
+    }
+    const bool below = on && dst >= w;
+    const unsigned bal = __ballot_sync(0xffffffffu, below);
+    if (bal) {
+      int slot = 0;
+      if (lane == 0) slot = atomicAdd(&p.state->swap_count, __popc(bal));
+      slot = __shfl_sync(0xffffffffu, slot, 0) + __popc(bal & ((1u << lane) - 1u));
+      if (below) {
+        p.swap_extra[2 * slot + 0] = b + dst;
+        p.swap_extra[2 * slot + 1] = b + src;
+      }
+    }
+  }
+  changed = __reduce_add_sync(0xffffffffu, changed);
+  if (lane == 0 && changed) atomicAdd(&p.state->block_changed, changed);
+  if (tid == 0 && stop >= 0) p.state->stop_k = b + stop;
+}
+
 size_t dynamic_smem(int max_n) {
   return ((size_t)panel_ld(std::max(max_n, 1)) * kMaxNb + (size_t)kStageN * kLdb) *
          sizeof(double);
@@ -788,6 +841,20 @@ int launch_raw(int count, int max_n, int sms, const int* d_n, const long long* d
 }
 
 }  // namespace batch
+
+int panel_small_max_rows() { return batch::kMaxN; }
+int panel_small_max_width() { return batch::kMaxNb; }
+
+int launch_panel_small(const PanelParams& pp, cudaStream_t st) {
+  const int rows = pp.m - pp.begin, w = pp.end - pp.begin;
+  if (rows < 1 || rows > batch::kMaxN || w < 1 || w > batch::kMaxNb) return kInvalidArgument;
+  const size_t smem = (size_t)batch::panel_ld(rows) * batch::kMaxNb * sizeof(double);
+  if (!ensure_smem((const void*)batch::panel_small_kernel, smem)) return kCudaFailure;
+  note_launch();
+  batch::panel_small_kernel<<<1, batch::kThreads, smem, st>>>(pp);
+  return cudaGetLastError() == cudaSuccess ? kOk : kCudaFailure;
+}
+
 }  // namespace dp
 
 namespace {

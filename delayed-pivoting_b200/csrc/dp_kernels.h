@@ -39,6 +39,12 @@ __global__ void panel_cluster_kernel(PanelParams p);
 size_t panel_cluster_smem_bytes(int w, int rows_per_cta);
 int panel_cluster_threads();
 constexpr int kPanelThreadsHost = 256;
+// Single-CTA panel (batched.cu) for panels of at most panel_small_max_rows()
+// rows and panel_small_max_width() columns: same contract as the cluster
+// panel, rows register-resident, one CTA barrier per step.
+int panel_small_max_rows();
+int panel_small_max_width();
+int launch_panel_small(const PanelParams& pp, cudaStream_t st);
 size_t panel_smem_bytes(int w, int rows_per_cta);
 
 // Applies the composite row permutation of one panel (swap list written by
@@ -169,5 +175,10 @@ int factor_create(Factor** out, int n, const double* A, int lda, int precision, 
 int factor_solve(Factor* f, const double* A, int lda, double* B, int ldb, int nrhs, int max_iter,
                  double tol, dp_ir_result* res, cudaStream_t st);
 void factor_destroy(Factor* f, cudaStream_t st);
+// Hager-Higham estimate of kappa_1(A) = ||A||_1 ||A^{-1}||_1 through the
+// factors held now (inv_norm: the estimate of ||A^{-1}||_1, may be null);
+// synchronises st.  A singular factorisation gives infinity.
+int factor_condest(Factor* f, const double* A, int lda, double* kappa, double* inv_norm,
+                   cudaStream_t st);
 
 }  // namespace dp

@@ -566,13 +566,18 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
     while (b < E) {
       int w = std::min(std::min(o.nb, ws.w_max), E - b);
       int G = 1, R = 1;
-      const bool use_cluster = o.panel_kernel != 2 && plan_cluster(m - b, w, di, G, R);
+      // short panels: one CTA, rows in registers (automatic choice only)
+      const bool use_small = o.panel_kernel == 0 && m - b <= panel_small_max_rows();
+      if (use_small) w = std::min(w, panel_small_max_width());
+      const bool use_cluster =
+          !use_small && o.panel_kernel != 2 && plan_cluster(m - b, w, di, G, R);
       // panel_kernel 1 is the cluster panel or nothing: the grid panel's
       // mailboxes may not exist in the workspace (the allocation-free path
       // lays them out with zero size)
       if (!use_cluster && o.panel_kernel == 1) return kInvalidArgument;
-      if (!use_cluster && !plan_panel(m - b, w, o.panel_rows, di, G, R)) return kInvalidArgument;
-      const bool enqueue = la && use_cluster;
+      if (!use_small && !use_cluster && !plan_panel(m - b, w, o.panel_rows, di, G, R))
+        return kInvalidArgument;
+      const bool enqueue = la && (use_cluster || use_small);
       if (!enqueue && unread) {
         // a synchronous panel follows enqueued ones: settle them first
         if (int err = read_state(hs, ws, st)) return err;
@@ -584,7 +589,7 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
         }
       }
       e = b + w;
-      if (la && !use_cluster) {
+      if (la && !use_cluster && !use_small) {
         // the cooperative grid needs all its CTAs resident: s2 finishes first
         DP_CHECK_CUDA(cudaEventRecord(sc.next, sc.s2));
         DP_CHECK_CUDA(cudaStreamWaitEvent(st, sc.next, 0));
@@ -611,7 +616,9 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       pp.swap_extra = la ? ext + 2 * (size_t)(b - B) : ws.swap_extra;
       pp.gated = enqueue ? 1 : 0;
       rec.begin(DP_KFAM_PANEL);
-      if (use_cluster) {
+      if (use_small) {
+        if (int err = launch_panel_small(pp, st)) return err;
+      } else if (use_cluster) {
         cudaLaunchConfig_t cfg = {};
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;

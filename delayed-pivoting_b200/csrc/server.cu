@@ -231,6 +231,7 @@ void dp_server::large_worker() {
       Factor* f = nullptr;
       r.status = dp::factor_create(&f, j.r.n, j.r.d_a, j.r.lda, opt.precision, st);
       r.info = f ? f->info : -1;
+      if (f) r.factor_ms = f->factor_ms;
       if (r.status == DP_SUCCESS) {
         r.status = dp::factor_solve(f, j.r.d_a, j.r.lda, j.r.d_b, j.r.ldb, j.r.nrhs, opt.max_iter,
                                     opt.tol, &ir, st);
@@ -239,6 +240,8 @@ void dp_server::large_worker() {
         r.iterations = ir.iterations;
         r.refactored = ir.refactored;
         r.backward_error = ir.backward_error;
+        r.factor_ms += ir.factor_ms;
+        r.solve_ms = ir.total_ms - ir.factor_ms;
       }
       if (r.status == DP_SUCCESS && j.r.followups > 0 && f && f->info == j.r.n) {
         keep = std::make_shared<Resident>();
@@ -262,6 +265,8 @@ void dp_server::large_worker() {
       r.iterations = ir.iterations;
       r.refactored = ir.refactored;
       r.backward_error = ir.backward_error;
+      r.factor_ms = ir.factor_ms;
+      r.solve_ms = ir.total_ms - ir.factor_ms;
     }
     r.t_done = clock_s();
     {

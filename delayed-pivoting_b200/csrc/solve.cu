@@ -100,6 +100,51 @@ __global__ void row_abs_sum_kernel(const double* __restrict__ A, long long lda, 
   if (i < n) atomic_max_pos(out, s == s ? s : __longlong_as_double(0x7ff0000000000000ll));
 }
 
+// out (n x n, leading dimension n) = in^T.  32 x 32 tiles through shared
+// memory (padded), both sides coalesced.
+__global__ void transpose_kernel(const double* __restrict__ in, long long ldi, double* out, int n) {
+  __shared__ double t[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int r = bx + threadIdx.x, c = by + k;
+    t[k][threadIdx.x] = (r < n && c < n) ? in[idx(r, c, ldi)] : 0.0;
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int r = by + threadIdx.x, c = bx + k;
+    if (r < n && c < n) out[idx(r, c, n)] = t[threadIdx.x][k];
+  }
+}
+
+// Diagonal-block inverses of the transposed factor: block i of `inv` holds
+// inv(L_ii) then inv(U_ii) (64 x 64 each, column-major); block i of `out`
+// gets inv(U_ii)^T = inv(U_ii^T) (the lower slot: U^T is the lower factor of
+// the transpose) then inv(L_ii)^T (the upper slot).
+__global__ void transpose_inverses_kernel(const double* __restrict__ inv, double* out, int blocks) {
+  constexpr int B = 64;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < 2LL * B * B * blocks;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long blk = e / (2 * B * B);
+    const int w = (int)(e % (2 * B * B));
+    const int slot = w / (B * B), el = w % (B * B), r = el % B, c = el / B;
+    const double* src = inv + blk * 2 * B * B + (slot == 0 ? B * B : 0);
+    out[e] = src[r * B + c];
+  }
+}
+
+// out[c] = sum_i |A(i, c)| over the n x n matrix, one warp per column; out
+// is the column sums (||A||_1 is their maximum).
+__global__ void col_abs_sum_kernel(const double* __restrict__ A, long long lda, int n, double* out) {
+  const int lane = threadIdx.x & 31;
+  const long long c = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  if (c >= n) return;
+  double s = 0.0;
+  for (int i = lane; i < n; i += 32) s += fabs(A[idx(i, c, lda)]);
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+  if (lane == 0) out[c] = s;
+}
+
 int grid_of(long long work) {
   long long g = (work + 255) / 256;
   return (int)std::max(1LL, std::min(g, 148LL * 16));
@@ -302,7 +347,150 @@ int solve_with(Factor& f, const double* B, int ldb, double* X, double* tmp, int 
   return cudaGetLastError() == cudaSuccess ? kOk : kCudaFailure;
 }
 
+// z = A^{-T} c through the factors: A^T = Q U^T L^T P, so with w[k] =
+// c[col[k]]: U^T v = w (lower solve on the transposed factor T = (L\U)^T),
+// L^T u = v (upper solve on T), z[row[k]] = u[k].  `lut` / `inv_t` are the
+// transpose of the compact factor and its transposed diagonal inverses.
+int solve_transposed(Factor& f, const double* lut, const double* inv_t, const double* c, double* z,
+                     double* tmp, cudaStream_t st) {
+  const int n = f.n;
+  dp::note_launch();
+  gather_rows_kernel<<<grid_of(n), 256, 0, st>>>(c, n, tmp, n, f.d_perm + n, n, 1);
+  int* status = reinterpret_cast<int*>(f.d_flags + tri_solve_flag_count(n));
+  for (int up = 0; up < 2; ++up) {
+    if (++f.epoch == 0) ++f.epoch;
+    const int s = up ? launch_tri_upper(lut, n, n, inv_t, tmp, n, 1, f.d_flags, f.epoch, status, st)
+                     : launch_tri_lower_unit(lut, n, n, inv_t, tmp, n, 1, f.d_flags, f.epoch,
+                                             status, st);
+    if (s != kOk) return s;
+  }
+  dp::note_launch();
+  scatter_rows_kernel<<<grid_of(n), 256, 0, st>>>(tmp, n, z, n, f.d_perm, n, 1);
+  return cudaGetLastError() == cudaSuccess ? kOk : kCudaFailure;
+}
+
 }  // namespace
+
+// Hager-Higham estimate of ||A^{-1}||_1 from the factors (Hager 1984, with
+// Higham's 1988 safeguards as in LAPACK's dlacon: at most 5 iterations, stop
+// when the sign vector repeats or the gradient test fails, then take the
+// larger of that estimate and 2 ||A^{-1} x||_1 / (3 n) for the alternating
+// vector x_i = (-1)^i (1 + i / (n - 1))); kappa_1 = ||A||_1 * estimate.  The
+// solves go through the factors held now (mixed factors estimate the
+// condition of the matrix they factor exactly, A + E).
+int factor_condest(Factor* f, const double* A, int lda, double* kappa, double* inv_norm,
+                   cudaStream_t st) {
+  if (!f || !kappa || !A || lda < f->n) return kInvalidArgument;
+  const int n = f->n;
+  *kappa = INFINITY;
+  if (inv_norm) *inv_norm = INFINITY;
+  if (f->info < n) return kOk;  // singular: infinite condition
+  double *lut = nullptr, *inv_t = nullptr, *vec = nullptr;
+  auto release = [&] {
+    if (lut) cudaFreeAsync(lut, st);
+    if (inv_t) cudaFreeAsync(inv_t, st);
+    if (vec) cudaFreeAsync(vec, st);
+    cudaStreamSynchronize(st);
+  };
+  const size_t nb = (size_t)(n + 63) / 64;
+  if (cudaMallocAsync(reinterpret_cast<void**>(&lut), sizeof(double) * (size_t)n * n, st) !=
+          cudaSuccess ||
+      cudaMallocAsync(reinterpret_cast<void**>(&inv_t), sizeof(double) * tri_inverse_doubles(n),
+                      st) != cudaSuccess ||
+      cudaMallocAsync(reinterpret_cast<void**>(&vec), sizeof(double) * 4 * (size_t)n, st) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    release();
+    return kAllocationFailed;
+  }
+  double* x = vec;          // input of a solve
+  double* y = vec + n;      // its result
+  double* tmp = vec + 2 * (size_t)n;
+  double* colsum = vec + 3 * (size_t)n;
+  dp::note_launch(3);
+  transpose_kernel<<<dim3((n + 31) / 32, (n + 31) / 32), dim3(32, 8), 0, st>>>(f->lu, n, lut, n);
+  transpose_inverses_kernel<<<grid_of((long long)(2 * 64 * 64 * nb)), 256, 0, st>>>(f->d_inv, inv_t,
+                                                                                  (int)nb);
+  col_abs_sum_kernel<<<(int)(((long long)n * 32 + 255) / 256), 256, 0, st>>>(A, lda, n, colsum);
+  int status = cudaGetLastError() == cudaSuccess ? kOk : kCudaFailure;
+  std::vector<double> hx(n), hy(n), hsum(n);
+  auto down = [&](std::vector<double>& h, const double* d) {
+    if (status == kOk && (cudaMemcpyAsync(h.data(), d, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                          st) != cudaSuccess ||
+                          cudaStreamSynchronize(st) != cudaSuccess))
+      status = kCudaFailure;
+  };
+  auto up = [&](const std::vector<double>& h, double* d) {
+    if (status == kOk &&
+        cudaMemcpyAsync(d, h.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st) != cudaSuccess)
+      status = kCudaFailure;
+  };
+  auto forward = [&] {  // y = A^{-1} x (x on the device), copied to hy
+    if (status == kOk) status = solve_with(*f, x, n, y, tmp, 1, st);
+    down(hy, y);
+  };
+  auto backward = [&] {  // y = A^{-T} x, copied to hy
+    if (status == kOk) status = solve_transposed(*f, lut, inv_t, x, y, tmp, st);
+    down(hy, y);
+  };
+  down(hsum, colsum);
+  double normA = 0.0;
+  for (double v : hsum) normA = std::max(normA, std::isnan(v) ? INFINITY : v);
+  double est = 0.0;
+  if (n == 1) {
+    hx[0] = 1.0;
+    up(hx, x);
+    forward();
+    est = std::fabs(hy[0]);
+  } else {
+    std::vector<double> sign(n, 0.0);
+    for (int i = 0; i < n; ++i) hx[i] = 1.0 / n;
+    up(hx, x);
+    forward();
+    int jlast = -1;
+    for (int it = 0; it < 5 && status == kOk; ++it) {
+      double s1 = 0.0;
+      for (double v : hy) s1 += std::fabs(v);
+      if (it > 0 && s1 <= est) break;  // no increase
+      est = s1;
+      bool same = it > 0;
+      for (int i = 0; i < n; ++i) {
+        const double sg = hy[i] >= 0.0 ? 1.0 : -1.0;
+        same = same && sg == sign[i];
+        sign[i] = sg;
+      }
+      if (same) break;  // the sign vector repeats: converged
+      up(sign, x);
+      backward();       // z = A^{-T} sign
+      int j = 0;
+      for (int i = 1; i < n; ++i)
+        if (std::fabs(hy[i]) > std::fabs(hy[j])) j = i;
+      if (it > 0 && j == jlast) break;
+      double zx = 0.0;
+      for (int i = 0; i < n; ++i) zx += hy[i] * hx[i];
+      if (it > 0 && std::fabs(hy[j]) <= zx) break;  // gradient test
+      jlast = j;
+      std::fill(hx.begin(), hx.end(), 0.0);
+      hx[j] = 1.0;
+      up(hx, x);
+      forward();
+    }
+    // alternating-sign vector safeguard
+    for (int i = 0; i < n; ++i)
+      hx[i] = ((i & 1) ? -1.0 : 1.0) * (1.0 + (double)i / (double)(n - 1));
+    up(hx, x);
+    forward();
+    double s1 = 0.0;
+    for (double v : hy) s1 += std::fabs(v);
+    est = std::max(est, 2.0 * s1 / (3.0 * n));
+  }
+  if (status == kOk && f->d_flags) status = solve_status(f->d_flags, n, st);
+  release();
+  if (status != kOk) return status;
+  if (inv_norm) *inv_norm = est;
+  *kappa = normA * est;
+  return kOk;
+}
 
 void factor_destroy(Factor* f, cudaStream_t st) {
   if (!f) return;
@@ -449,6 +637,13 @@ int factor_solve(Factor* f, const double* A, int lda, double* B, int ldb, int nr
       }
       if (it >= iters_left) return kOk;
       if (it > 0 && !(berr <= 0.5 * prev)) return kOk;  // stalled
+      // converging, but too slowly to reach tol within the steps left: the
+      // contraction rate of refinement is about constant (kappa times the
+      // factors' error), so stop now rather than after the last step
+      if (it > 0 && berr > 0.0 && tol > 0.0) {
+        const double needed = std::log(tol / berr) / std::log(berr / prev);
+        if (it + needed > iters_left + 0.5) return kOk;
+      }
       prev = berr;
       s = solve_with(*f, R, n, R, T, nrhs, st);
       if (s != kOk) return s;
@@ -583,6 +778,11 @@ int dp_factor_solve(dp_factor* h, const double* d_a, int lda, double* d_b, int l
   if (!h) return DP_INVALID_ARGUMENT;
   return dp::factor_solve(h->f, d_a, lda, d_b, ldb, nrhs, max_iter, tol, result,
                           static_cast<cudaStream_t>(stream));
+}
+
+int dp_factor_condest(dp_factor* h, const double* d_a, int lda, double* kappa1, void* stream) {
+  if (!h) return DP_INVALID_ARGUMENT;
+  return dp::factor_condest(h->f, d_a, lda, kappa1, nullptr, static_cast<cudaStream_t>(stream));
 }
 
 void dp_factor_destroy(dp_factor* h, void* stream) {

@@ -20,6 +20,7 @@
 // All CTAs are co-resident (cooperative launch), so no wait depends on a CTA
 // that has not started.
 #include <algorithm>
+#include <atomic>
 
 #include "dp_device.cuh"
 #include "dp_kernels.h"
@@ -32,6 +33,10 @@ constexpr int kTT = 256;          // threads
 constexpr int kTRhs = 64;         // right-hand sides per launch
 constexpr int kTAcc = kTRhs / 4;  // accumulators per thread (4 column groups)
 constexpr int kTMaxGrid = 32;     // CTAs of one launch
+
+// CTAs of a launch (dp_tri_solve_grid): 0 -> min(blocks, kTMaxGrid); g > 0 ->
+// min(blocks, g); g < 0 -> one CTA per -g row blocks (at least one CTA).
+std::atomic<int> g_tri_grid{0};
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
   unsigned v;
@@ -273,7 +278,11 @@ int launch_tri(const double* T, long long ldt, int n, const double* inv, double*
   // has to keep up with the blocks it owns, so 32 CTAs keep the latency of a
   // full grid while leaving the other SMs to concurrent work (the server).
   const int nblk = (n + kTB - 1) / kTB;
-  const int grid = std::max(1, std::min(std::min(nblk, kTMaxGrid), sms * per_sm));
+  const int policy = g_tri_grid.load(std::memory_order_relaxed);
+  const int want = policy == 0 ? kTMaxGrid
+                   : policy > 0 ? policy
+                                : std::max(1, std::min(kTMaxGrid, (nblk - policy - 1) / -policy));
+  const int grid = std::max(1, std::min(std::min(nblk, want), sms * per_sm));
   void* args[] = {(void*)&T,   (void*)&ldt,  (void*)&n,     (void*)&inv,
                   (void*)&Y,   (void*)&ldy,  (void*)&nrhs,  (void*)&flags,
                   (void*)&epoch, (void*)&status};
@@ -320,3 +329,8 @@ int launch_tri_upper(const double* U, long long ldu, int n, const double* inv, d
 }
 
 }  // namespace dp
+
+extern "C" int dp_tri_solve_grid(int policy) {
+  if (policy > 1024 || policy < -1024) return -2000;
+  return dp::g_tri_grid.exchange(policy);
+}

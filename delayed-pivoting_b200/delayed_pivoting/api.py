@@ -122,6 +122,8 @@ class RequestResult(ctypes.Structure):
         ("t_admit", ctypes.c_double),
         ("t_start", ctypes.c_double),
         ("t_done", ctypes.c_double),
+        ("factor_ms", ctypes.c_double),
+        ("solve_ms", ctypes.c_double),
     ]
 
 
@@ -515,6 +517,18 @@ class Factor:
         st = lib().dp_factor_solve(self._h, _dptr(self.d_a), self.lda, _dptr(d_b), ldb, nrhs,
                                    max_iter, tol, ctypes.byref(res), _stream(stream))
         return st, res
+
+    def condest(self, stream=None):
+        """dp_factor_condest: Hager-Higham estimate of kappa_1(A); returns
+        (status, kappa1)."""
+        L = lib()
+        L.dp_factor_condest.restype = ctypes.c_int
+        L.dp_factor_condest.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+        k = ctypes.c_double()
+        st = L.dp_factor_condest(self._h, _dptr(self.d_a), self.lda, ctypes.byref(k),
+                                 _stream(stream))
+        return st, k.value
 
     def close(self, stream=None):
         if getattr(self, "_h", None):

@@ -170,6 +170,17 @@ int dp_factor_info(const dp_factor *factor, int *info, int *precision, double *f
  * dp_gesv_ir_device.  Synchronises `stream`. */
 int dp_factor_solve(dp_factor *factor, const double *d_a, int lda, double *d_b, int ldb,
                     int nrhs, int max_iter, double tol, dp_ir_result *result, void *stream);
+/* Condition estimate (no reference counterpart): Hager's 1-norm estimator
+ * with Higham's safeguards (LAPACK dlacon's algorithm: at most 5 iterations,
+ * then the alternating-sign vector), i.e. kappa_1(A) ~= ||A||_1 ||A^{-1}||_1
+ * from a handful of solves with A and A^T through the resident factors -
+ * usually within a factor 3 of the true value, never above it.  d_a is the
+ * matrix the factors came from; mixed-precision factors estimate the
+ * condition of the matrix they factor exactly.  A singular factorisation
+ * (info < n) gives infinity.  Allocates n*n doubles of scratch for the
+ * duration of the call; synchronises `stream`. */
+int dp_factor_condest(dp_factor *factor, const double *d_a, int lda, double *kappa1,
+                      void *stream);
 void dp_factor_destroy(dp_factor *factor, void *stream);
 
 /* ---- Batched factorisation (no reference counterpart: the reference factors
@@ -281,6 +292,9 @@ typedef struct dp_request_result {
   int path;              /* 0: batched (small), 1: blocked (large) */
   double backward_error; /* max_c ||b_c - A x_c||_inf / (||A||_inf ||x_c||_inf + ||b_c||_inf) */
   double t_submit, t_admit, t_start, t_done; /* dp_server_clock() seconds */
+  double factor_ms;      /* large path: device time of the factorisation(s) on the worker's
+                            stream (events; includes waits for SMs held by other requests) */
+  double solve_ms;       /* large path: device time of the solve and its refinement */
 } dp_request_result;
 
 typedef struct dp_server_stats {
@@ -354,6 +368,12 @@ int dp_schur_update_device(int M, int N, int K, const double *A, int lda, const 
  * with two stages (four CTAs per SM).
  * Returns the previous setting, or -1 for an invalid one. */
 int dp_gemm_tile(int tile);
+
+/* CTAs of one triangular-solve launch of the solve / refinement path (tuning;
+ * no result bit depends on it): 0 automatic (min(row blocks, 32)), g > 0 at
+ * most g, g < 0 one CTA per -g blocks of 64 rows (at most 32).  Returns the
+ * previous setting, or -2000 for a setting outside [-1024, 1024]. */
+int dp_tri_solve_grid(int policy);
 
 /* delayed_dgetrf_cuda.hpp:63 (delayed_getrf_cuda_status_string). */
 const char *dp_status_string(int status);

@@ -11,6 +11,10 @@ CPU leg of bench.py, never by the product library.
   ``_ref/libref_delayed_lu.so`` by the Makefile beside this file.
 * ``residual`` - ||P A Q - Lbar Ubar||_F and ||A||_F of a compact factor, the
   reconstruction check of delayed_lu_cuda/example.cu:24-80.
+* ``_ref/ref_cuda_benchmark`` / ``_ref/ref_cuda_example`` - the reference's own
+  GPU build (cuBLAS), and ``_ref/benchmark_on_b200`` / ``_ref/example_on_b200``
+  - the same unmodified callers linked against libdelayed_lu_b200.so; see
+  ``ref_binary``.
 """
 from __future__ import annotations
 
@@ -33,7 +37,7 @@ def build(ref: bool = True) -> None:
     """Compiles the oracle (and, when the reference tree exists, the reference)."""
     targets = ["oracle"]
     if ref and Path(os.environ.get("DP_REFERENCE", "/root/reference")).exists():
-        targets.append("ref")
+        targets += ["ref", "refgpu"]
     env = dict(os.environ)
     if "DP_REFERENCE" in os.environ:
         env["REF"] = os.environ["DP_REFERENCE"]
@@ -183,3 +187,10 @@ def scaled_residual(orig, fac, m, n, info, ipiv, jpiv) -> float:
     if an == 0.0:
         return 0.0 if r == 0.0 else float("inf")
     return r / (an * max(m, n) * np.finfo(np.float64).eps / 2)
+
+
+def ref_binary(name: str):
+    """Path of a prebuilt reference-side executable under _ref/ (None when it
+    was not built: the reference tree was absent at build time)."""
+    p = HERE / "_ref" / name
+    return p if p.exists() else None

@@ -159,3 +159,48 @@ def test_mixed_factorisation_is_close():
     PAQ = A[torch.from_numpy(row).cuda()][:, torch.from_numpy(col).cuda()]
     rel = (torch.linalg.norm(PAQ - L @ U) / torch.linalg.norm(A)).item()
     assert rel < 1e-4
+
+
+def _conditioned(n, kappa, seed):
+    """A = U diag(sigma) V^T, U and V orthogonal (QR of seeded N(0,1)), sigma
+    geometric from 1 to 1/kappa; returns (A (host, Fortran), kappa_1(A))."""
+    rng = np.random.default_rng(seed)
+    u, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    v, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    s = np.logspace(0, -np.log10(kappa), n)
+    a = np.asfortranarray((u * s) @ v.T)
+    ainv = (v / s) @ u.T  # exact inverse of the construction
+    k1 = np.abs(a).sum(axis=0).max() * np.abs(ainv).sum(axis=0).max()
+    return a, k1
+
+
+@pytest.mark.parametrize("n", [1, 70, 300])
+@pytest.mark.parametrize("kappa", [1e2, 1e6, 1e10])
+def test_condest_brackets_kappa1(n, kappa):
+    """Hager-Higham through FP64 factors: a lower bound of kappa_1 (up to
+    rounding) and within a factor 10 of it (the estimator is exact for n = 1
+    and usually within 3)."""
+    import delayed_pivoting as dp
+
+    torch = _torch()
+    a, k1 = _conditioned(n, kappa, 100 + n)
+    d_a = colmajor(torch, a)
+    f = dp.Factor(n, d_a, n, precision=dp.PRECISION_FP64)
+    st, est = f.condest()
+    f.close()
+    assert st == 0
+    assert est <= k1 * (1 + 1e-4), (est, k1)  # solves through FP64 factors: kappa u <= 1e-6
+    assert est >= k1 / 10.0, (est, k1)
+
+
+def test_condest_of_singular_factorisation_is_infinite():
+    import delayed_pivoting as dp
+
+    torch = _torch()
+    a = np.asfortranarray(np.random.default_rng(3).standard_normal((50, 50)))
+    a[:, 7] = 0.0
+    f = dp.Factor(50, colmajor(torch, a), 50, precision=dp.PRECISION_FP64)
+    assert f.info()[0] < 50
+    st, est = f.condest()
+    f.close()
+    assert st == 0 and est == float("inf")
