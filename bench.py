@@ -75,7 +75,10 @@ def parse():
                     help="serve: skip the n=16384 plain-LU key of the line")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "mixed3"],
                     help="trailing-update arithmetic of the lu workload: FP64, BF16x6, BF16x3")
-    ap.add_argument("--workload", default="serve", choices=["serve", "lu", "batched", "ir"])
+    ap.add_argument("--workload", default="serve",
+                    choices=["serve", "lu", "batched", "ir", "stream"])
+    ap.add_argument("--loads", default="0.5,0.7,0.9",
+                    help="stream: offered loads as fractions of the measured mixed capacity")
     ap.add_argument("--requests", type=int, default=1000, help="requests per serve step")
     ap.add_argument("--max-n", type=int, default=8192, help="largest order of the serve stream")
     ap.add_argument("--load", type=float, default=0.7, help="open-loop load / capacity")
@@ -226,7 +229,7 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    if args.workload == "serve":
+    if args.workload in ("serve", "stream"):
         return serve_reference_arm(args)
     if args.workload == "batched":
         return batched_reference_arm(args)
@@ -270,6 +273,8 @@ def main():
         return run_batched(args)
     if args.workload == "ir":
         return run_ir(args)
+    if args.workload == "stream":
+        return run_stream(args)
     return run_lu(args)
 
 
@@ -1026,6 +1031,74 @@ def run_serve(args):
             "lu_n16384": lu,
         }
         print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_stream(args):
+    """Config 5 as a swept open-loop stream: --requests requests (default
+    20,000 when the flag is left at its serve default) drawn like the served
+    bursts, Poisson arrivals at each offered load of --loads (fractions of the
+    mixed server's capacity, measured first on one 1000-request burst), run
+    through the mixed and the plain-FP64 server in turn.  Per rate and server:
+    solves/s over the stream's span (first submission to last completion),
+    p50 / p99 latency from the server's own timestamps, the backward-error
+    distribution, and how the kappa = 1e10 requests ended."""
+    import torch
+    import delayed_pivoting as dp
+    from delayed_pivoting import serving as sv
+
+    world, rank, local, dev, dist = _dist_setup(torch)
+    R = 20000 if args.requests == 1000 else args.requests
+    seed = args.seed + rank
+    reqs = sv.make_stream(R, seed, hi=args.max_n)
+    probe = reqs[:1000]
+    pool = sv.MatrixPool(torch, [(q.n, q.kappa) for q in reqs], seed=seed)
+    rhs = sv.RhsSet(torch, pool, reqs, seed=seed + 1)
+    solves = sum(len(q.solves) for q in reqs)
+    out = {}
+    servers = {m: dp.Server(precision=p) for m, p in
+               (("mixed", dp.PRECISION_MIXED_BF16X6), ("plain", dp.PRECISION_FP64))}
+    cap = {}
+    for mode, srv in servers.items():
+        rhs.reset(torch)
+        sv.replay(srv, pool, rhs, reqs[:100])  # warm-up
+        rhs.reset(torch)
+        t0 = time.perf_counter()
+        sv.replay(srv, pool, rhs, probe)
+        torch.cuda.synchronize()
+        cap[mode] = len(probe) / (time.perf_counter() - t0)
+    rates = []
+    for load in [float(x) for x in args.loads.split(",")]:
+        rate = load * cap["mixed"]
+        row = {"load": load, "rate_rps": rate}
+        for mode, srv in servers.items():
+            rhs.reset(torch)
+            with ClockSampler(local) as clk:
+                res, first, last = sv.replay(srv, pool, rhs, reqs, rate=rate, seed=seed + 2,
+                                             timeout=3600.0)
+            summ = _serve_summary(reqs, res)
+            berr = np.array([r.backward_error for r in res.values()])
+            summ.update({"solves_per_s": solves / (last - first), "span_s": last - first,
+                         "berr_hist": {f"<=1e-{e}": int((berr <= 10.0 ** -e).sum())
+                                       for e in (14, 15, 16)},
+                         "clocks": clk.summary()})
+            row[mode] = summ
+        rates.append(row)
+    for srv in servers.values():
+        srv.close()
+    if rank == 0:
+        print(json.dumps({
+            "metric": SERVE_METRIC + " (open-loop stream, swept rate)",
+            "value": max(r["mixed"]["solves_per_s"] for r in rates), "unit": "solves/s",
+            "n_gpus": world, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic: seeded QR-conditioned matrices, seeded Poisson stream",
+            "config": {"workload": SERVE_WORKLOAD, "requests": R, "solves": solves,
+                       "max_n": args.max_n, "capacity_rps_1000_burst": cap,
+                       "pool_gb": pool.bytes / 1e9},
+            "rates": rates}), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()

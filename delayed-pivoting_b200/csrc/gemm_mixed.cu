@@ -13,20 +13,21 @@
 // 2^-16 with three products and about 2^-24 (FP32 accumulation) with six;
 // FP64 iterative refinement recovers full accuracy.
 //
-// Pipeline (one CTA per 128 x 128 tile of C, 4 warps):
-//   split_*_kernel  FP64 column-major -> BF16 hi / lo, K-major, K padded to 64
-//   TMA             128 x 64 BF16 boxes with 128-byte swizzle into a 2-stage
-//                   ring, completion through mbarrier transaction counts
-//   tcgen05.mma     issued by one thread: 4 K-steps of 16 x 3 products per
-//                   stage into a 128 x 128 FP32 accumulator (128 TMEM columns)
-//   tcgen05.commit  frees a stage / signals the epilogue
-//   epilogue        tcgen05.ld (32 lanes x 16 columns per warp and call),
-//                   C -= acc in FP64, coalesced along the column
+// Pipeline:
+//   split_*_kernel  FP64 column-major -> BF16 pieces, K-major, K padded to 64
+//   gemm kernel     persistent (one CTA per SM over 128 x 128 tiles of C),
+//                   warp-specialised: a TMA warp feeds 128 x 64 BF16 boxes
+//                   (128-byte swizzle) into a 2-stage ring, an MMA warp
+//                   issues tcgen05.mma (kind::f16, FP32 accumulation) into a
+//                   double-buffered TMEM accumulator, 16 epilogue warps
+//                   prefetch their rows of C, then C -= acc in FP64 through
+//                   tcgen05.ld while the next tile's MMAs run
 // Every mbarrier wait is bounded; on timeout the kernel records
-// kDeviceTimeout, skips the epilogue and still frees its tensor memory.
+// kDeviceTimeout, skips the rest and still frees its tensor memory.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "dp_device.cuh"
@@ -37,10 +38,8 @@ namespace dp {
 namespace mixed {
 
 constexpr int BM = 128, BN = 128, BK = 64;  // BK: BF16 elements per 128-byte swizzle row
-constexpr int kThreads = 128;
 constexpr int kTileBytes = BM * BK * 2;     // 16 KB per operand tile (BN == BM)
 constexpr int kStages = 2;
-constexpr unsigned kTmemCols = BN;
 // A pieces then B pieces per stage
 template <int TERMS>
 constexpr int stage_bytes() { return 2 * TERMS * kTileBytes; }
@@ -192,31 +191,64 @@ struct Maps {
   CUtensorMap a[3], b[3];
 };
 
+// Persistent, warp-specialised kernel: CTA c takes the 128 x 128 tiles c,
+// c + grid, ... of C (m fastest).
+//   warp 0 (one lane)  TMA producer: per K chunk of 64 the TERMS pieces of A
+//                      and of B into a kStages ring (full / empty barriers)
+//   warp 1 (one lane)  MMA issuer: tcgen05.mma of the split products into
+//                      one of two 128-column TMEM accumulators (tile parity),
+//                      tcgen05.commit frees a stage and, after the last
+//                      chunk, hands the accumulator to the epilogue
+//   warps 2..17        epilogue: each thread owns one row and 32 columns of
+//                      the tile; it loads those 32 C values BEFORE the
+//                      accumulator is ready (the FP64 read-modify-write of C
+//                      is the bound: 16 bytes per element against 2 K x
+//                      products flops), then C -= acc through tcgen05.ld
+//                      and releases the accumulator - so the C traffic of
+//                      tile t overlaps the MMAs of tile t + 1
+// Warp w reads TMEM lanes 32 (w % 4) .. + 31 (the hardware's lane split);
+// warps w, w + 4, w + 8, w + 12 take the four 32-column quarters of those
+// rows.
+constexpr int kEpiWarps = 16;
+constexpr int kThreadsP = 64 + 32 * kEpiWarps;  // 576
+constexpr int kEpiCols = BN / (kEpiWarps / 4);  // 32 columns per epilogue thread
+constexpr unsigned kTmemColsP = 2 * BN;         // double-buffered accumulator
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 template <int TERMS>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreadsP, 1)
 gemm_bf16x3_kernel(const __grid_constant__ Maps tm, int M, int N, int kchunks, double* C,
                    long long ldc, int* status) {
   constexpr int kStageBytes = stage_bytes<TERMS>();
   extern __shared__ unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages], done_bar;
+  __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages];
+  __shared__ __align__(8) uint64_t tfull_bar[2], tempty_bar[2], done_bar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ int failed;
   unsigned char* smem =
       reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int tiles_m = (M + BM - 1) / BM;
+  const int tiles = tiles_m * ((N + BN - 1) / BN);
 
-  if (warp == 0) {
+  if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(&tmem_base_sh)),
-                 "r"(kTmemCols)
+                 "r"(kTmemColsP)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  if (tid == 32) {
+  if (tid == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full_bar[s], 1);
       mbar_init(&empty_bar[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull_bar[b], 1);
+      mbar_init(&tempty_bar[b], kEpiWarps);
     }
     mbar_init(&done_bar, 1);
     failed = 0;
@@ -227,95 +259,130 @@ gemm_bf16x3_kernel(const __grid_constant__ Maps tm, int M, int N, int kchunks, d
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base_sh;
+  // `failed` is written and polled by different warps: volatile accesses
+  volatile int* const vfailed = &failed;
+  auto fail = [&] {
+    *vfailed = 1;
+    atomicCAS(status, kOk, kDeviceTimeout);
+  };
 
-  if (tid == 0) {
-    auto load_chunk = [&](int c, int s) {
-      unsigned char* st = smem + (size_t)s * kStageBytes;
-      mbar_expect_tx(&full_bar[s], kStageBytes);
-#pragma unroll
-      for (int q = 0; q < TERMS; ++q) {
-        tma_load_2d(st + q * kTileBytes, &tm.a[q], &full_bar[s], c * BK, m0);
-        tma_load_2d(st + (TERMS + q) * kTileBytes, &tm.b[q], &full_bar[s], c * BK, n0);
-      }
-    };
-    const uint32_t idesc = idesc_bf16_f32(BM, BN);
-    for (int c = 0; c < kchunks && c < kStages; ++c) load_chunk(c, c);
-    bool ok = true;
-    for (int c = 0; c < kchunks && ok; ++c) {
-      const int s = c % kStages;
-      const unsigned ph = (unsigned)((c / kStages) & 1);
-      if (!mbar_wait(&full_bar[s], ph)) {
-        ok = false;
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      unsigned char* st = smem + (size_t)s * kStageBytes;
-#pragma unroll
-      for (int kk = 0; kk < BK / 16; ++kk) {
-        uint64_t ad[TERMS], bd[TERMS];
-#pragma unroll
-        for (int q = 0; q < TERMS; ++q) {
-          ad[q] = umma_desc_k_sw128(st + q * kTileBytes + kk * 32);
-          bd[q] = umma_desc_k_sw128(st + (TERMS + q) * kTileBytes + kk * 32);
-        }
-        // products of pieces (i, j) with i + j <= TERMS - 1, leading one first
-        bool first = c == 0 && kk == 0;
-#pragma unroll
-        for (int d = 0; d < TERMS; ++d)
-#pragma unroll
-          for (int i = 0; i <= d; ++i) {
-            umma_f16(tmem, ad[i], bd[d - i], idesc, first ? 0u : 1u);
-            first = false;
+  if (warp == 0) {
+    if (lane == 0) {  // TMA producer
+      int g = 0;      // chunk counter over this CTA's tiles
+      for (int t = blockIdx.x; t < tiles && !*vfailed; t += gridDim.x) {
+        const int m0 = (t % tiles_m) * BM, n0 = (t / tiles_m) * BN;
+        for (int c = 0; c < kchunks; ++c, ++g) {
+          const int s = g % kStages;
+          const unsigned ph = (unsigned)((g / kStages) & 1);
+          if (!mbar_wait(&empty_bar[s], ph ^ 1u)) {  // a fresh barrier passes parity 1
+            fail();
+            break;
           }
+          unsigned char* st = smem + (size_t)s * kStageBytes;
+          mbar_expect_tx(&full_bar[s], kStageBytes);
+#pragma unroll
+          for (int q = 0; q < TERMS; ++q) {
+            tma_load_2d(st + q * kTileBytes, &tm.a[q], &full_bar[s], c * BK, m0);
+            tma_load_2d(st + (TERMS + q) * kTileBytes, &tm.b[q], &full_bar[s], c * BK, n0);
+          }
+        }
       }
-      umma_commit(&empty_bar[s]);
-      if (c + kStages < kchunks) {
-        if (!mbar_wait(&empty_bar[s], ph)) {
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      const uint32_t idesc = idesc_bf16_f32(BM, BN);
+      int g = 0, it = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++it) {
+        const int buf = it & 1;
+        if (!mbar_wait(&tempty_bar[buf], (unsigned)((it >> 1) & 1) ^ 1u)) {
           ok = false;
           break;
         }
-        load_chunk(c + kStages, s);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t acc = tmem + (uint32_t)(buf * BN);
+        for (int c = 0; c < kchunks; ++c, ++g) {
+          const int s = g % kStages;
+          const unsigned ph = (unsigned)((g / kStages) & 1);
+          if (!mbar_wait(&full_bar[s], ph)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          unsigned char* st = smem + (size_t)s * kStageBytes;
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk) {
+            uint64_t ad[TERMS], bd[TERMS];
+#pragma unroll
+            for (int q = 0; q < TERMS; ++q) {
+              ad[q] = umma_desc_k_sw128(st + q * kTileBytes + kk * 32);
+              bd[q] = umma_desc_k_sw128(st + (TERMS + q) * kTileBytes + kk * 32);
+            }
+            // products of pieces (i, j) with i + j <= TERMS - 1, leading one first
+            bool first = c == 0 && kk == 0;
+#pragma unroll
+            for (int d = 0; d < TERMS; ++d)
+#pragma unroll
+              for (int i = 0; i <= d; ++i) {
+                umma_f16(acc, ad[i], bd[d - i], idesc, first ? 0u : 1u);
+                first = false;
+              }
+          }
+          umma_commit(&empty_bar[s]);  // the stage is free once these MMAs complete
+        }
+        if (!ok) break;
+        umma_commit(&tfull_bar[buf]);  // the accumulator is complete
       }
+      if (!ok) fail();
+      umma_commit(&done_bar);  // arrives once every issued MMA has completed
     }
-    if (!ok) {
-      failed = 1;
-      atomicCAS(status, kOk, kDeviceTimeout);
-    }
-    umma_commit(&done_bar);  // arrives once every issued MMA has completed
-  }
-  __syncwarp();
-  const bool done_ok = mbar_wait(&done_bar, 0);
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  __syncthreads();
-  if (done_ok && !failed) {
-    const int row = m0 + warp * 32 + lane;
-    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll 1
-    for (int cc = 0; cc < BN / 16; ++cc) {
-      uint32_t r[16];
-      tmem_ld16(lane_base + (uint32_t)(cc * 16), r);
-      if (row < M) {
-        double old[16];
+  } else {  // epilogue
+    const int q = warp & 3, h = (warp - 2) >> 2;
+    const uint32_t lane_base = tmem + ((uint32_t)(q * 32) << 16);
+    int it = 0;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
+      const int buf = it & 1;
+      const int m0 = (t % tiles_m) * BM, n0 = (t / tiles_m) * BN;
+      const int row = m0 + q * 32 + lane;
+      const int col0 = n0 + h * kEpiCols;
+      const bool row_ok = row < M;
+      double* crow = C + idx(row_ok ? row : 0, col0, ldc);
+      double old[kEpiCols];  // read-only, L2-cached loads: all in flight at once
+#pragma unroll
+      for (int j = 0; j < kEpiCols; ++j)
+        old[j] = (row_ok && col0 + j < N) ? __ldcg(crow + (size_t)j * ldc) : 0.0;
+      const bool got = mbar_wait(&tfull_bar[buf], (unsigned)((it >> 1) & 1));
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (!got || *vfailed) {
+        if (lane == 0) fail();
+        break;
+      }
+      const uint32_t acc = lane_base + (uint32_t)(buf * BN + h * kEpiCols);
+#pragma unroll
+      for (int cc = 0; cc < kEpiCols / 16; ++cc) {
+        uint32_t r[16];
+        tmem_ld16(acc + (uint32_t)(cc * 16), r);
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
-          const int col = n0 + cc * 16 + j;
-          old[j] = col < N ? C[idx(row, col, ldc)] : 0.0;
-        }
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int col = n0 + cc * 16 + j;
-          if (col < N) C[idx(row, col, ldc)] = old[j] - (double)__uint_as_float(r[j]);
+          const int jj = cc * 16 + j;
+          if (row_ok && col0 + jj < N)
+            crow[(size_t)jj * ldc] = old[jj] - (double)__uint_as_float(r[j]);
         }
       }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty_bar[buf]);
     }
-  } else if (!done_ok && tid == 0) {
-    atomicCAS(status, kOk, kDeviceTimeout);
   }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  // every issued MMA has completed before the tensor memory is released
   __syncthreads();
-  if (warp == 0) {
+  if (warp == 1) {
+    const bool ok = mbar_wait(&done_bar, 0);
+    if (!ok && lane == 0) fail();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    __syncwarp();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(kTmemCols)
+                 "r"(kTmemColsP)
                  : "memory");
   }
 }
@@ -385,10 +452,11 @@ int launch(int M, int N, int K, const double* A, long long lda, const double* B,
     if (!make_map(&tm.a[q], ap + (size_t)q * M * kp, M, kp) ||
         !make_map(&tm.b[q], bp + (size_t)q * N * kp, N, kp))
       return kLibraryFailure;
-  dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
+  const int tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN);
+  const int grid = std::max(1, std::min(tiles, sm_count()));
   dp::note_launch();
-  gemm_bf16x3_kernel<TERMS><<<grid, kThreads, smem_bytes<TERMS>(), s>>>(tm, M, N, kp / BK, C, ldc,
-                                                                       status);
+  gemm_bf16x3_kernel<TERMS><<<grid, kThreadsP, smem_bytes<TERMS>(), s>>>(tm, M, N, kp / BK, C, ldc,
+                                                                        status);
   return cudaGetLastError() == cudaSuccess ? kOk : kCudaFailure;
 }
 
@@ -406,3 +474,35 @@ int launch_gemm_minus_mixed(int M, int N, int K, const double* A, long long lda,
 }
 
 }  // namespace dp
+
+// The mixed-precision update alone (tests and measurements of the kernel):
+// scratch from the stream-ordered pool, status read back (synchronises).
+extern "C" int dp_schur_update_mixed_device(int M, int N, int K, const double* A, int lda,
+                                            const double* B, int ldb, double* C, int ldc,
+                                            int precision, void* stream) {
+  using namespace dp;
+  const int terms = mixed_terms(precision);
+  if (M < 0 || N < 0 || K < 0 || terms == 0) return kInvalidArgument;
+  if (M == 0 || N == 0 || K == 0) return kOk;
+  if (!A || !B || !C || lda < M || ldb < K || ldc < M) return kInvalidArgument;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t bytes = mixed_scratch_bytes(M, N, K, terms) + 256;
+  char* scratch = nullptr;
+  if (cudaMallocAsync(reinterpret_cast<void**>(&scratch), bytes, st) != cudaSuccess) {
+    cudaGetLastError();
+    return kAllocationFailed;
+  }
+  int* status = reinterpret_cast<int*>(scratch + bytes - 256);
+  int rc = cudaMemsetAsync(status, 0, sizeof(int), st) == cudaSuccess ? kOk : kCudaFailure;
+  if (rc == kOk)
+    rc = launch_gemm_minus_mixed(M, N, K, A, lda, B, ldb, C, ldc, scratch, terms, status, st);
+  int h = kOk;
+  if (rc == kOk &&
+      (cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+       cudaStreamSynchronize(st) != cudaSuccess))
+    rc = kCudaFailure;
+  cudaFreeAsync(scratch, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && rc == kOk) rc = kCudaFailure;
+  if (rc != kOk) cudaGetLastError();
+  return rc == kOk ? h : rc;
+}

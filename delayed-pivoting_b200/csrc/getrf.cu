@@ -119,7 +119,8 @@ struct Workspace {
   int* swap_block = nullptr;
   int* swap_extra = nullptr;
   Cand* cands = nullptr;
-  void* mixed = nullptr;  // BF16 operand scratch of the tensor-core update (mixed precision)
+  void* mixed = nullptr;   // BF16 operand scratch of the tensor-core update (mixed precision)
+  void* mixed1 = nullptr;  // the same for the next outer block's update on the panel stream
   // Look-ahead: swap lists of the panels of an outer block, kept until the
   // block completes (two buffers, alternating between consecutive blocks;
   // panel [b, e) of block [B, E) at defer_blk + (b - B), defer_ext + 2 (b - B)),
@@ -136,7 +137,7 @@ size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 // Lays the workspace out from `base` (nullptr: only computes the size).
 size_t layout_workspace(Workspace& ws, char* base, int pivots, int max_ctas, int w_max,
-                        size_t mixed_bytes, int defer_cap = 0) {
+                        size_t mixed_bytes, int defer_cap = 0, size_t mixed1_bytes = 0) {
   size_t off = 0;
   auto take = [&](size_t bytes) {
     const size_t at = off;
@@ -162,6 +163,7 @@ size_t layout_workspace(Workspace& ws, char* base, int pivots, int max_ctas, int
     ws.aux_status = reinterpret_cast<int*>(take(sizeof(int)));
   }
   ws.mixed = mixed_bytes ? reinterpret_cast<void*>(take(mixed_bytes)) : nullptr;
+  ws.mixed1 = mixed1_bytes ? reinterpret_cast<void*>(take(mixed1_bytes)) : nullptr;
   ws.base = base;
   ws.bytes = off;
   return off;
@@ -707,7 +709,10 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       if (pending) DP_CHECK_CUDA(cudaStreamWaitEvent(st, sc.next, 0));
       if (int err = apply_deferred(a, lda, blk, ext, B, widths, E, NE, NE, NE, st, rec))
         return err;
-      update_columns(a, lda, m, B, E - B, E, E, NE, st, rec);
+      // (mixed precision: its own BF16 scratch, the trailing stream uses ws.mixed)
+      if (int err = update_columns(a, lda, m, B, E - B, E, E, NE, st, rec,
+                                   terms ? ws.mixed1 : nullptr, &ws.state->status, terms))
+        return err;
       DP_CHECK_CUDA(cudaGetLastError());
       DP_CHECK_CUDA(cudaEventRecord(sc.block, st));
       // s2: everything else, behind the block
@@ -846,18 +851,22 @@ int getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* 
   Lanes* lanes = nullptr;
   if (o.lookahead == 1 || (o.lookahead == 0 && pivots > NB)) lanes = lanes_for_device();
   const int defer_cap = lanes ? std::min(NB, pivots) : 0;
+  const size_t mixed1_bytes =
+      lanes && mixed_terms(o.precision) ? mixed_scratch_bytes(m, NB, NB, mixed_terms(o.precision))
+                                        : 0;
   const size_t bytes =
-      layout_workspace(ws, nullptr, pivots, di.sms, w_max, mixed_bytes, defer_cap);
+      layout_workspace(ws, nullptr, pivots, di.sms, w_max, mixed_bytes, defer_cap, mixed1_bytes);
   char* base = nullptr;
   if (cudaMallocAsync(reinterpret_cast<void**>(&base), bytes, st) != cudaSuccess) {
     cudaGetLastError();
     *info = -1;
     return kAllocationFailed;
   }
-  layout_workspace(ws, base, pivots, di.sms, w_max, mixed_bytes, defer_cap);
+  layout_workspace(ws, base, pivots, di.sms, w_max, mixed_bytes, defer_cap, mixed1_bytes);
   int status = kOk;
-  // the BF16 scratch is fully written before use; clear only the rest
-  if (cudaMemsetAsync(base, 0, bytes - mixed_bytes, st) != cudaSuccess) status = kCudaFailure;
+  // the BF16 scratch (at the end) is fully written before use; clear the rest
+  const size_t clear = mixed_bytes ? (size_t)(static_cast<char*>(ws.mixed) - base) : bytes;
+  if (cudaMemsetAsync(base, 0, clear, st) != cudaSuccess) status = kCudaFailure;
   int inf = pivots;
   HostTrace trace;
   g_trace = &trace;

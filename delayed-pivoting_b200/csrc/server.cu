@@ -81,8 +81,8 @@ struct Job {
   std::shared_ptr<Resident> res;     // follow-ups
 };
 
-size_t scratch_bytes(int n, int nrhs) {  // X, R, D / T of one solve
-  return 3 * sizeof(double) * (size_t)n * nrhs + 4096;
+size_t scratch_bytes(int n, int nrhs) {  // X, R, T of one solve, its columns in a coalesced solve
+  return 4 * sizeof(double) * (size_t)n * nrhs + 4096;
 }
 
 size_t small_factor_bytes(int n) {
@@ -91,8 +91,9 @@ size_t small_factor_bytes(int n) {
 
 size_t large_factor_bytes(int n) {
   // factors + composite orders, the blocked factorisation's workspace
-  // (mailboxes, candidate rows, BF16 operand split of the mixed update)
-  return dp::factor_bytes(n) + 2048 * (size_t)n + (8u << 20);
+  // (mailboxes, candidate rows, the BF16 pieces of the mixed updates: three
+  // pieces of 256 columns for n + n and n + 256 operand rows)
+  return dp::factor_bytes(n) + 5120 * (size_t)n + (8u << 20);
 }
 
 }  // namespace
@@ -184,6 +185,9 @@ struct dp_server {
   }
 
   void large_worker();
+  void take_followups_locked(unsigned long long factor_id, int& rhs, std::vector<Job>& batch);
+  void solve_large(std::vector<Job>& batch, size_t first, Factor* f, const double* A, int lda,
+                   std::vector<dp_request_result>& out, cudaStream_t st);
   void small_worker();
   void run_small_new(std::vector<Job>& jobs, cudaStream_t st);
   void run_small_followups(std::vector<Job>& jobs, cudaStream_t st);
@@ -208,83 +212,170 @@ void dp_server::drop_resident_locked(const std::shared_ptr<Resident>& r, cudaStr
   r->group.reset();
 }
 
+// Moves the admitted follow-up solves of factorisation `factor_id` out of
+// the large queue into `batch` while the right-hand sides fit one solve
+// (at most dp::serve::kMaxRhs columns in all).
+void dp_server::take_followups_locked(unsigned long long factor_id, int& rhs,
+                                      std::vector<Job>& batch) {
+  for (auto it = large_q.begin(); it != large_q.end();) {
+    if (it->r.factor_id == factor_id && rhs + it->r.nrhs <= dp::serve::kMaxRhs) {
+      rhs += it->r.nrhs;
+      batch.push_back(*it);
+      ++running;
+      it = large_q.erase(it);
+    } else {
+      ++it;
+    }
+  }
+}
+
+// Solves batch[first..] with the factors f in ONE refined multi-RHS solve:
+// the requests' right-hand sides are copied side by side into one n x k
+// block (k = sum of their nrhs), solved together, and the solution columns
+// copied back; one request is solved in place.  Every request gets the
+// combined solve's backward error (the largest over all columns) and
+// refinement steps, and its share of the device time.
+void dp_server::solve_large(std::vector<Job>& batch, size_t first, Factor* f, const double* A,
+                            int lda, std::vector<dp_request_result>& out, cudaStream_t st) {
+  const int n = f->n;
+  const size_t cnt = batch.size() - first;
+  if (cnt == 0) return;
+  int k = 0;
+  for (size_t i = first; i < batch.size(); ++i) k += batch[i].r.nrhs;
+  dp_ir_result ir{};
+  int status = DP_SUCCESS;
+  double* W = nullptr;
+  if (cnt == 1) {
+    const Job& j = batch[first];
+    status = dp::factor_solve(f, A, lda, j.r.d_b, j.r.ldb, j.r.nrhs, opt.max_iter, opt.tol, &ir, st);
+  } else {
+    if (cudaMallocAsync(reinterpret_cast<void**>(&W), sizeof(double) * (size_t)n * k, st) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      W = nullptr;
+      status = DP_ALLOCATION_FAILED;
+    }
+    int c = 0;
+    for (size_t i = first; i < batch.size() && status == DP_SUCCESS; ++i) {
+      const Job& j = batch[i];
+      if (cudaMemcpy2DAsync(W + (size_t)c * n, sizeof(double) * n, j.r.d_b,
+                            sizeof(double) * j.r.ldb, sizeof(double) * n, j.r.nrhs,
+                            cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        status = DP_CUDA_FAILURE;
+      c += j.r.nrhs;
+    }
+    if (status == DP_SUCCESS)
+      status = dp::factor_solve(f, A, lda, W, n, k, opt.max_iter, opt.tol, &ir, st);
+    c = 0;
+    for (size_t i = first; i < batch.size() && status == DP_SUCCESS; ++i) {
+      const Job& j = batch[i];
+      if (cudaMemcpy2DAsync(j.r.d_b, sizeof(double) * j.r.ldb, W + (size_t)c * n,
+                            sizeof(double) * n, sizeof(double) * n, j.r.nrhs,
+                            cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        status = DP_CUDA_FAILURE;
+      c += j.r.nrhs;
+    }
+    if (W) cudaFreeAsync(W, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess && status == DP_SUCCESS) status = DP_CUDA_FAILURE;
+  }
+  const double solve_ms = ir.total_ms - ir.factor_ms;
+  for (size_t i = first; i < batch.size(); ++i) {
+    dp_request_result& r = out[i];
+    r.status = status;
+    r.info = f->info;
+    r.precision = f->precision;
+    r.iterations = ir.iterations;
+    r.refactored = ir.refactored;
+    r.backward_error = ir.backward_error;
+    r.factor_ms += i == first ? ir.factor_ms : 0.0;
+    r.solve_ms = solve_ms * batch[i].r.nrhs / (double)k;
+  }
+}
+
 void dp_server::large_worker() {
   cudaSetDevice(device);
   cudaStream_t st;
   cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
   for (;;) {
-    Job j;
+    std::vector<Job> batch;  // batch[0] as popped; then follow-ups of the same factorisation
+    int rhs = 0;
     {
       std::unique_lock<std::mutex> lk(m);
       cv_large.wait(lk, [&] { return stop || !large_q.empty(); });
       if (large_q.empty()) break;
-      j = large_q.front();
+      batch.push_back(large_q.front());
       large_q.pop_front();
       ++running;
+      rhs = batch[0].r.nrhs;
+      if (batch[0].r.factor_id != 0) take_followups_locked(batch[0].r.factor_id, rhs, batch);
     }
-    dp_request_result r{};
-    r.path = 1;
-    r.t_start = clock_s();
-    dp_ir_result ir{};
+    std::vector<dp_request_result> out(batch.size());
+    for (auto& r : out) {
+      r.path = 1;
+      r.t_start = clock_s();
+    }
+    // copies: appending follow-ups to `batch` may move its elements
+    const dp_request r0 = batch[0].r;
+    const size_t factor0 = batch[0].factor;
+    const std::shared_ptr<Resident> res0 = batch[0].res;
     std::shared_ptr<Resident> keep;
-    if (j.r.factor_id == 0) {
+    if (r0.factor_id == 0) {
       Factor* f = nullptr;
-      r.status = dp::factor_create(&f, j.r.n, j.r.d_a, j.r.lda, opt.precision, st);
-      r.info = f ? f->info : -1;
-      if (f) r.factor_ms = f->factor_ms;
-      if (r.status == DP_SUCCESS) {
-        r.status = dp::factor_solve(f, j.r.d_a, j.r.lda, j.r.d_b, j.r.ldb, j.r.nrhs, opt.max_iter,
-                                    opt.tol, &ir, st);
-        r.info = f->info;
-        r.precision = f->precision;
-        r.iterations = ir.iterations;
-        r.refactored = ir.refactored;
-        r.backward_error = ir.backward_error;
-        r.factor_ms += ir.factor_ms;
-        r.solve_ms = ir.total_ms - ir.factor_ms;
-      }
-      if (r.status == DP_SUCCESS && j.r.followups > 0 && f && f->info == j.r.n) {
+      const int status = dp::factor_create(&f, r0.n, r0.d_a, r0.lda, opt.precision, st);
+      out[0].status = status;
+      out[0].info = f ? f->info : -1;
+      if (f) out[0].factor_ms = f->factor_ms;
+      if (status == DP_SUCCESS && r0.followups > 0 && f && f->info == r0.n) {
         keep = std::make_shared<Resident>();
-        keep->id = j.r.id;
-        keep->n = j.r.n;
-        keep->lda = j.r.lda;
-        keep->A = j.r.d_a;
+        keep->id = r0.id;
+        keep->n = r0.n;
+        keep->lda = r0.lda;
+        keep->A = r0.d_a;
         keep->factor = f;
-        keep->left = keep->admits_left = j.r.followups;
-        keep->bytes = j.factor;
-      } else if (f) {
-        dp::factor_destroy(f, st);
+        keep->left = keep->admits_left = r0.followups;
+        keep->bytes = factor0;
+        // resident before the first solve: follow-ups already submitted are
+        // admitted now and solved together with it
+        std::lock_guard<std::mutex> lk(m);
+        residents[keep->id] = keep;
+        schedule_locked();
+        take_followups_locked(keep->id, rhs, batch);
+        out.resize(batch.size());
+        for (size_t i = 1; i < out.size(); ++i) {
+          out[i].path = 1;
+          out[i].t_start = clock_s();
+        }
       }
+      if (status == DP_SUCCESS) {
+        std::unique_lock<std::mutex> g;
+        if (keep) g = std::unique_lock<std::mutex>(keep->m);
+        solve_large(batch, 0, f, r0.d_a, r0.lda, out, st);
+      }
+      if (!keep && f) dp::factor_destroy(f, st);
     } else {
-      std::shared_ptr<Resident> res = j.res;
-      std::lock_guard<std::mutex> g(res->m);
-      r.status = dp::factor_solve(res->factor, res->A, res->lda, j.r.d_b, j.r.ldb, j.r.nrhs,
-                                  opt.max_iter, opt.tol, &ir, st);
-      r.info = res->factor->info;
-      r.precision = res->factor->precision;
-      r.iterations = ir.iterations;
-      r.refactored = ir.refactored;
-      r.backward_error = ir.backward_error;
-      r.factor_ms = ir.factor_ms;
-      r.solve_ms = ir.total_ms - ir.factor_ms;
+      std::lock_guard<std::mutex> g(res0->m);
+      solve_large(batch, 0, res0->factor, res0->A, res0->lda, out, st);
     }
-    r.t_done = clock_s();
+    const double t_done = clock_s();
     {
       std::lock_guard<std::mutex> lk(m);
-      release(j.scratch);
-      if (j.r.factor_id == 0) {
-        if (keep) {
-          residents[keep->id] = keep;
-        } else {
-          release(j.factor);
-          live_ids.erase(j.r.id);
+      for (size_t i = 0; i < batch.size(); ++i) {
+        Job& b = batch[i];
+        dp_request_result r = out[i];
+        r.t_done = t_done;
+        release(b.scratch);
+        if (b.r.factor_id == 0) {
+          if (!keep) {
+            release(b.factor);
+            live_ids.erase(b.r.id);
+          }
+        } else if (--b.res->left == 0) {
+          drop_resident_locked(b.res, st);
         }
-      } else if (--j.res->left == 0) {
-        drop_resident_locked(j.res, st);
+        ++large_items;
+        --running;
+        finish_locked(b, r);
       }
-      ++large_items;
-      --running;
-      finish_locked(j, r);
       schedule_locked();
     }
   }

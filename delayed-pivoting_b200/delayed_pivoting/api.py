@@ -368,6 +368,19 @@ def schur_update_device(M, N, K, d_a, lda, d_b, ldb, d_c, ldc, stream=None):
                                     _stream(stream))
 
 
+def schur_update_mixed_device(M, N, K, d_a, lda, d_b, ldb, d_c, ldc,
+                              precision=PRECISION_MIXED_BF16X6, stream=None):
+    """dp_schur_update_mixed_device: C -= A * B on the tensor cores (BF16
+    split, FP32 accumulation, C updated in FP64); synchronises.  Returns the
+    status."""
+    L = lib()
+    L.dp_schur_update_mixed_device.restype = ctypes.c_int
+    L.dp_schur_update_mixed_device.argtypes = [ctypes.c_int] * 3 + \
+        [ctypes.c_void_p, ctypes.c_int] * 3 + [ctypes.c_int, ctypes.c_void_p]
+    return L.dp_schur_update_mixed_device(M, N, K, _dptr(d_a), lda, _dptr(d_b), ldb, _dptr(d_c),
+                                          ldc, precision, _stream(stream))
+
+
 def gemm_tile(tile: int) -> int:
     """dp_gemm_tile: 0 automatic (= 5), 1 128 x 128, 2 128 x 64, 3 64 x 64, 4 128 x 64
     (8 warps), 5 64 x 64 (two stages).

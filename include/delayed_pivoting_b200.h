@@ -362,6 +362,15 @@ long long dp_kernel_launches(void);
 int dp_schur_update_device(int M, int N, int K, const double *A, int lda, const double *B,
                            int ldb, double *C, int ldc, void *stream);
 
+/* The same update on the tensor cores, as the mixed-precision factorisation
+ * runs it (precision DP_PRECISION_MIXED_BF16X3 / _BF16X6: A and B split into
+ * 2 / 3 BF16 pieces, 3 / 6 products, FP32 accumulation in tensor memory, C -=
+ * acc in FP64).  Scratch for the pieces comes from the stream-ordered pool;
+ * synchronises `stream`.  Returns DP_DEVICE_TIMEOUT if a bounded wait of the
+ * kernel gave up. */
+int dp_schur_update_mixed_device(int M, int N, int K, const double *A, int lda, const double *B,
+                                 int ldb, double *C, int ldc, int precision, void *stream);
+
 /* Tile of that kernel for N > 32 (tuning; no result bit depends on it):
  * 0 automatic (= 5), 1 128 x 128 (one CTA per SM), 2 128 x 64 (two CTAs per
  * SM), 3 64 x 64 (three CTAs per SM), 4 128 x 64 with eight warps, 5 64 x 64

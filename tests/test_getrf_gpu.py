@@ -352,3 +352,31 @@ def test_near_tie_report_of_failed_call(built):
     assert st == dp.INVALID_ARGUMENT and info == -1
     rep = dp.getrf_last_report()
     assert rep["info"] == -1 and rep["decisions"] == 0 and rep["near_ties"] == 0
+
+
+@pytest.mark.parametrize("M,N,K", [(1, 1, 1), (130, 70, 64), (1000, 3000, 256), (4099, 385, 100),
+                                   (300, 20000, 32)])
+@pytest.mark.parametrize("prec", ["x3", "x6"])
+def test_mixed_schur_update_against_torch(built, M, N, K, prec):
+    """The tensor-core update C -= A B (BF16 split, FP32 accumulation) against
+    an FP64 torch product: |error| <= c K 2^-p max|A| max|B| with 2^-p the
+    split's resolution (x3: 2^-16, x6: 2^-24, plus the FP32 accumulation);
+    rows and columns outside C are untouched.  Many tiles per CTA (persistent
+    grid) and ragged edges are covered."""
+    import delayed_pivoting as dp
+
+    torch = _torch()
+    g = torch.Generator(device="cuda").manual_seed(M * 7 + N * 3 + K)
+    lda, ldb, ldc = M + 3, K + 1, M + 5
+    A = torch.randn(K, lda, dtype=torch.float64, device="cuda", generator=g)  # column-major lda x K
+    B = torch.randn(N, ldb, dtype=torch.float64, device="cuda", generator=g)
+    C = torch.randn(N, ldc, dtype=torch.float64, device="cuda", generator=g)
+    C0 = C.clone()
+    ref = C0[:, :M].T - A[:, :M].T @ B[:, :K].T
+    p = dp.PRECISION_MIXED_BF16X3 if prec == "x3" else dp.PRECISION_MIXED_BF16X6
+    assert dp.schur_update_mixed_device(M, N, K, A, lda, B, ldb, C, ldc, precision=p) == 0
+    err = (C[:, :M].T - ref).abs().max().item()
+    scale = A[:, :M].abs().max().item() * B[:, :K].abs().max().item()
+    tol = K * scale * (2.0**-14 if prec == "x3" else 2.0**-21)
+    assert err <= tol, (err, tol)
+    assert torch.equal(C[:, M:], C0[:, M:])
