@@ -358,3 +358,30 @@ def test_batched_near_tie_detector_counts_planted_ties(built):
     rep = b.last_report()
     assert rep["near_ties"] == 2, rep
     assert rep["max_closeness"] == 1.0 and rep["info"] == 3
+
+
+@pytest.mark.gpu
+def test_batched_nan_inputs_follow_the_reference_gpu_rule(built):
+    """NaN never wins in the batched kernel either: NaN entry / column / row
+    matrices get the oracle's records."""
+    import delayed_pivoting as dp
+    import oracle as orc
+
+    mats = []
+    for seed, kind in ((41, "entry"), (42, "column"), (43, "row")):
+        a = dp.planted_matrix(250, 250, seed)
+        if kind == "entry":
+            a[60, 80] = np.nan
+        elif kind == "column":
+            a[:, 10] = np.nan
+        else:
+            a[125, :] = np.nan
+        mats.append(a)
+    ns = np.array([250, 250, 250], dtype=np.int32)
+    b, host, fac, ipiv, jpiv, info = run_batch(ns, None, 0, matrices=mats)
+    ip, jp = split_records(ipiv, ns), split_records(jpiv, ns)
+    for i, a in enumerate(mats):
+        oi, oj, oinfo = orc.oracle_getrf(a.copy(order="F"))
+        assert info[i] == oinfo
+        assert np.array_equal(ip[i], oi) and np.array_equal(jp[i], oj)
+    assert b.last_report()["near_ties"] == 0

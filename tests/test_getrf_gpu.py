@@ -380,3 +380,37 @@ def test_mixed_schur_update_against_torch(built, M, N, K, prec):
     tol = K * scale * (2.0**-14 if prec == "x3" else 2.0**-21)
     assert err <= tol, (err, tol)
     assert torch.equal(C[:, M:], C0[:, M:])
+
+
+def _nan_matrix(n, kind, seed):
+    import delayed_pivoting as dp
+
+    a = dp.planted_matrix(n, n, seed)
+    if kind == "entry":
+        a[n // 4, n // 3] = np.nan
+    elif kind == "column":
+        a[:, 10] = np.nan
+    else:  # row
+        a[n // 2, :] = np.nan
+    return a
+
+
+@pytest.mark.parametrize("n", [300, 700])
+@pytest.mark.parametrize("kind", ["entry", "column", "row"])
+def test_nan_inputs_follow_the_reference_gpu_rule(built, n, kind):
+    """NaN never wins a pivot search (delayed_lu_cuda/delayed_dgetrf_cuda.cu:46):
+    a NaN entry, a NaN column (delayed to the end) and a NaN row give the
+    oracle's records and info on the single-CTA (n = 300) and the cluster
+    panel (n = 700) paths, with no order-sensitive decision."""
+    import oracle as orc
+
+    a = _nan_matrix(n, kind, 31 + n)
+    o = a.copy(order="F")
+    oi, oj, oinfo = orc.oracle_getrf(o)
+    fac, ipiv, jpiv, info, st = run_device(a, n, n)
+    assert st == 0 and info == oinfo
+    if kind != "entry":
+        assert info == n - 1  # the NaN column / row ends as the delayed block
+    np.testing.assert_array_equal(ipiv, oi)
+    np.testing.assert_array_equal(jpiv, oj)
+    assert_no_near_ties(info)
