@@ -76,7 +76,8 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "mixed3"],
                     help="trailing-update arithmetic of the lu workload: FP64, BF16x6, BF16x3")
     ap.add_argument("--workload", default="serve",
-                    choices=["serve", "lu", "batched", "ir", "stream"])
+                    choices=["serve", "lu", "batched", "ir", "stream", "update"])
+    ap.add_argument("--k", type=int, default=256, help="update: inner dimension (outer block)")
     ap.add_argument("--loads", default="0.5,0.7,0.9",
                     help="stream: offered loads as fractions of the measured mixed capacity")
     ap.add_argument("--requests", type=int, default=1000, help="requests per serve step")
@@ -275,6 +276,8 @@ def main():
         return run_ir(args)
     if args.workload == "stream":
         return run_stream(args)
+    if args.workload == "update":
+        return run_update(args)
     return run_lu(args)
 
 
@@ -1034,6 +1037,70 @@ def run_serve(args):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+    return 0
+
+
+def run_update(args):
+    """The trailing update alone, C (n x n) -= A (n x k) B (k x n), as the LU
+    runs it: on the tensor cores (BF16x6 split, dp_schur_update_mixed_device:
+    the two split kernels and the persistent tcgen05 kernel) and in FP64 on
+    DMMA (dp_schur_update_device).  Per call: CUDA events on the stream
+    around the call; the mixed entry point synchronises itself, so its time
+    includes one host round trip.  Rooflines: algorithmic bytes 16 n^2 +
+    8 k (2 n) (C read and written once, A and B read once) against the
+    measured HBM copy bandwidth, and 6 x 2 n^2 k BF16 flops against the
+    measured BF16 peak; the FP64 kernel against the live cuBLAS DGEMM."""
+    import torch
+    import delayed_pivoting as dp
+
+    world, rank, local, dev, dist = _dist_setup(torch)
+    n, k = args.n, args.k
+    A = torch.randn(k, n, dtype=torch.float64, device=dev)  # column-major n x k
+    B = torch.randn(n, k, dtype=torch.float64, device=dev)  # column-major k x n
+    C = torch.randn(n, n, dtype=torch.float64, device=dev)
+    peaks = measured_peaks()
+    out = {}
+    for name, fn in (("mixed_bf16x6", lambda: dp.schur_update_mixed_device(n, n, k, A, n, B, k, C, n)),
+                     ("fp64_dmma", lambda: dp.schur_update_device(n, n, k, A, n, B, k, C, n))):
+        for _ in range(args.warmup):
+            assert fn() == 0
+        torch.cuda.synchronize()
+        ms = []
+        with ClockSampler(local) as clk:
+            for _ in range(args.steps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                assert fn() == 0
+                e1.record()
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+        t = statistics.median(ms) * 1e-3
+        fl, by = 2.0 * n * n * k, 16.0 * n * n + 16.0 * k * n
+        out[name] = {"ms_median": t * 1e3, "fp64_equiv_tflops": fl / t / 1e12,
+                     "alg_gbs": by / t / 1e9, "hbm_frac": by / t / 1e9 / peaks["hbm_gbs"],
+                     "clocks": clk.summary()}
+        if name.startswith("mixed"):
+            bf16 = peaks.get("bf16_tflops") or 1590.0
+            out[name]["bf16_tflops"] = 6 * fl / t / 1e12
+            out[name]["tensor_frac"] = 6 * fl / t / 1e12 / bf16
+    fp64 = fp64_peak_tflops(torch, dev)
+    out["fp64_dmma"]["frac_of_cublas_dgemm"] = out["fp64_dmma"]["fp64_equiv_tflops"] / fp64
+    m = out["mixed_bf16x6"]
+    if rank == 0:
+        print(json.dumps({
+            "metric": f"trailing update C -= A B, n={n}, k={k}: mixed BF16x6 tensor-core kernel",
+            "value": m["fp64_equiv_tflops"], "unit": "TFLOP/s (FP64-equivalent 2 n^2 k)",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": m["ms_median"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 (operands split to BF16, FP32 accumulation)",
+            "data": "synthetic N(0,1)",
+            "config": {"workload": f"Schur update n={n} k={k}", "n": n, "k": k,
+                       "l2": f"C {8 * n * n / 2**30:.2f} GiB"},
+            "roofline": {"bound": "hbm", "achieved": m["alg_gbs"], "peak": peaks["hbm_gbs"],
+                         "unit": "GB/s", "frac": m["hbm_frac"], "traffic": None,
+                         "tensor_frac": m["tensor_frac"]},
+            "kernels": out, "fp64_peak_tflops_cublas_dgemm": fp64}), flush=True)
     return 0
 
 

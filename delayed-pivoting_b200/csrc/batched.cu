@@ -842,6 +842,11 @@ int launch_raw(int count, int max_n, int sms, const int* d_n, const long long* d
 
 }  // namespace batch
 
+void launch_fill_normal(double* x, long long len, unsigned long long seed, cudaStream_t st) {
+  note_launch();
+  batch::fill_normal_kernel<<<1184, 256, 0, st>>>(x, len, seed);
+}
+
 int panel_small_max_rows() { return batch::kMaxN; }
 int panel_small_max_width() { return batch::kMaxNb; }
 

@@ -45,6 +45,8 @@ constexpr int kPanelThreadsHost = 256;
 int panel_small_max_rows();
 int panel_small_max_width();
 int launch_panel_small(const PanelParams& pp, cudaStream_t st);
+// x[0..len) <- seeded N(0,1) (hashed Box-Muller; tuner inputs).
+void launch_fill_normal(double* x, long long len, unsigned long long seed, cudaStream_t st);
 size_t panel_smem_bytes(int w, int rows_per_cta);
 
 // Applies the composite row permutation of one panel (swap list written by

@@ -797,6 +797,31 @@ bool valid_arguments(int m, int n, const double* a, int lda, const int* ipiv, co
   return matrix_byte_count(lda, n, ignored);
 }
 
+// Panel-width tuning table (dp_getrf_autotune): per device and order bucket
+// floor(log2 n), the (panel width, outer block) pair the tuner found fastest;
+// {0, 0} where untuned.  Used by the entry points when the caller leaves
+// both widths automatic.
+constexpr int kTuneBuckets = 32;
+std::mutex g_tune_mutex;
+int g_tune[64][kTuneBuckets][2] = {};
+
+int tune_bucket(int n) {
+  int b = 0;
+  while (b + 1 < kTuneBuckets && (2LL << b) <= n) ++b;
+  return b;
+}
+
+void apply_tuned_widths(int pivots, Options& o) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  const int* t = g_tune[dev][tune_bucket(pivots)];
+  if (t[0] > 0 && t[1] > 0) {
+    o.nb = t[0];
+    o.nb_outer = t[1];
+  }
+}
+
 bool resolve_options(const dp_options* in, Options& o) {
   if (!in) return true;
   if (in->nb < 0 || in->panel_rows < 0) return false;
@@ -829,6 +854,7 @@ int getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* 
   if (!valid_arguments(m, n, d_a, lda, ipiv, jpiv) || !resolve_options(opt, o))
     return kInvalidArgument;
   const int pivots = std::min(m, n);
+  if (!opt || (opt->nb == 0 && opt->nb_outer == 0)) apply_tuned_widths(pivots, o);
   *info = pivots;
   for (int k = 0; k < pivots; ++k) ipiv[k] = jpiv[k] = k;
   if (pivots == 0) {
@@ -1132,6 +1158,121 @@ int dp_getrf_hybrid_host(int m, int n, double* a, int lda, int* ipiv, int* jpiv,
 int dp_getrf_last_report(dp_getrf_report* out) {
   if (!out) return DP_INVALID_ARGUMENT;
   *out = dp::g_report;
+  return DP_SUCCESS;
+}
+
+int dp_getrf_autotune(int n, int* nb, int* nb_outer, void* stream) {
+  if (n < 1 || n > 65536) return DP_INVALID_ARGUMENT;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return DP_CUDA_FAILURE;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  static const int kCand[][2] = {{32, 64},  {64, 64},   {32, 128}, {64, 128},
+                                 {128, 128}, {32, 256}, {64, 256}, {128, 256}};
+  const size_t elems = (size_t)n * n;
+  double *src = nullptr, *work = nullptr;
+  if (cudaMallocAsync(reinterpret_cast<void**>(&src), sizeof(double) * elems, st) != cudaSuccess ||
+      cudaMallocAsync(reinterpret_cast<void**>(&work), sizeof(double) * elems, st) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    if (src) cudaFreeAsync(src, st);
+    cudaStreamSynchronize(st);
+    return DP_ALLOCATION_FAILED;
+  }
+  dp::launch_fill_normal(src, (long long)elems, 0x5eed0000ull + (unsigned long long)n, st);
+  std::vector<int> ipiv(n), jpiv(n);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess
+               ? DP_SUCCESS
+               : DP_CUDA_FAILURE;
+  float best = 1e30f;
+  int bnb = 0, bNB = 0;
+  for (const auto& c : kCand) {
+    if (rc != DP_SUCCESS) break;
+    if (c[1] > n && c[1] != 64) continue;  // an outer block beyond the order changes nothing
+    dp_options o;
+    dp_options_init(&o);
+    o.nb = c[0];
+    o.nb_outer = c[1];
+    float t = 1e30f;
+    for (int rep = 0; rep < 2 && rc == DP_SUCCESS; ++rep) {
+      int info = -1;
+      if (cudaMemcpyAsync(work, src, sizeof(double) * elems, cudaMemcpyDeviceToDevice, st) !=
+              cudaSuccess ||
+          cudaEventRecord(e0, st) != cudaSuccess) {
+        rc = DP_CUDA_FAILURE;
+        break;
+      }
+      rc = dp::getrf_device(n, n, work, n, ipiv.data(), jpiv.data(), &info, st, &o);
+      float ms = 0.f;
+      if (rc == DP_SUCCESS && (cudaEventRecord(e1, st) != cudaSuccess ||
+                               cudaEventSynchronize(e1) != cudaSuccess ||
+                               cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+        rc = DP_CUDA_FAILURE;
+      t = std::min(t, ms);
+    }
+    if (rc == DP_SUCCESS && t < best) {
+      best = t;
+      bnb = c[0];
+      bNB = c[1];
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFreeAsync(src, st);
+  cudaFreeAsync(work, st);
+  cudaStreamSynchronize(st);
+  if (rc != DP_SUCCESS) return rc;
+  {
+    std::lock_guard<std::mutex> lock(dp::g_tune_mutex);
+    dp::g_tune[dev][dp::tune_bucket(n)][0] = bnb;
+    dp::g_tune[dev][dp::tune_bucket(n)][1] = bNB;
+  }
+  if (nb) *nb = bnb;
+  if (nb_outer) *nb_outer = bNB;
+  return DP_SUCCESS;
+}
+
+int dp_getrf_tune_save(const char* path) {
+  int dev = 0;
+  if (!path || cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+    return DP_INVALID_ARGUMENT;
+  FILE* f = std::fopen(path, "w");
+  if (!f) return DP_INVALID_ARGUMENT;
+  {
+    std::lock_guard<std::mutex> lock(dp::g_tune_mutex);
+    for (int b = 0; b < dp::kTuneBuckets; ++b)
+      if (dp::g_tune[dev][b][0] > 0)
+        std::fprintf(f, "%lld %lld %d %d\n", 1LL << b, (2LL << b) - 1, dp::g_tune[dev][b][0],
+                     dp::g_tune[dev][b][1]);
+  }
+  return std::fclose(f) == 0 ? DP_SUCCESS : DP_INVALID_ARGUMENT;
+}
+
+int dp_getrf_tune_load(const char* path) {
+  int dev = 0;
+  if (!path || cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+    return DP_INVALID_ARGUMENT;
+  FILE* f = std::fopen(path, "r");
+  if (!f) return DP_INVALID_ARGUMENT;
+  int table[dp::kTuneBuckets][2] = {};
+  long long lo = 0, hi = 0;
+  int nb = 0, NB = 0, rc = DP_SUCCESS;
+  while (true) {
+    const int got = std::fscanf(f, "%lld %lld %d %d", &lo, &hi, &nb, &NB);
+    if (got == EOF) break;
+    const int b = lo >= 1 ? dp::tune_bucket((int)std::min<long long>(lo, 1 << 30)) : -1;
+    if (got != 4 || b < 0 || (1LL << b) != lo || hi != (2LL << b) - 1 || nb < 1 ||
+        nb > dp::kMaxPanelWidth || NB < nb) {
+      rc = DP_INVALID_ARGUMENT;
+      break;
+    }
+    table[b][0] = nb;
+    table[b][1] = NB;
+  }
+  std::fclose(f);
+  if (rc != DP_SUCCESS) return rc;
+  std::lock_guard<std::mutex> lock(dp::g_tune_mutex);
+  std::memcpy(dp::g_tune[dev], table, sizeof(table));
   return DP_SUCCESS;
 }
 

@@ -338,6 +338,32 @@ def getrf_device_ex(m, n, d_a, lda, ipiv, jpiv, stream=None, nb=64, threshold=0.
     return st, info.value
 
 
+def getrf_autotune(n, stream=None):
+    """dp_getrf_autotune: times the panel-width pairs for order n and records
+    the fastest for n's order bucket; returns (status, nb, nb_outer)."""
+    L = lib()
+    L.dp_getrf_autotune.restype = ctypes.c_int
+    L.dp_getrf_autotune.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(ctypes.c_int), ctypes.c_void_p]
+    nb, nbo = ctypes.c_int(0), ctypes.c_int(0)
+    st = L.dp_getrf_autotune(n, ctypes.byref(nb), ctypes.byref(nbo), _stream(stream))
+    return st, nb.value, nbo.value
+
+
+def getrf_tune_save(path) -> int:
+    L = lib()
+    L.dp_getrf_tune_save.restype = ctypes.c_int
+    L.dp_getrf_tune_save.argtypes = [ctypes.c_char_p]
+    return L.dp_getrf_tune_save(str(path).encode())
+
+
+def getrf_tune_load(path) -> int:
+    L = lib()
+    L.dp_getrf_tune_load.restype = ctypes.c_int
+    L.dp_getrf_tune_load.argtypes = [ctypes.c_char_p]
+    return L.dp_getrf_tune_load(str(path).encode())
+
+
 def getrf_last_report() -> dict:
     """dp_getrf_last_report: the near-tie report of this thread's last
     dp_getrf_* call (decisions, near_ties, max_closeness, info)."""

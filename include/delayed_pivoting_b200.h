@@ -101,6 +101,21 @@ int dp_getrf_device_noalloc(int m, int n, double *d_a, int lda, int *ipiv, int *
 int dp_getrf_device_ex(int m, int n, double *d_a, int lda, int *ipiv, int *jpiv, int *info,
                        void *stream, const dp_options *opt);
 
+/* Panel-width autotuner of the single-matrix LU (no reference counterpart:
+ * the reference fixes block_size = 64, delayed_lu/delayed_dgetrf.cpp:16).
+ * Times the (panel width nb, outer block nb_outer) pairs {32, 64, 128} x
+ * {64, 128, 256} (nb <= nb_outer) on a seeded N(0,1) n x n matrix, best of
+ * two runs each, and records the fastest pair for n's order bucket
+ * [2^b, 2^(b+1)) on the current device.  Every dp_getrf_* call whose caller
+ * leaves both widths automatic (no options, or nb = nb_outer = 0) then uses
+ * the pair of its min(m, n) bucket.  Widths change rounding only, never the
+ * records.  Allocates 2 n^2 doubles while it runs; synchronises `stream`.
+ * dp_getrf_tune_save / _load write / read the current device's table
+ * ("<smallest n> <largest n> <nb> <nb_outer>" per tuned bucket). */
+int dp_getrf_autotune(int n, int *nb, int *nb_outer, void *stream);
+int dp_getrf_tune_save(const char *path);
+int dp_getrf_tune_load(const char *path);
+
 /* Near-tie report (no reference counterpart; the reference decides every
  * pivot by a bare argmax, delayed_lu/delayed_dgetrf.cpp:170-178 and :32-47,
  * delayed_lu_cuda/delayed_dgetrf_cuda.cu:13-20).  Every pivot decision of a

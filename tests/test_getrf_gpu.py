@@ -414,3 +414,32 @@ def test_nan_inputs_follow_the_reference_gpu_rule(built, n, kind):
     np.testing.assert_array_equal(ipiv, oi)
     np.testing.assert_array_equal(jpiv, oj)
     assert_no_near_ties(info)
+
+
+def test_autotuned_widths_keep_the_records(built, tmp_path):
+    """dp_getrf_autotune picks a (panel width, outer block) pair for n's
+    bucket; the default entry point then uses it and still reproduces the
+    reference's records; the table survives a save / load round trip."""
+    import delayed_pivoting as dp
+
+    _torch()
+    st, nb, nbo = dp.getrf_autotune(2000)
+    assert st == 0 and nb in (32, 64, 128) and nbo in (64, 128, 256) and nb <= nbo
+    a, case = gc.load("square_2000_zero20")
+    fac, ipiv, jpiv, info, st = run_device(a, 2000, 2000)
+    assert st == 0 and info == case["info"]
+    np.testing.assert_array_equal(ipiv, case["ipiv"])
+    np.testing.assert_array_equal(jpiv, case["jpiv"])
+    assert_no_near_ties(info)
+    path = tmp_path / "lu_tune.txt"
+    assert dp.getrf_tune_save(path) == 0
+    line = [ln.split() for ln in path.read_text().splitlines() if ln.split()[0] == "1024"]
+    assert line == [["1024", "2047", str(nb), str(nbo)]]
+    assert dp.getrf_tune_load(path) == 0
+    bad = tmp_path / "bad.txt"
+    bad.write_text("1000 2047 64 256\n")
+    assert dp.getrf_tune_load(bad) == dp.INVALID_ARGUMENT
+    # leave the process's table empty (later tests use the default widths)
+    empty = tmp_path / "empty.txt"
+    empty.write_text("")
+    assert dp.getrf_tune_load(empty) == 0
