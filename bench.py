@@ -62,7 +62,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=16384)
-    ap.add_argument("--nb", type=int, default=64)
+    ap.add_argument("--nb", type=int, default=0,
+                    help="LU panel width (0: the autotuned / default width)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="lu: skip dp_getrf_autotune (default widths 64 / 256)")
     ap.add_argument("--nb-outer", type=int, default=0,
                     help="LU outer block width (0: the library's default)")
     ap.add_argument("--lookahead", type=int, default=0, choices=[0, 1, 2],
@@ -310,6 +313,13 @@ def run_lu(args):
     L = dp.lib()
     prec = {"fp64": dp.PRECISION_FP64, "mixed": dp.PRECISION_MIXED_BF16X6,
             "mixed3": dp.PRECISION_MIXED_BF16X3}[args.precision]
+    tuned = None
+    if not args.no_autotune and args.nb == 0 and args.nb_outer == 0:
+        st_t, tnb, tnbo = dp.getrf_autotune(n, stream=stream)
+        if st_t != 0:
+            raise RuntimeError(f"dp_getrf_autotune: status {st_t}")
+        tuned = {"nb": tnb, "nb_outer": tnbo, "candidates": "nb {32,64,128} x nb_outer "
+                 "{64,128,256}, best of 2 on a seeded N(0,1) matrix of the same order"}
 
     def step(timed_events=None):
         work.copy_(orig)
@@ -478,7 +488,9 @@ def run_lu(args):
             "data": f"synthetic: N(0,1) MT19937-64 seeded per rank, {w['n_tiny']} tiny (x1e-18) + "
                     f"{w['n_zero']} zero columns",
             "config": {"workload": f"delayed_getrf {args.precision} n={n} (single matrix)", "n": n,
-                       "nb": args.nb, "nb_outer": args.nb_outer or 256,
+                       "nb": (tuned or {}).get("nb", args.nb or 64),
+                       "nb_outer": (tuned or {}).get("nb_outer", args.nb_outer or 256),
+                       "autotuned": tuned,
                        "lookahead": {0: "auto", 1: "on", 2: "off"}[args.lookahead],
                        "parallelism": f"replicas x{world}",
                        "l2": f"input {8 * n * n / 2**30:.2f} GiB " + (
@@ -867,6 +879,9 @@ def lu_key(torch, dp, dev, L, n=16384, warmup=2, steps=3):
     ipiv = np.zeros(n, dtype=np.int32)
     jpiv = np.zeros(n, dtype=np.int32)
     stream = torch.cuda.current_stream(dev)
+    st_t, tnb, tnbo = dp.getrf_autotune(n, stream=stream)
+    if st_t != 0:
+        raise RuntimeError(f"dp_getrf_autotune: status {st_t}")
     ms, info = [], None
     for i in range(warmup + steps + 1):
         work.copy_(orig)
@@ -877,11 +892,13 @@ def lu_key(torch, dp, dev, L, n=16384, warmup=2, steps=3):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        st, info = dp.getrf_device_ex(n, n, work, n, ipiv, jpiv, stream=stream)
+        st, info = dp.delayed_getrf_cuda_device(n, n, work, n, ipiv, jpiv, stream=stream)
         e1.record(stream)
         e1.synchronize()
         if st != 0:
             raise RuntimeError(dp.delayed_getrf_cuda_status_string(st))
+        if i == warmup + steps - 1:
+            report = dp.getrf_last_report()
         if last:
             L.dp_stats_enable(0)
         elif i >= warmup:
@@ -897,6 +914,7 @@ def lu_key(torch, dp, dev, L, n=16384, warmup=2, steps=3):
             for i, nm in enumerate(fam) if stats["launches"][i]}
     out = {"n": n, "gflops": gf, "ms_per_factorisation": statistics.mean(ms),
            "step_ms": [round(x, 3) for x in ms], "info": info,
+           "autotuned_widths": {"nb": tnb, "nb_outer": tnbo}, "near_tie_report": report,
            "fp64_peak_tflops_cublas_dgemm": fp64, "frac_of_fp64_peak": gf / 1e3 / fp64,
            "target_frac": 0.70, "kernels_one_step": kern,
            "panel_roofline": _family_roofline(stats, 0, measured_peaks())}
