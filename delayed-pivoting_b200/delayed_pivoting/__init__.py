@@ -26,6 +26,8 @@ from .api import (  # noqa: F401
     BATCH_MAX_N, BATCH_MAX_NB, BATCH_BUCKETS, BatchOptions, Batch, BatchError, batch_options,
     batch_autotune, batch_tune_save, batch_tune_load, Factor, Server, ServerOptions, Request,
     RequestResult, ServerStats, server_options, server_clock, schur_update_device, gemm_tile,
+    schur_update_mixed_device, GetrfReport, getrf_last_report, getrf_autotune, getrf_tune_save,
+    getrf_tune_load,
 )
 from .inputs import (  # noqa: F401
     normal_matrix, plant_columns, mt64_nth, planted_matrix, uniform_stream, normal_vector,

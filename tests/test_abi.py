@@ -111,3 +111,17 @@ def test_options_rejected():
     assert dp.getrf_device_ex(4, 4, 0x1000, 4, ipiv, jpiv, threshold=float("nan")) == (dp.INVALID_ARGUMENT, -1)
     assert dp.getrf_device_ex(4, 4, 0x1000, 4, ipiv, jpiv, policy=7) == (dp.INVALID_ARGUMENT, -1)
     assert dp.getrf_device_ex(4, 4, 0x1000, 4, ipiv, jpiv, nb=-2) == (dp.INVALID_ARGUMENT, -1)
+
+
+def test_package_exports_every_binding():
+    """Every public function of delayed_pivoting.api is reachable from the
+    package (the tests and bench.py call them as delayed_pivoting.<name>)."""
+    import re
+    from pathlib import Path
+
+    import delayed_pivoting as dp
+
+    src = (Path(dp.__file__).parent / "api.py").read_text()
+    names = re.findall(r"^def ([a-z][a-z0-9_]*)\(", src, re.M)
+    assert names
+    assert [n for n in names if not hasattr(dp, n)] == []
