@@ -165,13 +165,15 @@ struct Factor {
   unsigned* d_flags = nullptr;        // triangular-solve block flags, then a status word
   double* d_inv = nullptr;            // inverses of the diagonal blocks of L and U
   unsigned epoch = 0;                 // last epoch used on d_flags
+  int panel_rows = 0;                 // rows per panel CTA of its factorisations (0: default)
   std::vector<int> ipiv, jpiv;
 };
 
 // Device bytes a Factor of order n holds.
 size_t factor_bytes(int n);
 // Factor A (n x n, lda, device, not modified) at `precision`; synchronises st.
-int factor_create(Factor** out, int n, const double* A, int lda, int precision, cudaStream_t st);
+int factor_create(Factor** out, int n, const double* A, int lda, int precision, cudaStream_t st,
+                  int panel_rows = 0);
 // Solve A X = B with FP64 refinement; B (n x nrhs, device) becomes X.  Mixed
 // factors whose refinement stalls are replaced by plain FP64 factors of A.
 int factor_solve(Factor* f, const double* A, int lda, double* B, int ldb, int nrhs, int max_iter,

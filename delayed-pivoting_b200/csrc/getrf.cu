@@ -194,13 +194,16 @@ bool plan_panel(int rows, int& w, int target_rows, const DeviceInfo& di, int& G,
   return false;
 }
 
-// Cluster panel: C CTAs (one cluster) of R rows each; the R x w slice per
-// CTA must fit in shared memory.  Returns false when even an 8-wide panel
-// does not fit (very tall panels then use panel_factor_kernel).
-bool plan_cluster(int rows, int& w, const DeviceInfo& di, int& C, int& R) {
+// Cluster panel: C CTAs (one cluster) of R rows each, about target_rows per
+// CTA (fewer CTAs per panel: less SM time per column, more latency); the
+// R x w slice per CTA must fit in shared memory.  Returns false when even an
+// 8-wide panel does not fit (very tall panels then use panel_factor_kernel).
+bool plan_cluster(int rows, int& w, const DeviceInfo& di, int& C, int& R,
+                  int target_rows = kDefaultPanelRows) {
   if (di.max_cluster <= 0) return false;
   const size_t budget = (size_t)di.smem_optin - 1024 - 512;
-  C = (int)std::min<long long>(di.max_cluster, std::max(1LL, ((long long)rows + 255) / 256));
+  const long long t = std::max(1, target_rows);
+  C = (int)std::min<long long>(di.max_cluster, std::max(1LL, ((long long)rows + t - 1) / t));
   R = (rows + C - 1) / C;
   int wf = w;
   while (wf >= 1 && panel_cluster_smem_bytes(wf, R) > budget) --wf;
@@ -572,7 +575,7 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       const bool use_small = o.panel_kernel == 0 && m - b <= panel_small_max_rows();
       if (use_small) w = std::min(w, panel_small_max_width());
       const bool use_cluster =
-          !use_small && o.panel_kernel != 2 && plan_cluster(m - b, w, di, G, R);
+          !use_small && o.panel_kernel != 2 && plan_cluster(m - b, w, di, G, R, o.panel_rows);
       // panel_kernel 1 is the cluster panel or nothing: the grid panel's
       // mailboxes may not exist in the workspace (the allocation-free path
       // lays them out with zero size)

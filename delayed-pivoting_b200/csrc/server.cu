@@ -321,7 +321,8 @@ void dp_server::large_worker() {
     std::shared_ptr<Resident> keep;
     if (r0.factor_id == 0) {
       Factor* f = nullptr;
-      const int status = dp::factor_create(&f, r0.n, r0.d_a, r0.lda, opt.precision, st);
+      const int status =
+          dp::factor_create(&f, r0.n, r0.d_a, r0.lda, opt.precision, st, opt.panel_rows);
       out[0].status = status;
       out[0].info = f ? f->info : -1;
       if (f) out[0].factor_ms = f->factor_ms;
@@ -746,6 +747,7 @@ int dp_server_create(dp_server** out, const dp_server_options* opt) {
   if (o.large_workers == 0) o.large_workers = 6;
   if (!dp::valid_precision(o.precision) ||
       o.large_workers < 1 || o.large_workers > 64 || o.small_max_n > DP_BATCH_MAX_N ||
+      o.panel_rows < 0 ||
       o.small_max_batch < 1 || o.max_iter < 0 || !(o.tol > 0.0))
     return DP_INVALID_ARGUMENT;
   auto* s = new (std::nothrow) dp_server;

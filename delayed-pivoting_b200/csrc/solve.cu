@@ -304,6 +304,7 @@ int factorize(Factor& f, const double* A, int lda, int prec, cudaStream_t st) {
   dp_options opt;
   dp_options_init(&opt);
   opt.precision = prec;
+  opt.panel_rows = f.panel_rows;
   int info = -1;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
@@ -507,7 +508,8 @@ size_t factor_bytes(int n) {
          sizeof(unsigned) * ((size_t)tri_solve_flag_count(n) + 1);
 }
 
-int factor_create(Factor** out, int n, const double* A, int lda, int precision, cudaStream_t st) {
+int factor_create(Factor** out, int n, const double* A, int lda, int precision, cudaStream_t st,
+                  int panel_rows) {
   if (!out) return kInvalidArgument;
   *out = nullptr;
   if (n < 1 || lda < n || !A ||
@@ -516,6 +518,7 @@ int factor_create(Factor** out, int n, const double* A, int lda, int precision, 
   auto* f = new (std::nothrow) Factor;
   if (!f) return kAllocationFailed;
   f->n = n;
+  f->panel_rows = std::max(0, panel_rows);
   f->ipiv.resize(n);
   f->jpiv.resize(n);
   double* normA = nullptr;

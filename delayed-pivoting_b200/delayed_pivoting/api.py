@@ -85,7 +85,8 @@ class ServerOptions(ctypes.Structure):
         ("small_max_batch", ctypes.c_int),
         ("max_iter", ctypes.c_int),
         ("tol", ctypes.c_double),
-        ("reserved", ctypes.c_int * 4),
+        ("panel_rows", ctypes.c_int),
+        ("reserved", ctypes.c_int * 3),
     ]
 
 

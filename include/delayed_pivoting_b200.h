@@ -276,7 +276,9 @@ typedef struct dp_server_options {
   int small_max_batch; /* requests per batched launch; 0: 2048 */
   int max_iter;        /* refinement steps per solve; 0: 10 */
   double tol;          /* backward-error target; 0: 1e-14 */
-  int reserved[4];
+  int panel_rows;      /* rows per CTA of the large factorisations' cluster panels (fewer CTAs
+                          per panel: less SM time, more latency); 0: the library default (256) */
+  int reserved[3];
 } dp_server_options;
 
 void dp_server_options_init(dp_server_options *opt);
