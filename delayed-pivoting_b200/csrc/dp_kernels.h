@@ -132,10 +132,11 @@ void launch_set_record(int* ipiv, int* jpiv, int k, int p, int q, cudaStream_t s
 // ---- triangular solves with many right-hand sides (trisolve.cu) ----------
 
 // Y (n x nrhs, nrhs <= tri_solve_rhs_max()) <- L^{-1} Y (unit lower) or
-// U^{-1} Y (upper with diagonal), one cooperative launch; `flags` holds
-// tri_solve_flag_count(n) words whose values differ from `epoch` (nonzero,
-// new for every launch that uses the same flags); a bounded wait that runs
-// out sets *status = kDeviceTimeout.
+// U^{-1} Y (upper with diagonal), one launch; `flags` holds
+// tri_solve_flag_count(n) words: one per 64-row block, whose values differ
+// from `epoch` (nonzero, new for every launch that uses the same flags), then
+// the launch's block-ticket counter (reset by the launch); a bounded wait
+// that runs out sets *status = kDeviceTimeout.
 // `inv` holds the inverses of the 64 x 64 diagonal blocks of L and U
 // (launch_diag_inverse, tri_inverse_doubles(n) doubles, 16-byte aligned).
 int tri_solve_rhs_max();

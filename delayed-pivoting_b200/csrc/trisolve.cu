@@ -3,9 +3,13 @@
 //
 // Y (n x nrhs, nrhs <= 64) <- T^{-1} Y with T the unit-lower L or the upper U
 // (with its diagonal) of a compact L\U factorisation.  The rows are cut into
-// blocks of 64; a persistent cooperative grid takes the blocks in dependency
-// order (lower: top down, upper: bottom up, CTA c taking blocks c, c + G, ...),
-// so the earliest unfinished block always has every input it needs.  A block
+// blocks of 64; a grid of up to 32 CTAs takes the blocks in dependency order
+// (lower: top down, upper: bottom up) by tickets from an atomic counter, so
+// every block a CTA waits for was claimed earlier by a CTA that is already
+// running: the earliest unfinished block always has every input it needs,
+// and no CTA depends on one that has not started - no co-residency (no
+// cooperative launch) is needed, and the launch starts on whatever SMs are
+// free.  A block
 //   1. starts from its rows of Y,
 //   2. for each earlier block j: waits until j is published (a flag set to the
 //      launch's epoch, read with acquire semantics, bounded by kSpinLimitNs),
@@ -17,8 +21,6 @@
 //      instead of a 64-step serial substitution on the critical path,
 //   4. writes y_i and publishes it (fence, then a release store of the flag).
 // A wait that runs out sets *status = kDeviceTimeout and every CTA returns.
-// All CTAs are co-resident (cooperative launch), so no wait depends on a CTA
-// that has not started.
 #include <algorithm>
 #include <atomic>
 
@@ -156,12 +158,17 @@ __global__ void __launch_bounds__(kTT, 1) tri_solve_kernel(const double* __restr
   double* ds = ys + kTB * kTRhs;     // the block's right-hand sides, [kTRhs][kTB]
   double* dg = ds + kTB * kTRhs;     // diagonal block T(i, i), [kTB][kTB] column-major
   double* ls = dg + kTB * kTB;       // T(i, j) double buffer, 2 x [kTB][kTB]
-  __shared__ int abort_all;
+  __shared__ int abort_all, ticket;
   const int tid = threadIdx.x, r = tid & (kTB - 1), cg = tid >> 6;
   const int nblk = (n + kTB - 1) / kTB;
+  int* const counter = reinterpret_cast<int*>(flags + nblk);  // zeroed before the launch
   if (tid == 0) abort_all = 0;
-  __syncthreads();
-  for (int q = blockIdx.x; q < nblk; q += gridDim.x) {
+  for (;;) {
+    if (tid == 0) ticket = atomicAdd(counter, 1);
+    __syncthreads();
+    const int q = ticket;
+    __syncthreads();  // every thread holds q before the next claim
+    if (q >= nblk || abort_all) break;
     const int i = kUpper ? nblk - 1 - q : q;
     const int r0 = i * kTB, rows = min(kTB, n - r0);
     const int deps = kUpper ? nblk - 1 - i : i;
@@ -283,22 +290,19 @@ int launch_tri(const double* T, long long ldt, int n, const double* inv, double*
                    : policy > 0 ? policy
                                 : std::max(1, std::min(kTMaxGrid, (nblk - policy - 1) / -policy));
   const int grid = std::max(1, std::min(std::min(nblk, want), sms * per_sm));
-  void* args[] = {(void*)&T,   (void*)&ldt,  (void*)&n,     (void*)&inv,
-                  (void*)&Y,   (void*)&ldy,  (void*)&nrhs,  (void*)&flags,
-                  (void*)&epoch, (void*)&status};
+  // the ticket counter after the block flags
+  if (cudaMemsetAsync(flags + nblk, 0, sizeof(unsigned), st) != cudaSuccess) return kCudaFailure;
   note_launch();
-  if (cudaLaunchCooperativeKernel((const void*)tri_solve_kernel<kUpper, MACC>, dim3(grid), dim3(kTT),
-                                  args, smem, st) != cudaSuccess) {
-    cudaGetLastError();
-    return kCudaFailure;
-  }
+  tri_solve_kernel<kUpper, MACC><<<grid, kTT, smem, st>>>(T, ldt, n, inv, Y, ldy, nrhs, flags,
+                                                          epoch, status);
+  if (cudaGetLastError() != cudaSuccess) return kCudaFailure;
   return kOk;
 }
 
 }  // namespace
 
 int tri_solve_rhs_max() { return kTRhs; }
-int tri_solve_flag_count(int n) { return (n + kTB - 1) / kTB; }
+int tri_solve_flag_count(int n) { return (n + kTB - 1) / kTB + 1; }  // block flags, ticket
 size_t tri_inverse_doubles(int n) { return (size_t)2 * kTB * kTB * ((n + kTB - 1) / kTB); }
 
 int launch_diag_inverse(const double* lu, long long ldlu, int n, double* inv, cudaStream_t st) {
