@@ -37,6 +37,12 @@ __global__ void panel_factor_kernel(PanelParams p);
 // in distributed shared memory (launched with a cluster dimension).
 __global__ void panel_cluster_kernel(PanelParams p);
 size_t panel_cluster_smem_bytes(int w, int rows_per_cta);
+// Cluster variant with the sub-panel in registers (panel_reg.cu), for up to
+// panel_reg_max_rows() rows per CTA: the kernel instance for R rows per CTA
+// (nullptr beyond the limit) and its dynamic shared memory.
+int panel_reg_max_rows();
+const void* panel_reg_kernel_for(int rows_per_cta);
+size_t panel_reg_smem_bytes(int w, int rows_per_cta);
 int panel_cluster_threads();
 constexpr int kPanelThreadsHost = 256;
 // Single-CTA panel (batched.cu) for panels of at most panel_small_max_rows()

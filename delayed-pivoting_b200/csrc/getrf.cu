@@ -66,6 +66,14 @@ int device_info(DeviceInfo& out) {
                              d.smem_optin - 1024) != cudaSuccess)
       return kCudaFailure;
     d.max_cluster = 0;
+    for (int r : {256, 512, 1024}) {  // the register-sub-panel cluster kernels
+      const void* f = panel_reg_kernel_for(r);
+      if (!f || cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     d.smem_optin - 1024) != cudaSuccess ||
+          cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+              cudaSuccess)
+        return kCudaFailure;
+    }
     if (cudaFuncSetAttribute(panel_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              d.smem_optin - 1024) == cudaSuccess) {
       cudaFuncSetAttribute(panel_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
@@ -98,7 +106,7 @@ int device_info(DeviceInfo& out) {
 
 struct Options {
   int precision = DP_PRECISION_FP64;
-  int panel_kernel = 0;  // 0 automatic (cluster when it fits), 1 cluster, 2 multi-CTA grid
+  int panel_kernel = 0;  // 0 automatic, 1 cluster, 2 multi-CTA grid, 3 shared-memory cluster
   int nb = kDefaultNb;
   int nb_outer = kDefaultNbOuter;
   double threshold = 0.0;
@@ -198,15 +206,23 @@ bool plan_panel(int rows, int& w, int target_rows, const DeviceInfo& di, int& G,
 // CTA (fewer CTAs per panel: less SM time per column, more latency); the
 // R x w slice per CTA must fit in shared memory.  Returns false when even an
 // 8-wide panel does not fit (very tall panels then use panel_factor_kernel).
+// `reg` selects the kernel: the register-sub-panel one where R allows it
+// (unless `smem_only`), else the shared-memory one.
 bool plan_cluster(int rows, int& w, const DeviceInfo& di, int& C, int& R,
-                  int target_rows = kDefaultPanelRows) {
+                  int target_rows = kDefaultPanelRows, bool* reg = nullptr,
+                  bool smem_only = false) {
   if (di.max_cluster <= 0) return false;
   const size_t budget = (size_t)di.smem_optin - 1024 - 512;
   const long long t = std::max(1, target_rows);
   C = (int)std::min<long long>(di.max_cluster, std::max(1LL, ((long long)rows + t - 1) / t));
   R = (rows + C - 1) / C;
+  const bool use_reg = !smem_only && R <= panel_reg_max_rows();
+  if (reg) *reg = use_reg;
+  auto bytes = [&](int ww) {
+    return use_reg ? panel_reg_smem_bytes(ww, R) : panel_cluster_smem_bytes(ww, R);
+  };
   int wf = w;
-  while (wf >= 1 && panel_cluster_smem_bytes(wf, R) > budget) --wf;
+  while (wf >= 1 && bytes(wf) > budget) --wf;
   if (wf < std::min(w, 8)) return false;
   if (wf < w) w = wf >= 16 ? (wf & ~7) : wf;
   return true;
@@ -574,8 +590,10 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       // short panels: one CTA, rows in registers (automatic choice only)
       const bool use_small = o.panel_kernel == 0 && m - b <= panel_small_max_rows();
       if (use_small) w = std::min(w, panel_small_max_width());
+      bool use_reg = false;
       const bool use_cluster =
-          !use_small && o.panel_kernel != 2 && plan_cluster(m - b, w, di, G, R, o.panel_rows);
+          !use_small && o.panel_kernel != 2 &&
+          plan_cluster(m - b, w, di, G, R, o.panel_rows, &use_reg, o.panel_kernel == 3);
       // panel_kernel 1 is the cluster panel or nothing: the grid panel's
       // mailboxes may not exist in the workspace (the allocation-free path
       // lays them out with zero size)
@@ -632,12 +650,18 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
         attr[0].val.clusterDim.z = 1;
         cfg.gridDim = dim3(G);
         cfg.blockDim = dim3(panel_cluster_threads());
-        cfg.dynamicSmemBytes = panel_cluster_smem_bytes(w, R);
+        cfg.dynamicSmemBytes =
+            use_reg ? panel_reg_smem_bytes(w, R) : panel_cluster_smem_bytes(w, R);
         cfg.stream = st;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         dp::note_launch();
-        DP_CHECK_CUDA(cudaLaunchKernelEx(&cfg, panel_cluster_kernel, pp));
+        if (use_reg) {
+          void* args[] = {&pp};
+          DP_CHECK_CUDA(cudaLaunchKernelExC(&cfg, panel_reg_kernel_for(R), args));
+        } else {
+          DP_CHECK_CUDA(cudaLaunchKernelEx(&cfg, panel_cluster_kernel, pp));
+        }
       } else {
         void* args[] = {&pp};
         dp::note_launch();
@@ -836,7 +860,7 @@ bool resolve_options(const dp_options* in, Options& o) {
   o.threshold = in->threshold;
   o.policy = in->policy;
   o.panel_rows = in->panel_rows ? in->panel_rows : kDefaultPanelRows;
-  if (in->panel_kernel < 0 || in->panel_kernel > 2) return false;
+  if (in->panel_kernel < 0 || in->panel_kernel > 3) return false;
   o.panel_kernel = in->panel_kernel;
   if (!valid_precision(in->precision))
     return false;

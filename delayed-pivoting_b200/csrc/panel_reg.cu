@@ -1,0 +1,522 @@
+// Panel factorisation on one thread-block cluster with the sub-panel in
+// registers (panels of up to 1024 rows per CTA).
+//
+// Same contract and semantics as panel_cluster_kernel
+// (delayed_lu/delayed_dgetrf.cpp:164-240: column partial-pivot search with
+// first-index ties and NaN never winning, acceptance |alpha| > threshold,
+// row swap, scaling by the reciprocal pivot, rank-1 update, stop at the first
+// column without an acceptable pivot), with less work per column:
+//   * every thread holds its rows' 8-column sub-panel slice in registers
+//     (RPT rows per thread), so the swap, scaling and rank-1 update of a step
+//     touch no shared memory;
+//   * a step pushes one ~100-byte slot per CTA to every CTA of the cluster
+//     (its candidate: magnitude, row, runner-up, reciprocal, source row and
+//     the row's 8 sub-panel values; the owner of row k also pushes row k's
+//     slice), then one hardware cluster barrier; every CTA then picks the
+//     same winner and updates its own registers;
+//   * the rest of each row (the finished L columns left of the sub-panel and
+//     the columns right of it) does not change during a sub-panel, so rows
+//     are moved there only at the sub-panel's end: every CTA replays the
+//     sub-panel's swaps into a composite source map and pulls the content of
+//     its moved rows - and the pivot rows for U12 = L11^{-1} A12 - from the
+//     owning CTAs' shared memory (phase A), a second cluster barrier, then
+//     writes them in place (phase B) and applies the rank-8 update of the
+//     columns right of the sub-panel.
+// Push buffers are indexed by step parity: a slot written at step s + 2 is
+// written after the barrier of step s + 1, which every reader of step s
+// passes only after finishing step s.  No spin-waits: the only waits are the
+// hardware barriers.
+#include <cooperative_groups.h>
+
+#include "dp_device.cuh"
+#include "dp_kernels.h"
+#include "panel_argmax.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace dp {
+
+namespace {
+
+using panel::LocalBest;
+using panel::offer;
+using panel::warp_best;
+using panel::warp_lb;
+using panel::warp_max_pos;
+
+constexpr int kT = 256;      // threads
+constexpr int kW = kT / 32;  // warps
+constexpr int kS = 8;        // sub-panel width
+constexpr int kMaxC = 16;    // largest cluster
+
+// One CTA's candidate (or row k) as pushed to every CTA.
+struct __align__(16) Slot {
+  double val;    // magnitude (>= 0)
+  double sec;    // runner-up magnitude among the CTA's rows
+  double inv;    // reciprocal of the candidate's entry in the current column
+  int row;       // global row, -1 when the CTA has no candidate
+  int orig;      // source row of its content (for the swap lists)
+  double v[kS];  // the row over the sub-panel's columns
+};
+
+__device__ __forceinline__ void copy_slot(Slot* dst, const Slot* src) {
+  const int4* s = reinterpret_cast<const int4*>(src);
+  int4* d = reinterpret_cast<int4*>(dst);
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(Slot) / sizeof(int4)); ++i) d[i] = s[i];
+}
+
+struct Layout {
+  double* sm;     // [w][RP] the panel slice
+  Slot* slots;    // [2][kMaxC] candidates, by step parity and CTA rank
+  Slot* kslot;    // [2] row k, by step parity
+  Slot* stage;    // [kW] per-warp candidates, then [1] row k
+  double* psave;  // [kS][W1] the sub-panel's pivot rows
+  double* tmp;    // [2 kS][W1] pulled content of moved rows
+  int* orig;      // [R] source row of each local row
+  int* plist;     // [kS][2] (k, pivot row) of the sub-panel's steps
+  int* chg;       // [1 + 2 * 2 kS]: count, then (position, source) pairs
+};
+
+__host__ __device__ inline size_t reg_align16(size_t bytes) { return (bytes + 15) & ~(size_t)15; }
+
+__host__ __device__ inline size_t reg_layout(unsigned char* base, int w, int R, Layout* L) {
+  const size_t rp = (size_t)(R | 1), w1 = (size_t)w + 1;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    unsigned char* p = base ? base + off : nullptr;
+    off += reg_align16(bytes);
+    return p;
+  };
+  unsigned char* sm = take(sizeof(double) * (size_t)w * rp);
+  unsigned char* slots = take(sizeof(Slot) * 2 * kMaxC);
+  unsigned char* kslot = take(sizeof(Slot) * 2);
+  unsigned char* stage = take(sizeof(Slot) * (kW + 1));
+  unsigned char* psave = take(sizeof(double) * kS * w1);
+  unsigned char* tmp = take(sizeof(double) * 2 * kS * w1);
+  unsigned char* orig = take(sizeof(int) * (size_t)R);
+  unsigned char* plist = take(sizeof(int) * 2 * kS);
+  unsigned char* chg = take(sizeof(int) * (1 + 4 * kS));
+  if (L) {
+    L->sm = reinterpret_cast<double*>(sm);
+    L->slots = reinterpret_cast<Slot*>(slots);
+    L->kslot = reinterpret_cast<Slot*>(kslot);
+    L->stage = reinterpret_cast<Slot*>(stage);
+    L->psave = reinterpret_cast<double*>(psave);
+    L->tmp = reinterpret_cast<double*>(tmp);
+    L->orig = reinterpret_cast<int*>(orig);
+    L->plist = reinterpret_cast<int*>(plist);
+    L->chg = reinterpret_cast<int*>(chg);
+  }
+  return off;
+}
+
+}  // namespace
+
+template <int RPT>
+__global__ void __launch_bounds__(kT, 1) panel_reg_kernel(PanelParams p) {
+  // Every CTA reads the same word before any barrier or state write (a stop
+  // is recorded only by an earlier kernel), so all of them leave together.
+  if (p.gated && p.state->stop_k >= 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cg::cluster_group cluster = cg::this_cluster();
+  const int C = (int)cluster.num_blocks();
+  const int rank = (int)cluster.block_rank();
+  const int w = p.end - p.begin;
+  const int W1 = w + 1;
+  const int R = p.rows_per_cta;
+  const int RP = R | 1;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long long row0 = (long long)p.begin + (long long)rank * R;
+  const int rows_here = (int)max(0LL, min((long long)R, (long long)p.m - row0));
+  Layout S;
+  reg_layout(smem_raw, w, R, &S);
+  double* const sm = S.sm;
+  int* const orig = S.orig;
+
+  // the slice arrives by asynchronous copies, all in flight at once
+  for (int c = 0; c < w; ++c) {
+    const double* src = p.a + idx(row0, p.begin + c, p.lda);
+    for (int r = tid; r < rows_here; r += kT) panel::cp_async8(sm + c * RP + r, src + r);
+  }
+  for (int r = tid; r < rows_here; r += kT) orig[r] = (int)(row0 + r);
+  panel::cp_async_wait_all();
+  if (rank == 0 && tid == 0) {
+    p.state->stop_k = -1;
+    p.state->swap_count = 0;
+    p.state->block_changed = 0;
+  }
+  __syncthreads();
+
+  // candidate of column 0
+  LocalBest mine{0.0, -1, 0, 0.0};
+#pragma unroll
+  for (int i = 0; i < RPT; ++i) {
+    const int r = tid + i * kT;
+    if (r < rows_here) offer(mine, fabs(sm[r]), r);
+  }
+
+  bool stopped = false;
+  for (int base = 0; base < w && !stopped; base += kS) {
+    const int send = min(base + kS, w);
+    double x[RPT][kS];  // this thread's rows over the sub-panel's columns
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+      const int r = tid + i * kT;
+#pragma unroll
+      for (int t = 0; t < kS; ++t)
+        x[i][t] = (r < rows_here && base + t < w) ? sm[(base + t) * RP + r] : 0.0;
+    }
+    int kd = send - base;  // steps executed in this sub-panel
+
+#pragma unroll
+    for (int j = 0; j < kS; ++j) {
+      if (base + j >= w) break;
+      const int s = base + j;
+      const long long k = (long long)p.begin + s;
+      const int par = s & 1;
+      const bool positioned = (s == 0) && p.positioned;
+      const int kl = (int)(k - row0);
+      const bool own_k = kl >= 0 && kl < rows_here;
+
+      // 1. this CTA's candidate: per-warp winners staged with their slices
+      if (positioned) {
+        mine = LocalBest{0.0, -1, 0, 0.0};
+        if (own_k && tid == kl % kT) mine = LocalBest{__longlong_as_double(0x7ff0000000000000ll), kl, 0, 0.0};
+      }
+      const LocalBest wb = warp_lb(mine);
+      if (wb.row >= 0 && tid == wb.row % kT) {
+        Slot& st = S.stage[warp];
+        const int wi = wb.row / kT;
+#pragma unroll
+        for (int i = 0; i < RPT; ++i)
+          if (i == wi) {
+#pragma unroll
+            for (int t = 0; t < kS; ++t) st.v[t] = x[i][t];
+            st.inv = 1.0 / x[i][j];
+          }
+        st.val = wb.val;
+        st.sec = wb.sec;
+        st.row = (int)(row0 + wb.row);
+        st.orig = orig[wb.row];
+      } else if (wb.row < 0 && lane == 0) {
+        Slot& st = S.stage[warp];
+        st.val = 0.0;
+        st.sec = wb.sec;
+        st.inv = 0.0;
+        st.row = -1;
+        st.orig = -1;
+      }
+      if (own_k && tid == kl % kT) {
+        Slot& st = S.stage[kW];
+        const int ki = kl / kT;
+#pragma unroll
+        for (int i = 0; i < RPT; ++i)
+          if (i == ki) {
+#pragma unroll
+            for (int t = 0; t < kS; ++t) st.v[t] = x[i][t];
+          }
+        st.orig = orig[kl];
+        st.row = (int)k;
+      }
+      __syncthreads();
+      // 2. the CTA's winner among the warps, pushed to every CTA
+      {
+        const Slot* cs = S.stage + (lane & (kW - 1));
+        const bool have = lane < kW && cs->row >= 0;
+        double bv;
+        int brow;
+        warp_best(have ? cs->val : 0.0, have ? cs->row : 0x7fffffff, bv, brow);
+        const double bsec = warp_max_pos(
+            lane < kW ? ((have && cs->row == brow) ? cs->sec : (have ? cs->val : cs->sec)) : 0.0);
+        const int wsel = __ffs(__ballot_sync(0xffffffffu, have && cs->row == brow)) - 1;
+        if (warp == 0 && lane < C) {
+          Slot* dst = cluster.map_shared_rank(S.slots + par * kMaxC + rank, lane);
+          if (wsel >= 0) {
+            copy_slot(dst, S.stage + wsel);
+            dst->sec = bsec;
+          } else {
+            dst->val = 0.0;
+            dst->sec = bsec;
+            dst->inv = 0.0;
+            dst->row = -1;
+            dst->orig = -1;
+          }
+        }
+        if (warp == 1 && own_k && lane < C)
+          copy_slot(cluster.map_shared_rank(S.kslot + par, lane), S.stage + kW);
+      }
+      cluster.sync();
+
+      // 3. same decision everywhere
+      int wslot = -1;
+      double wval = 0.0, wsec = 0.0;
+      {
+        const Slot* cs = S.slots + par * kMaxC + (lane < C ? lane : 0);
+        const bool have = lane < C && cs->row >= 0;
+        double bv;
+        int brow;
+        warp_best(have ? cs->val : 0.0, have ? cs->row : 0x7fffffff, bv, brow);
+        wsec = warp_max_pos(lane < C ? ((have && cs->row == brow) ? cs->sec
+                                                                 : (have ? cs->val : cs->sec))
+                                     : 0.0);
+        if (brow != 0x7fffffff) {
+          wslot = __ffs(__ballot_sync(0xffffffffu, have && cs->row == brow)) - 1;
+          wval = bv;
+        }
+      }
+      if (rank == 0 && tid == 0 && !positioned) note_decision(p.state, k, wval, wsec);
+      const bool stop = !positioned && !(wslot >= 0 && wval > p.threshold);
+      if (stop) {
+        if (rank == 0 && tid == 0) p.state->stop_k = (int)k;
+        kd = j;
+        stopped = true;
+        break;
+      }
+      const Slot& ws = S.slots[par * kMaxC + wslot];
+      const long long prow = ws.row;
+      if (rank == 0 && tid == 0 && !positioned) p.ipiv[k] = (int)prow;
+      if (tid == 0) {
+        S.plist[2 * j] = (int)k;
+        S.plist[2 * j + 1] = (int)prow;
+      }
+      if (tid < kS && base + tid < w) S.psave[j * W1 + base + tid] = ws.v[tid];
+      double pv[kS];
+#pragma unroll
+      for (int t = 0; t < kS; ++t) pv[t] = ws.v[t];
+      const double inv = ws.inv;
+
+      // 4. swap: row k takes the pivot row, the pivot row's place row k
+      const int pl = (int)(prow - row0);
+      const bool swap_p = pl >= 0 && pl < rows_here && prow != k;
+      if (own_k && tid == kl % kT) {
+        const int ki = kl / kT;
+#pragma unroll
+        for (int i = 0; i < RPT; ++i)
+          if (i == ki) {
+#pragma unroll
+            for (int t = 0; t < kS; ++t) x[i][t] = pv[t];
+          }
+        orig[kl] = ws.orig;
+      }
+      if (swap_p && tid == pl % kT) {
+        const Slot& kr = S.kslot[par];
+        const int pi = pl / kT;
+#pragma unroll
+        for (int i = 0; i < RPT; ++i)
+          if (i == pi) {
+#pragma unroll
+            for (int t = 0; t < kS; ++t) x[i][t] = kr.v[t];
+          }
+        orig[pl] = kr.orig;
+      }
+
+      // 5. scale and update the rows below k; next column's candidate
+      mine = LocalBest{0.0, -1, 0, 0.0};
+#pragma unroll
+      for (int i = 0; i < RPT; ++i) {
+        const int r = tid + i * kT;
+        if (r >= rows_here || row0 + r <= k) continue;
+        const double l = x[i][j] * inv;
+        x[i][j] = l;
+#pragma unroll
+        for (int t = j + 1; t < kS; ++t) x[i][t] = fma(-l, pv[t], x[i][t]);
+        if (j + 1 < kS && s + 1 < send) offer(mine, fabs(x[i][j + 1 < kS ? j + 1 : 0]), r);
+      }
+    }
+
+    // ---- end of the sub-panel: kd steps executed at [base, base + kd) ----
+    if (kd == 0) break;  // stopped at its first step: nothing moved
+    // a. the register slices back to shared memory
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+      const int r = tid + i * kT;
+      if (r < rows_here) {
+#pragma unroll
+        for (int t = 0; t < kS; ++t)
+          if (base + t < w) sm[(base + t) * RP + r] = x[i][t];
+      }
+    }
+    // b. composite source map of the sub-panel's swaps (the same everywhere)
+    if (tid == 0) {
+      int pos[2 * kS], src[2 * kS], np = 0;
+      for (int t = 0; t < kd; ++t) {
+        const int a = S.plist[2 * t], b = S.plist[2 * t + 1];
+        if (a == b) continue;
+        int ia = -1, ib = -1;
+        for (int q = 0; q < np; ++q) {
+          if (pos[q] == a) ia = q;
+          if (pos[q] == b) ib = q;
+        }
+        if (ia < 0) {
+          ia = np++;
+          pos[ia] = a;
+          src[ia] = a;
+        }
+        if (ib < 0) {
+          ib = np++;
+          pos[ib] = b;
+          src[ib] = b;
+        }
+        const int tmp = src[ia];
+        src[ia] = src[ib];
+        src[ib] = tmp;
+      }
+      int nc = 0;
+      for (int q = 0; q < np; ++q)
+        if (pos[q] != src[q]) {
+          S.chg[1 + 2 * nc] = pos[q];
+          S.chg[2 + 2 * nc] = src[q];
+          ++nc;
+        }
+      S.chg[0] = nc;
+    }
+    __syncthreads();
+    const int nchg = S.chg[0];
+    // source of global row g after the sub-panel's swaps
+    auto source_of = [&](int g) {
+      for (int q = 0; q < nchg; ++q)
+        if (S.chg[1 + 2 * q] == g) return S.chg[2 + 2 * q];
+      return g;
+    };
+    const int ncol_out = base + (w - send);  // columns outside the sub-panel
+    auto out_col = [&](int c) { return c < base ? c : send + (c - base); };
+    // c. phase A: moved rows of this CTA (into tmp) and the pivot rows of
+    //    the sub-panel's far columns (into psave), read from their owners
+    int nmine = 0;  // moved rows of this CTA, in chg order
+    for (int q = 0; q < nchg; ++q) {
+      const long long g = S.chg[1 + 2 * q];
+      if (g >= row0 && g < row0 + rows_here) {
+        const int sg = S.chg[2 + 2 * q];
+        const int owner = (int)((sg - p.begin) / R), sl = (int)(sg - p.begin - (long long)owner * R);
+        const double* rsm = cluster.map_shared_rank(sm, owner);
+        for (int c = tid; c < ncol_out; c += kT)
+          S.tmp[nmine * W1 + c] = rsm[out_col(c) * RP + sl];
+        ++nmine;
+      }
+    }
+    if (send < w) {
+      for (int e = tid; e < kd * (w - send); e += kT) {
+        const int t = e / (w - send), c = send + (e - t * (w - send));
+        const int sg = source_of(S.plist[2 * t]);
+        const int owner = (int)((sg - p.begin) / R), sl = (int)(sg - p.begin - (long long)owner * R);
+        S.psave[t * W1 + c] = cluster.map_shared_rank(sm, owner)[c * RP + sl];
+      }
+    }
+    cluster.sync();  // every CTA has read what it needs before anyone overwrites
+    // d. phase B: moved rows take their sources' content
+    nmine = 0;
+    for (int q = 0; q < nchg; ++q) {
+      const long long g = S.chg[1 + 2 * q];
+      if (g >= row0 && g < row0 + rows_here) {
+        const int gl = (int)(g - row0);
+        for (int c = tid; c < ncol_out; c += kT) sm[out_col(c) * RP + gl] = S.tmp[nmine * W1 + c];
+        ++nmine;
+      }
+    }
+    if (send >= w) break;  // no columns right of the sub-panel
+    __syncthreads();       // psave and the moved rows complete
+    // e. U12 = L11^{-1} A12 of the sub-panel, one column per thread
+    for (int c = send + tid; c < w; c += kT) {
+      double u[kS];
+#pragma unroll
+      for (int q = 0; q < kS; ++q) u[q] = q < kd ? S.psave[q * W1 + c] : 0.0;
+#pragma unroll
+      for (int q = 1; q < kS; ++q) {
+        if (q < kd) {
+#pragma unroll
+          for (int t = 0; t < q; ++t) u[q] = fma(-S.psave[q * W1 + base + t], u[t], u[q]);
+          S.psave[q * W1 + c] = u[q];
+        }
+      }
+    }
+    __syncthreads();
+    const long long first = (long long)p.begin + base;  // global row of the first pivot
+    const int ncol = w - send;
+    // the solved rows to the pivot rows of this CTA
+    for (int e = tid; e < kd * ncol; e += kT) {
+      const int q = e / ncol, c = send + (e - q * ncol);
+      const long long g = first + q;
+      if (g >= row0 && g < row0 + rows_here) sm[c * RP + (int)(g - row0)] = S.psave[q * W1 + c];
+    }
+    // f. rank-kd update of the rows below the sub-panel's pivots; the next
+    //    sub-panel's first candidate
+    mine = LocalBest{0.0, -1, 0, 0.0};
+    const double* __restrict__ ps = S.psave;
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+      const int r = tid + i * kT;
+      if (r >= rows_here || row0 + r < first + kd) continue;
+      double* __restrict__ row = sm + r;
+      double l[kS];
+#pragma unroll
+      for (int t = 0; t < kS; ++t) l[t] = t < kd ? row[(base + t) * RP] : 0.0;
+      {
+        double xs = row[send * RP];
+#pragma unroll
+        for (int t = 0; t < kS; ++t)
+          if (t < kd) xs = fma(-l[t], ps[t * W1 + send], xs);
+        row[send * RP] = xs;
+        offer(mine, fabs(xs), r);
+      }
+#pragma unroll 4
+      for (int c = send + 1; c < w; ++c) {
+        double xc = row[c * RP];
+#pragma unroll
+        for (int t = 0; t < kS; ++t)
+          if (t < kd) xc = fma(-l[t], ps[t * W1 + c], xc);
+        row[c * RP] = xc;
+      }
+    }
+    __syncthreads();  // the next sub-panel's columns are final in shared memory
+  }
+  // No CTA may exit while a peer could still read its shared memory, and
+  // rows were written by other threads than those writing them back.
+  cluster.sync();
+
+#pragma unroll 4
+  for (int c = 0; c < w; ++c) {
+    double* dst = p.a + idx(row0, p.begin + c, p.lda);
+    for (int r = tid; r < rows_here; r += kT) dst[r] = sm[c * RP + r];
+  }
+  // Swap lists: whole warps walk the rows together, so that the moved rows
+  // below the block take their slots with one atomic per warp.
+  int changed = 0;
+  for (int r0w = warp * 32; r0w < rows_here; r0w += kT) {
+    const int r = r0w + lane;
+    const long long g = row0 + r;
+    const int src = r < rows_here ? orig[r] : (int)g;
+    if (r < rows_here && g < p.end) {
+      p.swap_block[g - p.begin] = src;
+      changed += src != (int)g;
+    }
+    const bool moved = r < rows_here && g >= p.end && src != (int)g;
+    const unsigned bal = __ballot_sync(0xffffffffu, moved);
+    if (bal) {
+      int slot = 0;
+      if (lane == 0) slot = atomicAdd(&p.state->swap_count, __popc(bal));
+      slot = __shfl_sync(0xffffffffu, slot, 0) + __popc(bal & ((1u << lane) - 1u));
+      if (moved) {
+        p.swap_extra[2 * slot + 0] = (int)g;
+        p.swap_extra[2 * slot + 1] = src;
+      }
+    }
+  }
+  changed = __reduce_add_sync(0xffffffffu, changed);
+  if (lane == 0 && changed) atomicAdd(&p.state->block_changed, changed);
+}
+
+size_t panel_reg_smem_bytes(int w, int rows_per_cta) {
+  return reg_layout(nullptr, w, rows_per_cta, nullptr);
+}
+
+int panel_reg_max_rows() { return 4 * kT; }
+
+const void* panel_reg_kernel_for(int rows_per_cta) {
+  if (rows_per_cta <= kT) return (const void*)panel_reg_kernel<1>;
+  if (rows_per_cta <= 2 * kT) return (const void*)panel_reg_kernel<2>;
+  if (rows_per_cta <= 4 * kT) return (const void*)panel_reg_kernel<4>;
+  return nullptr;
+}
+
+}  // namespace dp

@@ -48,7 +48,9 @@ typedef struct dp_options {
                         DP_POLICY_NONZERO_COLUMN (delayed_getrf_column) */
   int panel_rows;    /* target rows per CTA in the panel kernel; 0 = automatic */
   int nb_outer;      /* outer block width of the trailing update; 0 = automatic */
-  int panel_kernel;  /* 0 automatic (cluster panel when it fits), 1 cluster, 2 grid-wide */
+  int panel_kernel;  /* 0 automatic (single-CTA panel up to 512 rows, else the cluster
+                        panel), 1 cluster (sub-panel in registers up to 1024 rows per
+                        CTA), 2 grid-wide, 3 cluster with the sub-panel in shared memory */
   int precision;     /* DP_PRECISION_FP64 (reference arithmetic) or
                         DP_PRECISION_MIXED_BF16X3 (tensor-core trailing update) */
   int lookahead;     /* 0 automatic (on beyond one outer block), 1 on, 2 off: the

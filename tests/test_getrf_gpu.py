@@ -443,3 +443,27 @@ def test_autotuned_widths_keep_the_records(built, tmp_path):
     empty = tmp_path / "empty.txt"
     empty.write_text("")
     assert dp.getrf_tune_load(empty) == 0
+
+
+@pytest.mark.parametrize("name", ["config1_n1024", "config1_n1024_column", "square_2000_zero20",
+                                  "square_2000_zero20_column", "ref_far_pivot_70",
+                                  "square_517_lda520", "tall_300x200", "wide_150x260"])
+@pytest.mark.parametrize("kernel,rows,nb", [(1, 256, 64), (1, 512, 64), (1, 1024, 64),
+                                            (1, 64, 13), (1, 700, 100), (3, 256, 64)])
+def test_cluster_panels_keep_the_records(built, name, kernel, rows, nb):
+    """Every panel of the factorisation on a cluster kernel: the register
+    sub-panel one (panel_kernel 1) with 1, 2 and 4 rows per thread (rows per
+    CTA up to 256, 512, 1024), odd widths and partial sub-panels, and the
+    shared-memory one (panel_kernel 3): records equal the reference's, no
+    order-sensitive decision, residual within the bound."""
+    import oracle as orc
+
+    a, case = gc.load(name)
+    m, n = case["m"], case["n"]
+    fac, ipiv, jpiv, info, st = run_device(a, m, n, nb=nb, panel_kernel=kernel, panel_rows=rows,
+                                           policy=case["policy"])
+    assert st == 0 and info == case["info"]
+    np.testing.assert_array_equal(ipiv, case["ipiv"])
+    np.testing.assert_array_equal(jpiv, case["jpiv"])
+    assert_no_near_ties(info)
+    assert orc.scaled_residual(a, fac, m, n, info, ipiv, jpiv) <= 10.0
