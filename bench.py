@@ -503,6 +503,7 @@ def run_lu(args):
             "step_ms": [round(e0.elapsed_time(e1), 3) for e0, e1, _ in events],
             "clocks": clk.summary(),
             "kernels": kern,
+            "reference_gpu": reference_cuda_figures(n) if args.precision == "fp64" else None,
             "fp64_peak_tflops": fp64,
             "frac_of_fp64_peak": value / world / 1e3 / fp64,
             "hbm_peak_gbs": peaks.get("hbm_gbs"),
@@ -917,6 +918,7 @@ def lu_key(torch, dp, dev, L, n=16384, warmup=2, steps=3):
            "autotuned_widths": {"nb": tnb, "nb_outer": tnbo}, "near_tie_report": report,
            "fp64_peak_tflops_cublas_dgemm": fp64, "frac_of_fp64_peak": gf / 1e3 / fp64,
            "target_frac": 0.70, "kernels_one_step": kern,
+           "reference_gpu": reference_cuda_figures(n),
            "panel_roofline": _family_roofline(stats, 0, measured_peaks())}
     if gold.exists():
         with np.load(gold) as z:

@@ -141,16 +141,43 @@ constexpr double kNearTieC = 4.0;
 
 // Records one pivot decision of step k with winner magnitude `best` and
 // runner-up `second` (both >= 0; NaN never reaches here).  Called by one
-// thread per decision.
+// thread per decision, inside the panels' per-column critical path: only
+// reduction atomics whose results are unused, so the thread issues them and
+// goes on without waiting for a round trip to memory.
 __device__ __forceinline__ void note_decision(State* st, long long k, double best, double second) {
-  st->ties_checked += 1;
+  atomicAdd(&st->ties_checked, 1ull);
   if (best > 0.0) {
-    const double ratio = second / best;
-    if (best - second <= kNearTieC * (double)(k + 1) * 0x1p-53 * best) st->near_ties += 1;
-    const unsigned long long bits = (unsigned long long)__double_as_longlong(ratio);
-    if (bits > st->closeness) st->closeness = bits;
+    if (best - second <= kNearTieC * (double)(k + 1) * 0x1p-53 * best)
+      atomicAdd(&st->near_ties, 1ull);
+    atomicMax(&st->closeness, (unsigned long long)__double_as_longlong(second / best));
   }
 }
+
+// The same record kept in registers by the one thread of a panel kernel that
+// records its decisions, and flushed to the state once, when it finishes:
+// the per-column critical path then carries no memory operation for it.
+// The largest ratio second / best is kept as its (second, best) pair,
+// compared by cross products, so that the one division happens at the flush.
+struct DecisionTally {
+  unsigned long long checked = 0, near = 0;
+  double c_sec = 0.0, c_best = 1.0;  // pair of the largest ratio so far
+  __device__ __forceinline__ void note(long long k, double best, double second) {
+    ++checked;
+    if (best > 0.0) {
+      if (best - second <= kNearTieC * (double)(k + 1) * 0x1p-53 * best) ++near;
+      if (second * c_best > c_sec * best) {
+        c_sec = second;
+        c_best = best;
+      }
+    }
+  }
+  __device__ __forceinline__ void flush(State* st) const {
+    if (checked) atomicAdd(&st->ties_checked, checked);
+    if (near) atomicAdd(&st->near_ties, near);
+    if (c_sec > 0.0)
+      atomicMax(&st->closeness, (unsigned long long)__double_as_longlong(c_sec / c_best));
+  }
+};
 
 // Bounded wait: every spin in this library gives up after kSpinLimitNs of
 // wall time, records kDeviceTimeout in the state and lets the caller return.

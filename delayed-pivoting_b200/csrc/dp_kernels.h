@@ -89,6 +89,14 @@ int launch_laswp_seq(double* a, long long lda, const int* blk, const int* ext, i
 int trsm_max_width();
 void launch_trsm_unit_lower(double* a, long long lda, int r0, int w, int c0, int nc,
                             cudaStream_t s, const int* gate = nullptr);
+// T (w x w, column stride ldt) <- I - L^{-1} for the unit lower w x w block L,
+// w <= lower_inverse_max_width(): the solve L^{-1} B is then B - T B, a GEMM.
+int lower_inverse_max_width();
+void launch_lower_inverse(const double* L, long long ldl, int w, double* T, long long ldt,
+                          cudaStream_t s);
+// dst <- src for a rows x cols column-major block (device memory).
+void launch_copy_block(const double* src, long long lds, double* dst, long long ldd, int rows,
+                       int cols, cudaStream_t s);
 // Same with separate operands; and B <- U^{-1} B for upper U with diagonal.
 void launch_trsm_lower_unit(const double* L, long long ldl, double* B, long long ldb, int w, int nc,
                             cudaStream_t s, const int* gate = nullptr);

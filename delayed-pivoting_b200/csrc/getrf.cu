@@ -137,15 +137,36 @@ struct Workspace {
   int* defer_ext = nullptr;
   int defer_cap = 0;
   int* aux_status = nullptr;
+  // Block solves of the outer blocks as GEMMs: T = I - L11^{-1} of an outer
+  // block (two, alternating between consecutive blocks like the deferred swap
+  // lists; tinv_ld x tinv_ld each) and copies of the block rows being solved
+  // (tcopy1: the panel stream's, up to copy1_cols columns; tcopy2: the
+  // trailing stream's or the only stream's, up to copy2_cols columns).
+  // Absent (tinv == nullptr) in the allocation-free workspace.
+  double* tinv = nullptr;
+  double* tcopy1 = nullptr;
+  double* tcopy2 = nullptr;
+  int tinv_ld = 0;
+  char* scratch = nullptr;  // from here on, every region is written before it is read
   int max_ctas = 0;
   int w_max = 0;
+};
+
+// dp_block_solve: 0 automatic (inverse), 1 inverse, 2 substitution.
+std::atomic<int> g_block_solve{0};
+
+// Geometry of the block solves by inverse (Workspace::tinv).
+struct InvPlan {
+  int ld = 0;              // 0: no block solves by inverse
+  long long copy1_cols = 0, copy2_cols = 0;
 };
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 // Lays the workspace out from `base` (nullptr: only computes the size).
 size_t layout_workspace(Workspace& ws, char* base, int pivots, int max_ctas, int w_max,
-                        size_t mixed_bytes, int defer_cap = 0, size_t mixed1_bytes = 0) {
+                        size_t mixed_bytes, int defer_cap = 0, size_t mixed1_bytes = 0,
+                        const InvPlan& inv = InvPlan{}) {
   size_t off = 0;
   auto take = [&](size_t bytes) {
     const size_t at = off;
@@ -170,8 +191,18 @@ size_t layout_workspace(Workspace& ws, char* base, int pivots, int max_ctas, int
     ws.defer_ext = reinterpret_cast<int*>(take(sizeof(int) * 4 * (size_t)defer_cap));
     ws.aux_status = reinterpret_cast<int*>(take(sizeof(int)));
   }
+  ws.scratch = base ? base + off : nullptr;
   ws.mixed = mixed_bytes ? reinterpret_cast<void*>(take(mixed_bytes)) : nullptr;
   ws.mixed1 = mixed1_bytes ? reinterpret_cast<void*>(take(mixed1_bytes)) : nullptr;
+  ws.tinv_ld = inv.ld;
+  if (inv.ld > 0) {
+    const size_t ld = (size_t)inv.ld;
+    ws.tinv = reinterpret_cast<double*>(take(sizeof(double) * 2 * ld * ld));
+    ws.tcopy1 = inv.copy1_cols > 0
+                    ? reinterpret_cast<double*>(take(sizeof(double) * ld * (size_t)inv.copy1_cols))
+                    : nullptr;
+    ws.tcopy2 = reinterpret_cast<double*>(take(sizeof(double) * ld * (size_t)inv.copy2_cols));
+  }
   ws.base = base;
   ws.bytes = off;
   return off;
@@ -428,12 +459,29 @@ void trsm_blocked(double* a, long long lda, int r0, int W, int c0, int nc, cudaS
 // When `mixed_ws` is set the rank-W update runs on the tensor cores (BF16
 // split into `terms` pieces, FP32 accumulation); the TRSM always runs in FP64.
 // A non-null `gate` (FP64 only) makes the kernels do nothing once *gate >= 0.
+// A non-null `bi` holding T = I - L^{-1} of the W x W block at a(s0, s0)
+// solves blocks wider than trsm_max_width() as U = B - T C, C a copy of B
+// (one copy and one GEMM instead of the chain of 64-row solves and updates).
+struct BlockInv {
+  const double* T = nullptr;
+  long long ldt = 0;
+  double* copy = nullptr;  // ldt x (columns) doubles
+};
+
 int update_columns(double* a, long long lda, int m, int s0, int W, int r_gemm, int c0, int n_end,
                    cudaStream_t st, Recorder& rec, void* mixed_ws = nullptr,
-                   int* status = nullptr, int terms = 2, const int* gate = nullptr) {
+                   int* status = nullptr, int terms = 2, const int* gate = nullptr,
+                   const BlockInv* bi = nullptr) {
   const int nc = n_end - c0;
   if (W <= 0 || nc <= 0) return kOk;
-  trsm_blocked(a, lda, s0, W, c0, nc, st, rec, gate);
+  if (bi && bi->T && W > trsm_max_width() && W <= bi->ldt) {
+    rec.begin(DP_KFAM_TRSM);
+    launch_copy_block(a + idx(s0, c0, lda), lda, bi->copy, W, W, nc, st);
+    launch_gemm_minus(W, nc, W, bi->T, bi->ldt, bi->copy, W, a + idx(s0, c0, lda), lda, st, gate);
+    rec.end(2.0 * W * (double)W * nc, 8.0 * ((double)W * W + 4.0 * W * (double)nc), 2);
+  } else {
+    trsm_blocked(a, lda, s0, W, c0, nc, st, rec, gate);
+  }
   const int M = m - r_gemm;
   if (M <= 0) return kOk;
   const double fl = 2.0 * M * (double)nc * W;
@@ -458,26 +506,32 @@ int update_columns(double* a, long long lda, int m, int s0, int W, int r_gemm, i
 // in-block updates, the next outer block's columns - and `trail` (lowest
 // priority) the bulk of each trailing update, so that panel CTAs are placed
 // ahead of waiting GEMM tiles.
+// `left` (lowest priority) carries the row swaps of the finished L columns
+// left of each outer block, which nothing reads until the factorisation
+// ends, beside the trailing update instead of in front of it.
 struct Lanes {
-  cudaStream_t panel = nullptr, trail = nullptr;
-  cudaEvent_t fork = nullptr, block = nullptr, next = nullptr, join = nullptr;
+  cudaStream_t panel = nullptr, trail = nullptr, left = nullptr;
+  cudaEvent_t fork = nullptr, block = nullptr, next = nullptr, join = nullptr, ldone = nullptr,
+              tdone = nullptr;
   bool ready = false;
   bool init() {
     int least = 0, greatest = 0;
     if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
         cudaStreamCreateWithPriority(&panel, cudaStreamNonBlocking, greatest) != cudaSuccess ||
-        cudaStreamCreateWithPriority(&trail, cudaStreamNonBlocking, least) != cudaSuccess)
+        cudaStreamCreateWithPriority(&trail, cudaStreamNonBlocking, least) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&left, cudaStreamNonBlocking, least) != cudaSuccess)
       return false;
-    for (cudaEvent_t* e : {&fork, &block, &next, &join})
+    for (cudaEvent_t* e : {&fork, &block, &next, &join, &ldone, &tdone})
       if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) return false;
     ready = true;
     return true;
   }
   ~Lanes() {
-    for (cudaEvent_t e : {fork, block, next, join})
+    for (cudaEvent_t e : {fork, block, next, join, ldone, tdone})
       if (e) cudaEventDestroy(e);
     if (panel) cudaStreamDestroy(panel);
     if (trail) cudaStreamDestroy(trail);
+    if (left) cudaStreamDestroy(left);
   }
 };
 thread_local Lanes g_lanes[64];
@@ -497,12 +551,16 @@ Lanes* lanes_for_device() {
 // trailing updates right of the next outer block, ordered against `s1` by
 // the events `block` (s1 -> s2: an outer block and the next block's columns
 // are done) and `next` (s2 -> s1: the columns of the block after next have
-// this block's update).
+// this block's update).  `s3` takes the swaps of the columns left of each
+// block, after `block` and after `tdone` (s2 -> s3: the previous block's
+// trailing update, the last reader of its L columns, is done); `ldone`
+// (s3 -> s1) marks them applied.
 struct Schedule {
-  cudaStream_t s1 = nullptr, s2 = nullptr;
+  cudaStream_t s1 = nullptr, s2 = nullptr, s3 = nullptr;
   Recorder* r1 = nullptr;
   Recorder* r2 = nullptr;
-  cudaEvent_t block = nullptr, next = nullptr;
+  Recorder* r3 = nullptr;
+  cudaEvent_t block = nullptr, next = nullptr, ldone = nullptr, tdone = nullptr;
 };
 
 // Applies the deferred swap lists of the panels [B, B + sum widths) of an
@@ -574,6 +632,20 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
   int* const stop_word = &ws.state->stop_k;
   std::vector<int> widths;  // the current block's panels (look-ahead)
   if (la) DP_CHECK_CUDA(cudaMemsetAsync(stop_word, 0xFF, sizeof(int), st));  // stop_k = -1
+  // T = I - L^{-1} of the W x W block at a(s0, s0) into buffer `which`, when
+  // the block is solved by inverse (wider than the TRSM kernel's blocks);
+  // returns the solve's operands for the panel stream and the other stream
+  auto block_inverse = [&](int s0, int W, int which, BlockInv& on1, BlockInv& on2) {
+    on1 = on2 = BlockInv{};
+    if (!ws.tinv || W <= trsm_max_width() || W > ws.tinv_ld) return;
+    double* T = ws.tinv + (size_t)which * ws.tinv_ld * ws.tinv_ld;
+    rec.begin(DP_KFAM_TRSM);
+    launch_lower_inverse(a + idx(s0, s0, lda), lda, W, T, ws.tinv_ld, st);
+    rec.end((double)W * W * W / 3.0, 8.0 * (0.5 * (double)W * W + (double)W * W), 1);
+    on1 = BlockInv{T, ws.tinv_ld, ws.tcopy1 ? ws.tcopy1 : ws.tcopy2};
+    on2 = BlockInv{T, ws.tinv_ld, ws.tcopy2};
+  };
+  BlockInv inv1, inv2;
   while (B < pivots) {
     const int E = std::min(pivots, B + NB);
     int* blk = la ? ws.defer_blk + (size_t)half * ws.defer_cap : ws.swap_block;
@@ -722,8 +794,10 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
     }
     if (stop < 0 && !la) {
       // right of the outer block: the O(n^3) update
+      inv1 = inv2 = BlockInv{};
+      if (E < n) block_inverse(B, E - B, 0, inv1, inv2);
       if (int err = update_columns(a, lda, m, B, E - B, E, E, n, st, rec, mixed_ws,
-                                   &ws.state->status, terms))
+                                   &ws.state->status, terms, nullptr, &inv2))
         return err;
       DP_CHECK_CUDA(cudaGetLastError());
       B = E;
@@ -734,28 +808,52 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       const int NNE = std::min(pivots, NE + NB);  // the block after next
       // s1: the next block's columns, then on to its panels
       if (pending) DP_CHECK_CUDA(cudaStreamWaitEvent(st, sc.next, 0));
+      // the left swaps of the previous block have read their lists, whose
+      // buffer the next block's panels reuse
+      DP_CHECK_CUDA(cudaStreamWaitEvent(st, sc.ldone, 0));
+      inv1 = inv2 = BlockInv{};
+      if (E < n) {
+        // T of this block goes to the buffer of two blocks ago, whose last
+        // reader is that block's update on the trailing stream: the wait
+        // above follows it; without one, wait for the trailing stream here
+        if (!pending) {
+          DP_CHECK_CUDA(cudaEventRecord(sc.next, sc.s2));
+          DP_CHECK_CUDA(cudaStreamWaitEvent(st, sc.next, 0));
+        }
+        block_inverse(B, E - B, half, inv1, inv2);
+      }
       if (int err = apply_deferred(a, lda, blk, ext, B, widths, E, NE, NE, NE, st, rec))
         return err;
       // (mixed precision: its own BF16 scratch, the trailing stream uses ws.mixed)
       if (int err = update_columns(a, lda, m, B, E - B, E, E, NE, st, rec,
-                                   terms ? ws.mixed1 : nullptr, &ws.state->status, terms))
+                                   terms ? ws.mixed1 : nullptr, &ws.state->status, terms, nullptr,
+                                   &inv1))
         return err;
       DP_CHECK_CUDA(cudaGetLastError());
       DP_CHECK_CUDA(cudaEventRecord(sc.block, st));
+      // (s2's work so far ends with the previous block's trailing update)
+      DP_CHECK_CUDA(cudaEventRecord(sc.tdone, sc.s2));
       // s2: everything else, behind the block
       DP_CHECK_CUDA(cudaStreamWaitEvent(sc.s2, sc.block, 0));
-      if (int err = apply_deferred(a, lda, blk, ext, B, widths, 0, B, NE, n, sc.s2, *sc.r2))
+      if (int err = apply_deferred(a, lda, blk, ext, B, widths, NE, n, n, n, sc.s2, *sc.r2))
         return err;
+      // s3: the block's swaps on the finished columns left of it, once the
+      // previous block's trailing update has read its L columns
+      DP_CHECK_CUDA(cudaStreamWaitEvent(sc.s3, sc.block, 0));
+      DP_CHECK_CUDA(cudaStreamWaitEvent(sc.s3, sc.tdone, 0));
+      if (int err = apply_deferred(a, lda, blk, ext, B, widths, 0, B, B, B, sc.s3, *sc.r3))
+        return err;
+      DP_CHECK_CUDA(cudaEventRecord(sc.ldone, sc.s3));
       pending = false;
       if (NNE > NE) {
         if (int err = update_columns(a, lda, m, B, E - B, E, NE, NNE, sc.s2, *sc.r2, mixed_ws,
-                                     ws.aux_status, terms))
+                                     ws.aux_status, terms, nullptr, &inv2))
           return err;
         DP_CHECK_CUDA(cudaEventRecord(sc.next, sc.s2));
         pending = true;
       }
       if (int err = update_columns(a, lda, m, B, E - B, E, std::max(NE, NNE), n, sc.s2, *sc.r2,
-                                   mixed_ws, ws.aux_status, terms))
+                                   mixed_ws, ws.aux_status, terms, nullptr, &inv2))
         return err;
       DP_CHECK_CUDA(cudaGetLastError());
       half ^= 1;
@@ -766,15 +864,21 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
     // Stopped at k inside panel [b, e): materialize, then search.
     const int k = stop;
     if (la) {
-      // s2 drains; the block's kept swaps reach every column outside it
+      // s2 and s3 drain; the block's kept swaps reach every column outside it
       DP_CHECK_CUDA(cudaEventRecord(sc.next, sc.s2));
       DP_CHECK_CUDA(cudaStreamWaitEvent(st, sc.next, 0));
+      DP_CHECK_CUDA(cudaEventRecord(sc.ldone, sc.s3));
+      DP_CHECK_CUDA(cudaStreamWaitEvent(st, sc.ldone, 0));
       pending = false;
       if (int err = apply_deferred(a, lda, blk, ext, B, widths, 0, B, E, n, st, rec)) return err;
     }
     update_columns(a, lda, m, b, k - b, k, e, E, st, rec);  // rest of the outer block
+    // (the trailing stream has drained: its buffers are free)
+    inv1 = inv2 = BlockInv{};
+    if (E < n) block_inverse(B, k - B, half, inv1, inv2);
     if (int err = update_columns(a, lda, m, B, k - B, k, E, n, st, rec, mixed_ws,
-                                 &ws.state->status, terms))  // right of the outer block
+                                 &ws.state->status, terms, nullptr,
+                                 &inv2))  // right of the outer block
       return err;
     rec.begin(DP_KFAM_SEARCH);
     if (o.policy == DP_POLICY_NONZERO_COLUMN)
@@ -907,18 +1011,25 @@ int getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* 
   const size_t mixed1_bytes =
       lanes && mixed_terms(o.precision) ? mixed_scratch_bytes(m, NB, NB, mixed_terms(o.precision))
                                         : 0;
-  const size_t bytes =
-      layout_workspace(ws, nullptr, pivots, di.sms, w_max, mixed_bytes, defer_cap, mixed1_bytes);
+  InvPlan ip;  // outer blocks wider than the TRSM kernel's are solved by inverse
+  if (g_block_solve.load() != 2 && NB > trsm_max_width() && NB <= lower_inverse_max_width() &&
+      n > NB) {
+    ip.ld = NB;
+    ip.copy1_cols = lanes ? NB : 0;
+    ip.copy2_cols = n;
+  }
+  const size_t bytes = layout_workspace(ws, nullptr, pivots, di.sms, w_max, mixed_bytes,
+                                        defer_cap, mixed1_bytes, ip);
   char* base = nullptr;
   if (cudaMallocAsync(reinterpret_cast<void**>(&base), bytes, st) != cudaSuccess) {
     cudaGetLastError();
     *info = -1;
     return kAllocationFailed;
   }
-  layout_workspace(ws, base, pivots, di.sms, w_max, mixed_bytes, defer_cap, mixed1_bytes);
+  layout_workspace(ws, base, pivots, di.sms, w_max, mixed_bytes, defer_cap, mixed1_bytes, ip);
   int status = kOk;
-  // the BF16 scratch (at the end) is fully written before use; clear the rest
-  const size_t clear = mixed_bytes ? (size_t)(static_cast<char*>(ws.mixed) - base) : bytes;
+  // the scratch regions (at the end) are fully written before use; clear the rest
+  const size_t clear = (size_t)(ws.scratch - base);
   if (cudaMemsetAsync(base, 0, clear, st) != cudaSuccess) status = kCudaFailure;
   int inf = pivots;
   HostTrace trace;
@@ -926,31 +1037,40 @@ int getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* 
   Schedule sc;
   sc.s1 = lanes ? lanes->panel : st;
   sc.s2 = lanes ? lanes->trail : nullptr;
-  Recorder rec(sc.s1), rec2(lanes ? lanes->trail : st);
+  sc.s3 = lanes ? lanes->left : nullptr;
+  Recorder rec(sc.s1), rec2(lanes ? lanes->trail : st), rec3(lanes ? lanes->left : st);
   sc.r1 = &rec;
   sc.r2 = &rec2;
+  sc.r3 = &rec3;
   rec2.lane = 1;
+  rec3.lane = 2;
   cudaEvent_t tl_base = nullptr;
   if (rec.on && timeline_path()) {
     tl_base = event_get();
     cudaEventRecord(tl_base, st);
-    rec.base = rec2.base = tl_base;
+    rec.base = rec2.base = rec3.base = tl_base;
   }
   if (lanes) {
     sc.block = lanes->block;
     sc.next = lanes->next;
+    sc.ldone = lanes->ldone;
+    sc.tdone = lanes->tdone;
     if (status == kOk && (cudaEventRecord(lanes->fork, st) != cudaSuccess ||
                           cudaStreamWaitEvent(lanes->panel, lanes->fork, 0) != cudaSuccess ||
-                          cudaStreamWaitEvent(lanes->trail, lanes->fork, 0) != cudaSuccess))
+                          cudaStreamWaitEvent(lanes->trail, lanes->fork, 0) != cudaSuccess ||
+                          cudaStreamWaitEvent(lanes->left, lanes->fork, 0) != cudaSuccess ||
+                          cudaEventRecord(lanes->ldone, lanes->left) != cudaSuccess))
       status = kCudaFailure;
   }
   if (status == kOk) status = factorize(m, n, d_a, lda, o, ws, di, sc, inf);
   int aux = kOk;
   if (lanes) {
-    // st waits for both lanes whatever happened, before the workspace is freed
+    // st waits for every lane whatever happened, before the workspace is freed
     cudaEventRecord(lanes->join, lanes->panel);
     cudaStreamWaitEvent(st, lanes->join, 0);
     cudaEventRecord(lanes->join, lanes->trail);
+    cudaStreamWaitEvent(st, lanes->join, 0);
+    cudaEventRecord(lanes->join, lanes->left);
     cudaStreamWaitEvent(st, lanes->join, 0);
     if (status == kOk &&
         cudaMemcpyAsync(&aux, ws.aux_status, sizeof(int), cudaMemcpyDeviceToHost, st) !=
@@ -971,6 +1091,7 @@ int getrf_device(int m, int n, double* d_a, int lda, int* ipiv, int* jpiv, int* 
   if (status == kOk && aux != kOk) status = aux;
   rec.flush(status == kOk);
   rec2.flush(status == kOk);
+  rec3.flush(status == kOk);
   if (tl_base) {
     std::lock_guard<std::mutex> lock(g_stats_mutex);
     ++g_timeline_calls;
@@ -1114,6 +1235,7 @@ int getrf_device_noalloc(int m, int n, double* d_a, int lda, int* ipiv, int* jpi
   sc.s1 = st;
   sc.r1 = &rec;
   sc.r2 = &rec;
+  sc.r3 = &rec;
   if (status == kOk) status = factorize(m, n, d_a, lda, o, ws, di, sc, inf);
   State fin{};
   if (status == kOk) {
@@ -1180,6 +1302,11 @@ int dp_getrf_hybrid_device(int m, int n, double* d_a, int lda, int* ipiv, int* j
 int dp_getrf_hybrid_host(int m, int n, double* a, int lda, int* ipiv, int* jpiv, int* info,
                          void* stream) {
   return dp_getrf_host(m, n, a, lda, ipiv, jpiv, info, stream);
+}
+
+int dp_block_solve(int mode) {
+  if (mode < 0 || mode > 2) return -1;
+  return dp::g_block_solve.exchange(mode);
 }
 
 int dp_getrf_last_report(dp_getrf_report* out) {

@@ -74,5 +74,71 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// ---- cluster exchange by transaction barriers ------------------------------
+// A CTA expects a known number of bytes per exchange on a barrier in its own
+// shared memory; its peers write them with st.async, each store completing
+// its bytes on that barrier, so a reader waits for the data alone (one-way
+// latency) instead of for every CTA of the cluster to reach a barrier.
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+// The address of the same shared-memory location in CTA `rank` of the cluster.
+__device__ __forceinline__ unsigned peer_addr(unsigned local, int rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void xbar_init(unsigned bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+}
+// Makes initialised barriers visible to the cluster's other CTAs.
+__device__ __forceinline__ void xbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// The one local arrival of a phase, announcing `bytes` to come.
+__device__ __forceinline__ void xbar_expect(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool xbar_test(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for the phase of parity `parity` to complete; false when
+// kSpinLimitNs passed first.
+__device__ __forceinline__ bool xbar_wait(unsigned bar, unsigned parity) {
+  if (xbar_test(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer_ns();
+  for (;;) {
+    for (int i = 0; i < 64; ++i)
+      if (xbar_test(bar, parity)) return true;
+    if (globaltimer_ns() - t0 > kSpinLimitNs) return false;
+  }
+}
+// 16 bytes to peer shared memory `peer` (a peer_addr), completing them on
+// the peer's barrier `peer_bar`.
+__device__ __forceinline__ void st_async16(unsigned peer, uint4 v, unsigned peer_bar) {
+  asm volatile(
+      "st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];"
+      ::"r"(peer), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w), "r"(peer_bar)
+      : "memory");
+}
+// The two halves of a cluster barrier: writes before arrive() are visible to
+// every CTA of the cluster after its wait().
+__device__ __forceinline__ void cluster_arrive() {
+  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() {
+  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
 }  // namespace panel
 }  // namespace dp

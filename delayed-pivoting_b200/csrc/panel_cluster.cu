@@ -168,6 +168,7 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
     }
   };
 
+  DecisionTally tally;  // rank 0, thread 0 records the decisions
   for (int s = 0; s < w; ++s) {
     const long long k = (long long)p.begin + s;
     const int par = s & 1;
@@ -245,7 +246,7 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
         win.inv = __shfl_sync(0xffffffffu, c.inv, max(src, 0));
       }
     }
-    if (rank == 0 && tid == 0 && !positioned) note_decision(p.state, k, win.val, win.sec);
+    if (rank == 0 && tid == 0 && !positioned) tally.note(k, win.val, win.sec);
     const bool stop = !positioned && !(win.row >= 0 && win.val > p.threshold);
     if (stop) {
       if (rank == 0 && tid == 0) p.state->stop_k = (int)k;
@@ -313,6 +314,7 @@ __global__ void __launch_bounds__(kThreads, 1) panel_cluster_kernel(PanelParams 
   // Rows were swapped and updated by other threads than those writing them
   // back, and no CTA may exit while a peer could still push into it.
   cluster.sync();
+  if (rank == 0 && tid == 0) tally.flush(p.state);
 
 #pragma unroll 4
   for (int c = 0; c < w; ++c) {

@@ -59,11 +59,21 @@ struct __align__(16) Slot {
   double v[kS];  // the row over the sub-panel's columns
 };
 
-__device__ __forceinline__ void copy_slot(Slot* dst, const Slot* src) {
-  const int4* s = reinterpret_cast<const int4*>(src);
-  int4* d = reinterpret_cast<int4*>(dst);
-#pragma unroll
-  for (int i = 0; i < (int)(sizeof(Slot) / sizeof(int4)); ++i) d[i] = s[i];
+constexpr int kSlotChunks = (int)(sizeof(Slot) / sizeof(uint4));
+static_assert(sizeof(Slot) % sizeof(uint4) == 0, "slots travel in 16-byte stores");
+
+// offer() that also keeps the signed entry of the best row, whose reciprocal
+// is then taken before the warp reduction instead of after it.
+__device__ __forceinline__ void offer_x(LocalBest& b, double& bx, double x, int r) {
+  const double v = fabs(x);
+  if (v > b.val) {
+    b.sec = b.val;
+    b.val = v;
+    b.row = r;
+    bx = x;
+  } else if (v > b.sec) {
+    b.sec = v;
+  }
 }
 
 struct Layout {
@@ -72,10 +82,11 @@ struct Layout {
   Slot* kslot;    // [2] row k, by step parity
   Slot* stage;    // [kW] per-warp candidates, then [1] row k
   double* psave;  // [kS][W1] the sub-panel's pivot rows
-  double* tmp;    // [2 kS][W1] pulled content of moved rows
+  double* tmp;    // [2 kS][W1] pulled content of moved rows (by map entry)
   int* orig;      // [R] source row of each local row
   int* plist;     // [kS][2] (k, pivot row) of the sub-panel's steps
   int* chg;       // [1 + 2 * 2 kS]: count, then (position, source) pairs
+  unsigned long long* xbar;  // [2] exchange barriers, by step parity
 };
 
 __host__ __device__ inline size_t reg_align16(size_t bytes) { return (bytes + 15) & ~(size_t)15; }
@@ -93,10 +104,11 @@ __host__ __device__ inline size_t reg_layout(unsigned char* base, int w, int R, 
   unsigned char* kslot = take(sizeof(Slot) * 2);
   unsigned char* stage = take(sizeof(Slot) * (kW + 1));
   unsigned char* psave = take(sizeof(double) * kS * w1);
-  unsigned char* tmp = take(sizeof(double) * 2 * kS * w1);
+  unsigned char* tmp = take(sizeof(double) * 2 * kS * w1);  // row q: map entry q
   unsigned char* orig = take(sizeof(int) * (size_t)R);
   unsigned char* plist = take(sizeof(int) * 2 * kS);
   unsigned char* chg = take(sizeof(int) * (1 + 4 * kS));
+  unsigned char* xbar = take(sizeof(unsigned long long) * 2);
   if (L) {
     L->sm = reinterpret_cast<double*>(sm);
     L->slots = reinterpret_cast<Slot*>(slots);
@@ -107,6 +119,7 @@ __host__ __device__ inline size_t reg_layout(unsigned char* base, int w, int R, 
     L->orig = reinterpret_cast<int*>(orig);
     L->plist = reinterpret_cast<int*>(plist);
     L->chg = reinterpret_cast<int*>(chg);
+    L->xbar = reinterpret_cast<unsigned long long*>(xbar);
   }
   return off;
 }
@@ -146,17 +159,28 @@ __global__ void __launch_bounds__(kT, 1) panel_reg_kernel(PanelParams p) {
     p.state->swap_count = 0;
     p.state->block_changed = 0;
   }
-  __syncthreads();
+  const unsigned xbar0 = panel::smem_addr(S.xbar);
+  if (tid == 0) {
+    panel::xbar_init(xbar0);
+    panel::xbar_init(xbar0 + 8);
+    panel::xbar_init_fence();
+  }
+  // every CTA's slice loaded and exchange barriers initialised before any
+  // peer reads the one or writes to the other
+  cluster.sync();
 
   // candidate of column 0
   LocalBest mine{0.0, -1, 0, 0.0};
+  double mine_x = 0.0;  // signed entry of the candidate
 #pragma unroll
   for (int i = 0; i < RPT; ++i) {
     const int r = tid + i * kT;
-    if (r < rows_here) offer(mine, fabs(sm[r]), r);
+    if (r < rows_here) offer_x(mine, mine_x, sm[r], r);
   }
 
-  bool stopped = false;
+  DecisionTally tally;  // rank 0, thread 0 records the decisions
+  bool stopped = false, timed_out = false;
+  bool pending = false;  // a cluster_arrive() awaits its cluster_wait()
   for (int base = 0; base < w && !stopped; base += kS) {
     const int send = min(base + kS, w);
     double x[RPT][kS];  // this thread's rows over the sub-panel's columns
@@ -179,11 +203,18 @@ __global__ void __launch_bounds__(kT, 1) panel_reg_kernel(PanelParams p) {
       const int kl = (int)(k - row0);
       const bool own_k = kl >= 0 && kl < rows_here;
 
+      const unsigned xb = xbar0 + 8u * (unsigned)par;
+      if (tid == 0) panel::xbar_expect(xb, (unsigned)((C + 1) * sizeof(Slot)));
+
       // 1. this CTA's candidate: per-warp winners staged with their slices
       if (positioned) {
         mine = LocalBest{0.0, -1, 0, 0.0};
-        if (own_k && tid == kl % kT) mine = LocalBest{__longlong_as_double(0x7ff0000000000000ll), kl, 0, 0.0};
+        if (own_k && tid == kl % kT) {
+          mine = LocalBest{__longlong_as_double(0x7ff0000000000000ll), kl, 0, 0.0};
+          mine_x = sm[kl];  // step 0: column 0 in shared memory is still current
+        }
       }
+      const double mine_inv = mine.row >= 0 ? 1.0 / mine_x : 0.0;
       const LocalBest wb = warp_lb(mine);
       if (wb.row >= 0 && tid == wb.row % kT) {
         Slot& st = S.stage[warp];
@@ -193,8 +224,8 @@ __global__ void __launch_bounds__(kT, 1) panel_reg_kernel(PanelParams p) {
           if (i == wi) {
 #pragma unroll
             for (int t = 0; t < kS; ++t) st.v[t] = x[i][t];
-            st.inv = 1.0 / x[i][j];
           }
+        st.inv = mine_inv;
         st.val = wb.val;
         st.sec = wb.sec;
         st.row = (int)(row0 + wb.row);
@@ -231,22 +262,38 @@ __global__ void __launch_bounds__(kT, 1) panel_reg_kernel(PanelParams p) {
             lane < kW ? ((have && cs->row == brow) ? cs->sec : (have ? cs->val : cs->sec)) : 0.0);
         const int wsel = __ffs(__ballot_sync(0xffffffffu, have && cs->row == brow)) - 1;
         if (warp == 0 && lane < C) {
-          Slot* dst = cluster.map_shared_rank(S.slots + par * kMaxC + rank, lane);
-          if (wsel >= 0) {
-            copy_slot(dst, S.stage + wsel);
-            dst->sec = bsec;
-          } else {
-            dst->val = 0.0;
-            dst->sec = bsec;
-            dst->inv = 0.0;
-            dst->row = -1;
-            dst->orig = -1;
+          uint4 c[kSlotChunks];
+          const uint4* src = reinterpret_cast<const uint4*>(S.stage + (wsel >= 0 ? wsel : 0));
+#pragma unroll
+          for (int i = 0; i < kSlotChunks; ++i) c[i] = src[i];
+          if (wsel < 0) {  // no candidate: magnitude 0, row -1, reciprocal 0
+            c[0].x = c[0].y = 0u;
+            c[1] = make_uint4(0u, 0u, 0xffffffffu, 0xffffffffu);
           }
+          const unsigned long long sb = (unsigned long long)__double_as_longlong(bsec);
+          c[0].z = (unsigned)sb;
+          c[0].w = (unsigned)(sb >> 32);
+          const unsigned dst = panel::peer_addr(panel::smem_addr(S.slots + par * kMaxC + rank), lane);
+          const unsigned bar = panel::peer_addr(xb, lane);
+#pragma unroll
+          for (int i = 0; i < kSlotChunks; ++i) panel::st_async16(dst + 16u * i, c[i], bar);
         }
-        if (warp == 1 && own_k && lane < C)
-          copy_slot(cluster.map_shared_rank(S.kslot + par, lane), S.stage + kW);
+        if (warp == 1 && own_k && lane < C) {
+          const uint4* src = reinterpret_cast<const uint4*>(S.stage + kW);
+          const unsigned dst = panel::peer_addr(panel::smem_addr(S.kslot + par), lane);
+          const unsigned bar = panel::peer_addr(xb, lane);
+#pragma unroll
+          for (int i = 0; i < kSlotChunks; ++i) panel::st_async16(dst + 16u * i, src[i], bar);
+        }
       }
-      cluster.sync();
+      // every CTA's slot and row k's slice have arrived (use s >> 1 of this
+      // parity's barrier)
+      if (__syncthreads_or(!panel::xbar_wait(xb, (unsigned)(s >> 1) & 1u))) {
+        if (tid == 0) p.state->status = kDeviceTimeout;
+        timed_out = stopped = true;
+        kd = 0;
+        break;
+      }
 
       // 3. same decision everywhere
       int wslot = -1;
@@ -265,7 +312,7 @@ __global__ void __launch_bounds__(kT, 1) panel_reg_kernel(PanelParams p) {
           wval = bv;
         }
       }
-      if (rank == 0 && tid == 0 && !positioned) note_decision(p.state, k, wval, wsec);
+      if (rank == 0 && tid == 0 && !positioned) tally.note(k, wval, wsec);
       const bool stop = !positioned && !(wslot >= 0 && wval > p.threshold);
       if (stop) {
         if (rank == 0 && tid == 0) p.state->stop_k = (int)k;
@@ -321,7 +368,7 @@ __global__ void __launch_bounds__(kT, 1) panel_reg_kernel(PanelParams p) {
         x[i][j] = l;
 #pragma unroll
         for (int t = j + 1; t < kS; ++t) x[i][t] = fma(-l, pv[t], x[i][t]);
-        if (j + 1 < kS && s + 1 < send) offer(mine, fabs(x[i][j + 1 < kS ? j + 1 : 0]), r);
+        if (j + 1 < kS && s + 1 < send) offer_x(mine, mine_x, x[i][j + 1 < kS ? j + 1 : 0], r);
       }
     }
 
@@ -337,39 +384,32 @@ __global__ void __launch_bounds__(kT, 1) panel_reg_kernel(PanelParams p) {
           if (base + t < w) sm[(base + t) * RP + r] = x[i][t];
       }
     }
-    // b. composite source map of the sub-panel's swaps (the same everywhere)
-    if (tid == 0) {
-      int pos[2 * kS], src[2 * kS], np = 0;
-      for (int t = 0; t < kd; ++t) {
+    // b. composite source map of the sub-panel's swaps (the same everywhere):
+    //    lane q of warp 0 takes position k_q (q < kd) or p_{q - kd} and traces
+    //    it back through the swaps to the row whose content it holds now;
+    //    the moved positions are compacted by a ballot, duplicates (a pivot
+    //    row that is also a later step's row k) kept once
+    if (warp == 0) {
+      const bool on = lane < 2 * kd;
+      int x = on ? S.plist[lane < kd ? 2 * lane : 2 * (lane - kd) + 1] : 0;
+      const int pos = x;
+      for (int t = kd - 1; t >= 0 && on; --t) {
         const int a = S.plist[2 * t], b = S.plist[2 * t + 1];
-        if (a == b) continue;
-        int ia = -1, ib = -1;
-        for (int q = 0; q < np; ++q) {
-          if (pos[q] == a) ia = q;
-          if (pos[q] == b) ib = q;
-        }
-        if (ia < 0) {
-          ia = np++;
-          pos[ia] = a;
-          src[ia] = a;
-        }
-        if (ib < 0) {
-          ib = np++;
-          pos[ib] = b;
-          src[ib] = b;
-        }
-        const int tmp = src[ia];
-        src[ia] = src[ib];
-        src[ib] = tmp;
+        x = x == a ? b : (x == b ? a : x);
       }
-      int nc = 0;
-      for (int q = 0; q < np; ++q)
-        if (pos[q] != src[q]) {
-          S.chg[1 + 2 * nc] = pos[q];
-          S.chg[2 + 2 * nc] = src[q];
-          ++nc;
-        }
-      S.chg[0] = nc;
+      bool keep = on && x != pos;
+      // first occurrence of each position
+      for (int q = 0; q < 2 * kS; ++q) {
+        const int other = __shfl_sync(0xffffffffu, pos, q);
+        if (q < lane && q < 2 * kd && other == pos) keep = false;
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, keep);
+      if (keep) {
+        const int at = __popc(bal & ((1u << lane) - 1u));
+        S.chg[1 + 2 * at] = pos;
+        S.chg[2 + 2 * at] = x;
+      }
+      if (lane == 0) S.chg[0] = __popc(bal);
     }
     __syncthreads();
     const int nchg = S.chg[0];
@@ -379,21 +419,24 @@ __global__ void __launch_bounds__(kT, 1) panel_reg_kernel(PanelParams p) {
         if (S.chg[1 + 2 * q] == g) return S.chg[2 + 2 * q];
       return g;
     };
+    // the owners' writes of the previous sub-panel end are visible
+    if (pending) {
+      panel::cluster_wait();
+      pending = false;
+    }
     const int ncol_out = base + (w - send);  // columns outside the sub-panel
     auto out_col = [&](int c) { return c < base ? c : send + (c - base); };
-    // c. phase A: moved rows of this CTA (into tmp) and the pivot rows of
-    //    the sub-panel's far columns (into psave), read from their owners
-    int nmine = 0;  // moved rows of this CTA, in chg order
-    for (int q = 0; q < nchg; ++q) {
+    // c. phase A: moved rows of this CTA (into tmp, row q of tmp for entry q
+    //    of the map) and the pivot rows of the sub-panel's far columns (into
+    //    psave), read from their owners; every (row, column) element is an
+    //    independent load, spread over all threads
+    for (int e = tid; e < nchg * ncol_out; e += kT) {
+      const int q = e / ncol_out, c = e - q * ncol_out;
       const long long g = S.chg[1 + 2 * q];
-      if (g >= row0 && g < row0 + rows_here) {
-        const int sg = S.chg[2 + 2 * q];
-        const int owner = (int)((sg - p.begin) / R), sl = (int)(sg - p.begin - (long long)owner * R);
-        const double* rsm = cluster.map_shared_rank(sm, owner);
-        for (int c = tid; c < ncol_out; c += kT)
-          S.tmp[nmine * W1 + c] = rsm[out_col(c) * RP + sl];
-        ++nmine;
-      }
+      if (g < row0 || g >= row0 + rows_here) continue;
+      const int sg = S.chg[2 + 2 * q];
+      const int owner = (int)((sg - p.begin) / R), sl = (int)(sg - p.begin - (long long)owner * R);
+      S.tmp[q * W1 + c] = cluster.map_shared_rank(sm, owner)[out_col(c) * RP + sl];
     }
     if (send < w) {
       for (int e = tid; e < kd * (w - send); e += kT) {
@@ -405,14 +448,10 @@ __global__ void __launch_bounds__(kT, 1) panel_reg_kernel(PanelParams p) {
     }
     cluster.sync();  // every CTA has read what it needs before anyone overwrites
     // d. phase B: moved rows take their sources' content
-    nmine = 0;
-    for (int q = 0; q < nchg; ++q) {
+    for (int e = tid; e < nchg * ncol_out; e += kT) {
+      const int q = e / ncol_out, c = e - q * ncol_out;
       const long long g = S.chg[1 + 2 * q];
-      if (g >= row0 && g < row0 + rows_here) {
-        const int gl = (int)(g - row0);
-        for (int c = tid; c < ncol_out; c += kT) sm[out_col(c) * RP + gl] = S.tmp[nmine * W1 + c];
-        ++nmine;
-      }
+      if (g >= row0 && g < row0 + rows_here) sm[out_col(c) * RP + (int)(g - row0)] = S.tmp[q * W1 + c];
     }
     if (send >= w) break;  // no columns right of the sub-panel
     __syncthreads();       // psave and the moved rows complete
@@ -457,7 +496,7 @@ __global__ void __launch_bounds__(kT, 1) panel_reg_kernel(PanelParams p) {
         for (int t = 0; t < kS; ++t)
           if (t < kd) xs = fma(-l[t], ps[t * W1 + send], xs);
         row[send * RP] = xs;
-        offer(mine, fabs(xs), r);
+        offer_x(mine, mine_x, xs, r);
       }
 #pragma unroll 4
       for (int c = send + 1; c < w; ++c) {
@@ -469,10 +508,19 @@ __global__ void __launch_bounds__(kT, 1) panel_reg_kernel(PanelParams p) {
       }
     }
     __syncthreads();  // the next sub-panel's columns are final in shared memory
+    // released to the readers of the next sub-panel end (phase A); the
+    // steps in between exchange through the transaction barriers alone
+    panel::cluster_arrive();
+    pending = true;
   }
   // No CTA may exit while a peer could still read its shared memory, and
   // rows were written by other threads than those writing them back.
-  cluster.sync();
+  if (pending)
+    panel::cluster_wait();
+  else
+    cluster.sync();
+  if (timed_out) return;
+  if (rank == 0 && tid == 0) tally.flush(p.state);
 
 #pragma unroll 4
   for (int c = 0; c < w; ++c) {

@@ -92,8 +92,9 @@ size_t small_factor_bytes(int n) {
 size_t large_factor_bytes(int n) {
   // factors + composite orders, the blocked factorisation's workspace
   // (mailboxes, candidate rows, the BF16 pieces of the mixed updates: three
-  // pieces of 256 columns for n + n and n + 256 operand rows)
-  return dp::factor_bytes(n) + 5120 * (size_t)n + (8u << 20);
+  // pieces of 256 columns for n + n and n + 256 operand rows; the outer
+  // blocks' inverses and the 256-row copies of their block solves)
+  return dp::factor_bytes(n) + 7168 * (size_t)n + (10u << 20);
 }
 
 }  // namespace

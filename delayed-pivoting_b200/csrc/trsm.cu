@@ -175,7 +175,80 @@ void configure() {
 
 }  // namespace
 
+// T <- I - L^{-1} for a unit lower w x w block L (w <= 256), so that the
+// block solve X = L^{-1} B becomes the FP64 tensor-core update
+// X = B - T B (T strictly lower).  Column j of L^{-1} is one warp's forward
+// substitution L x = e_j: lane l holds rows l + 32 r, the pivot entry x_k
+// travels by shuffle, and column k of L is read once per step (coalesced;
+// the CTA's 8 warps read the same columns, so most reads hit L1).
+constexpr int kInvMaxW = 256;
+constexpr int kInvRows = kInvMaxW / 32;  // rows per lane
+constexpr int kInvWarps = 8;
+
+__global__ void __launch_bounds__(32 * kInvWarps)
+lower_inverse_kernel(const double* __restrict__ L, long long ldl, int w, double* __restrict__ T,
+                     long long ldt) {
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x * kInvWarps + (threadIdx.x >> 5);
+  if (j >= w) return;
+  double x[kInvRows];
+#pragma unroll
+  for (int r = 0; r < kInvRows; ++r) x[r] = lane + 32 * r == j ? 1.0 : 0.0;
+#pragma unroll
+  for (int kb = 0; kb < kInvRows; ++kb) {
+    if (32 * kb >= w - 1) break;      // no step left
+    if (32 * kb + 31 < j) continue;   // x_k = 0 for every k of this group
+#pragma unroll
+    for (int kk = 0; kk < 32; ++kk) {
+      const int k = 32 * kb + kk;
+      if (k < j || k >= w - 1) continue;  // (warp-uniform)
+      const double xk = __shfl_sync(0xffffffffu, x[kb], kk);
+      const double* Lk = L + (size_t)k * (size_t)ldl;
+#pragma unroll
+      for (int r = kb; r < kInvRows; ++r) {
+        const int i = lane + 32 * r;
+        if (i > k && i < w) x[r] = fma(-__ldg(Lk + i), xk, x[r]);
+      }
+    }
+  }
+  double* Tj = T + (size_t)j * (size_t)ldt;
+#pragma unroll
+  for (int r = 0; r < kInvRows; ++r) {
+    const int i = lane + 32 * r;
+    if (i < w) Tj[i] = i > j ? -x[r] : 0.0;
+  }
+}
+
+// dst(0:rows, 0:cols) <- src(0:rows, 0:cols), both column-major: a CTA per
+// column at a time, consecutive threads on consecutive rows.
+__global__ void __launch_bounds__(256)
+copy_block_kernel(const double* __restrict__ src, long long lds, double* __restrict__ dst,
+                  long long ldd, int rows, int cols) {
+  for (long long c = blockIdx.x; c < cols; c += gridDim.x) {
+    const double* s = src + c * lds;
+    double* d = dst + c * ldd;
+    for (int r = threadIdx.x; r < rows; r += blockDim.x) d[r] = s[r];
+  }
+}
+
 int trsm_max_width() { return kTrsmW; }
+
+void launch_copy_block(const double* src, long long lds, double* dst, long long ldd, int rows,
+                       int cols, cudaStream_t s) {
+  if (rows <= 0 || cols <= 0) return;
+  dp::note_launch();
+  copy_block_kernel<<<std::min(cols, 148 * 8), 256, 0, s>>>(src, lds, dst, ldd, rows, cols);
+}
+
+int lower_inverse_max_width() { return kInvMaxW; }
+
+void launch_lower_inverse(const double* L, long long ldl, int w, double* T, long long ldt,
+                          cudaStream_t s) {
+  if (w <= 0) return;
+  dp::note_launch();
+  lower_inverse_kernel<<<(w + kInvWarps - 1) / kInvWarps, 32 * kInvWarps, 0, s>>>(L, ldl, w, T,
+                                                                                  ldt);
+}
 
 void launch_trsm_lower_unit(const double* L, long long ldl, double* B, long long ldb, int w, int nc,
                             cudaStream_t s, const int* gate) {

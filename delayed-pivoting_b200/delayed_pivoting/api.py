@@ -416,6 +416,14 @@ def gemm_tile(tile: int) -> int:
     return lib().dp_gemm_tile(int(tile))
 
 
+def block_solve(mode: int) -> int:
+    """dp_block_solve: triangular solves of the outer blocks, 0 automatic (= 1),
+    1 by inverse (one FP64 tensor-core GEMM per block), 2 by substitution.
+
+    Returns the previous setting."""
+    return lib().dp_block_solve(int(mode))
+
+
 def gesv_ir_device(n, nrhs, d_a, lda, d_b, ldb, precision=PRECISION_MIXED_BF16X3, max_iter=10,
                    tol=1e-14, stream=None):
     """dp_gesv_ir_device: mixed-precision LU + FP64 iterative refinement.

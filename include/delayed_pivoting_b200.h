@@ -403,6 +403,16 @@ int dp_gemm_tile(int tile);
  * previous setting, or -2000 for a setting outside [-1024, 1024]. */
 int dp_tri_solve_grid(int policy);
 
+/* How the factorisations solve the triangular systems of their outer blocks
+ * (U12 = L11^{-1} A12 for blocks wider than 64 rows): 0 automatic (= 1),
+ * 1 by inverse (T = I - L11^{-1} once per block, then U12 = A12 - T A12 on
+ * the FP64 tensor path), 2 by substitution (64-row solves chained with
+ * updates).  Process-wide; the two differ in rounding only (pivot records
+ * differ only where a decision is a near tie).  The allocation-free entry
+ * point always uses substitution.  Returns the previous setting, or -1 for an
+ * invalid one. */
+int dp_block_solve(int mode);
+
 /* delayed_dgetrf_cuda.hpp:63 (delayed_getrf_cuda_status_string). */
 const char *dp_status_string(int status);
 

@@ -5,7 +5,11 @@ whole pool, a fixed HBM budget, an allocator other than the CUDA runtime's).
 It is called twice in a row on the same input through the C ABI and each
 result is checked against dp_getrf_device: identical pivot records and info,
 factors equal within the tests' residual bound (scaled residual <= 10, the
-same bound as the parity tests), and the scaled residual itself <= 10.
+same bound as the parity tests), and the scaled residual itself <= 10.  The
+allocation-free path solves the outer blocks' triangular systems by
+substitution (it has no room for their inverses), so its factors are
+compared with dp_getrf_device in that mode (dp_block_solve(2)); its records
+must also equal those of the default (by inverse) mode.
 Inputs beyond its fixed scratch are rejected before any device work.
 
 The file name makes pytest collect it last, so a run that stops at the first
@@ -46,8 +50,15 @@ def test_noalloc_matches_allocating_entry_point_twice(built, name):
 
     a, case = gc.load(name)
     m, n = case["m"], case["n"]
-    st0, info0, ip0, jp0, f0 = _factor(dp.delayed_getrf_cuda_device, a, m, n)
-    assert st0 == dp.SUCCESS
+    st1, info1, ip1, jp1, _ = _factor(dp.delayed_getrf_cuda_device, a, m, n)
+    prev = dp.block_solve(2)
+    try:
+        st0, info0, ip0, jp0, f0 = _factor(dp.delayed_getrf_cuda_device, a, m, n)
+    finally:
+        dp.block_solve(prev)
+    assert st0 == st1 == dp.SUCCESS and info0 == info1
+    np.testing.assert_array_equal(ip0, ip1)
+    np.testing.assert_array_equal(jp0, jp1)
     for _ in range(2):  # the shared scratch keeps the previous call's contents
         st, info, ip, jp, f = _factor(dp.getrf_device_noalloc, a, m, n)
         assert st == dp.SUCCESS
