@@ -222,8 +222,16 @@ using Small = Cfg<64, 64, 16, 3, 2, 2, 3>;
 using Small4 = Cfg<64, 64, 16, 2, 2, 2, 4>;
 // 128 x 64 tiles as Half with 8 warps of 32 x 32: 16 warps per SM.
 using HalfW8 = Cfg<128, 64, 16, 4, 4, 2, 2>;
+// 64 x 128 tiles (the shape of the library DGEMM on this part), three stages
+// of 16: 4 warps of 32 x 64, or 8 warps of 32 x 32; two CTAs per SM.
+using Wide = Cfg<64, 128, 16, 3, 2, 2, 2>;
+using Wide8 = Cfg<64, 128, 16, 3, 2, 4, 2>;
+// 64 x 64 tiles with 32-deep k chunks in two stages, three CTAs per SM.
+using SmallK32 = Cfg<64, 64, 32, 2, 2, 2, 3>;
 
-std::atomic<int> g_tile{0};  // 0 automatic (Small4), 1 Big, 2 Half, 3 Small, 4 HalfW8, 5 Small4
+// 0 automatic (Small4), 1 Big, 2 Half, 3 Small, 4 HalfW8, 5 Small4, 6 Wide,
+// 7 Wide8, 8 SmallK32
+std::atomic<int> g_tile{0};
 
 }  // namespace gemm
 
@@ -244,6 +252,12 @@ void launch_gemm_minus(int M, int N, int K, const double* A, long long lda, cons
     gemm::launch<gemm::Small>(M, N, K, A, lda, B, ldb, C, ldc, s, gate);
   else if (tile == 4)
     gemm::launch<gemm::HalfW8>(M, N, K, A, lda, B, ldb, C, ldc, s, gate);
+  else if (tile == 6)
+    gemm::launch<gemm::Wide>(M, N, K, A, lda, B, ldb, C, ldc, s, gate);
+  else if (tile == 7)
+    gemm::launch<gemm::Wide8>(M, N, K, A, lda, B, ldb, C, ldc, s, gate);
+  else if (tile == 8)
+    gemm::launch<gemm::SmallK32>(M, N, K, A, lda, B, ldb, C, ldc, s, gate);
   else
     gemm::launch<gemm::Small4>(M, N, K, A, lda, B, ldb, C, ldc, s, gate);
 }
@@ -262,7 +276,7 @@ int dp_schur_update_device(int M, int N, int K, const double* A, int lda, const 
 }
 
 int dp_gemm_tile(int tile) {
-  if (tile < 0 || tile > 5) return -1;
+  if (tile < 0 || tile > 8) return -1;
   return dp::gemm::g_tile.exchange(tile);
 }
 

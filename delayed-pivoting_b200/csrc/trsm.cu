@@ -178,39 +178,73 @@ void configure() {
 // T <- I - L^{-1} for a unit lower w x w block L (w <= 256), so that the
 // block solve X = L^{-1} B becomes the FP64 tensor-core update
 // X = B - T B (T strictly lower).  Column j of L^{-1} is one warp's forward
-// substitution L x = e_j: lane l holds rows l + 32 r, the pivot entry x_k
-// travels by shuffle, and column k of L is read once per step (coalesced;
-// the CTA's 8 warps read the same columns, so most reads hit L1).
+// substitution L x = e_j: lane l holds rows l + 32 r, the entry x_k travels
+// by shuffle.  The CTA's 8 warps share L through shared memory: 32-column
+// chunks of its strict lower part (zeros elsewhere) are staged by cp.async,
+// the next chunk in flight while the warps step through the current one.
 constexpr int kInvMaxW = 256;
 constexpr int kInvRows = kInvMaxW / 32;  // rows per lane
 constexpr int kInvWarps = 8;
+constexpr int kInvChunk = 32;            // columns of L per staged chunk
+constexpr size_t kInvSmem = 2 * (size_t)kInvChunk * kInvMaxW * sizeof(double);
+static_assert(kInvChunk == 32, "one chunk per lane row group");
+
+__device__ __forceinline__ void cp_async8_zfill(double* dst, const double* src, bool ok) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(ok ? 8 : 0)
+               : "memory");
+}
 
 __global__ void __launch_bounds__(32 * kInvWarps)
 lower_inverse_kernel(const double* __restrict__ L, long long ldl, int w, double* __restrict__ T,
                      long long ldt) {
-  const int lane = threadIdx.x & 31;
-  const int j = blockIdx.x * kInvWarps + (threadIdx.x >> 5);
-  if (j >= w) return;
+  extern __shared__ __align__(16) double ls[];  // [2][kInvChunk][kInvMaxW]
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int j0 = blockIdx.x * kInvWarps;
+  const int j = j0 + (tid >> 5);
+  const bool active = j < w;
   double x[kInvRows];
 #pragma unroll
   for (int r = 0; r < kInvRows; ++r) x[r] = lane + 32 * r == j ? 1.0 : 0.0;
+  const int c_first = j0 / kInvChunk;
+  const int c_last = w >= 2 ? (w - 2) / kInvChunk : -1;  // last chunk holding a step
+  auto stage = [&](int c, int buf) {
+    double* dst = ls + (size_t)buf * kInvChunk * kInvMaxW;
+    for (int e = tid; e < kInvChunk * kInvMaxW; e += 32 * kInvWarps) {
+      const int kk = e / kInvMaxW, i = e % kInvMaxW;
+      const int k = c * kInvChunk + kk;
+      const bool ok = i < w && i > k;
+      cp_async8_zfill(dst + e, ok ? L + i + (size_t)k * (size_t)ldl : L, ok);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  if (c_first <= c_last) stage(c_first, 0);
 #pragma unroll
-  for (int kb = 0; kb < kInvRows; ++kb) {
-    if (32 * kb >= w - 1) break;      // no step left
-    if (32 * kb + 31 < j) continue;   // x_k = 0 for every k of this group
+  for (int c = 0; c < kInvRows; ++c) {
+    if (c < c_first || c > c_last) continue;  // (CTA-uniform)
+    const int buf = (c - c_first) & 1;
+    if (c + 1 <= c_last) {
+      stage(c + 1, buf ^ 1);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+    const double* lc = ls + (size_t)buf * kInvChunk * kInvMaxW;
+    if (active) {
 #pragma unroll
-    for (int kk = 0; kk < 32; ++kk) {
-      const int k = 32 * kb + kk;
-      if (k < j || k >= w - 1) continue;  // (warp-uniform)
-      const double xk = __shfl_sync(0xffffffffu, x[kb], kk);
-      const double* Lk = L + (size_t)k * (size_t)ldl;
+      for (int kk = 0; kk < kInvChunk; ++kk) {
+        const int k = kInvChunk * c + kk;
+        if (k < j || k >= w - 1) continue;  // (warp-uniform)
+        const double xk = __shfl_sync(0xffffffffu, x[c], kk);
 #pragma unroll
-      for (int r = kb; r < kInvRows; ++r) {
-        const int i = lane + 32 * r;
-        if (i > k && i < w) x[r] = fma(-__ldg(Lk + i), xk, x[r]);
+        for (int r = c; r < kInvRows; ++r)
+          x[r] = fma(-lc[kk * kInvMaxW + lane + 32 * r], xk, x[r]);  // zero where i <= k
       }
     }
+    __syncthreads();  // this buffer is restaged two chunks later
   }
+  if (!active) return;
   double* Tj = T + (size_t)j * (size_t)ldt;
 #pragma unroll
   for (int r = 0; r < kInvRows; ++r) {
@@ -245,9 +279,10 @@ int lower_inverse_max_width() { return kInvMaxW; }
 void launch_lower_inverse(const double* L, long long ldl, int w, double* T, long long ldt,
                           cudaStream_t s) {
   if (w <= 0) return;
+  dp::ensure_smem((const void*)lower_inverse_kernel, kInvSmem);
   dp::note_launch();
-  lower_inverse_kernel<<<(w + kInvWarps - 1) / kInvWarps, 32 * kInvWarps, 0, s>>>(L, ldl, w, T,
-                                                                                  ldt);
+  lower_inverse_kernel<<<(w + kInvWarps - 1) / kInvWarps, 32 * kInvWarps, kInvSmem, s>>>(
+      L, ldl, w, T, ldt);
 }
 
 void launch_trsm_lower_unit(const double* L, long long ldl, double* B, long long ldb, int w, int nc,

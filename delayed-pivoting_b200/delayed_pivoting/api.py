@@ -410,7 +410,8 @@ def schur_update_mixed_device(M, N, K, d_a, lda, d_b, ldb, d_c, ldc,
 
 def gemm_tile(tile: int) -> int:
     """dp_gemm_tile: 0 automatic (= 5), 1 128 x 128, 2 128 x 64, 3 64 x 64, 4 128 x 64
-    (8 warps), 5 64 x 64 (two stages).
+    (8 warps), 5 64 x 64 (two stages), 6 64 x 128 (4 warps), 7 64 x 128 (8 warps),
+    8 64 x 64 (32-deep k chunks).
 
     Returns the previous setting."""
     return lib().dp_gemm_tile(int(tile))

@@ -393,7 +393,8 @@ int dp_schur_update_mixed_device(int M, int N, int K, const double *A, int lda, 
 /* Tile of that kernel for N > 32 (tuning; no result bit depends on it):
  * 0 automatic (= 5), 1 128 x 128 (one CTA per SM), 2 128 x 64 (two CTAs per
  * SM), 3 64 x 64 (three CTAs per SM), 4 128 x 64 with eight warps, 5 64 x 64
- * with two stages (four CTAs per SM).
+ * with two stages (four CTAs per SM), 6 64 x 128 with four warps, 7 64 x 128
+ * with eight warps, 8 64 x 64 with 32-deep k chunks.
  * Returns the previous setting, or -1 for an invalid one. */
 int dp_gemm_tile(int tile);
 
