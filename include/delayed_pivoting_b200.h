@@ -49,7 +49,7 @@ typedef struct dp_options {
   int panel_rows;    /* target rows per CTA in the panel kernel; 0 = automatic */
   int nb_outer;      /* outer block width of the trailing update; 0 = automatic */
   int panel_kernel;  /* 0 automatic (single-CTA panel up to 512 rows, else the cluster
-                        panel), 1 cluster (sub-panel in registers up to 1024 rows per
+                        panel), 1 cluster (sub-panel in registers up to 512 rows per
                         CTA), 2 grid-wide, 3 cluster with the sub-panel in shared memory */
   int precision;     /* DP_PRECISION_FP64 (reference arithmetic) or
                         DP_PRECISION_MIXED_BF16X3 (tensor-core trailing update) */
