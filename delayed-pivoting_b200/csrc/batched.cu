@@ -46,6 +46,8 @@
 #include <new>
 #include <vector>
 
+#include <cuda_bf16.h>
+
 #include "delayed_pivoting_b200.h"
 #include "dp_device.cuh"
 #include "dp_kernels.h"
@@ -122,6 +124,32 @@ __device__ __forceinline__ void mma_f64(double (&c)[4], double a0, double a1, do
       "{%0,%1,%2,%3};\n"
       : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
       : "d"(a0), "d"(a1), "d"(b0));
+}
+
+// Mixed form of the trailing update: BF16 pieces x = x1 + x2 [+ x3] (each the
+// BF16 rounding of what the earlier ones left, as in the single-matrix
+// tensor-core update), products of pieces (i, j) with i + j <= TERMS - 1 on
+// mma.sync.m16n8k16 with FP32 accumulation.
+template <int TERMS>
+__device__ __forceinline__ void split_pieces(double x, __nv_bfloat16 (&piece)[TERMS]) {
+#pragma unroll
+  for (int t = 0; t < TERMS; ++t) {
+    piece[t] = __double2bfloat16(x);
+    x -= (double)__bfloat162float(piece[t]);
+  }
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+  return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4],
+                                         const uint32_t (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
 // Candidate (magnitude v, logical row key) beats (cv, ck)?
@@ -443,7 +471,9 @@ __device__ __forceinline__ void permute_outside(double* A, int lda, int n, int b
 // Right of a panel that executed `kd` steps at [b, b + kd), its row
 // permutation already applied: for the columns [c0, n), U12 = L11^{-1}
 // A(b:b+kd, :) (written back) and A(b+kd:n, :) -= L21 U12, with L11 / L21 the
-// shared panel P.
+// shared panel P.  TERMS = 0: the product in FP64 (DMMA); TERMS = 2 / 3: the
+// BF16 split product (3 / 6 products, FP32 accumulation), subtracted in FP64.
+template <int TERMS>
 __device__ __forceinline__ void trailing_update(double* A, int lda, int n, int b, int kd, int c0,
                                                 const double* P, int pr, double* Bs) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -501,29 +531,83 @@ __device__ __forceinline__ void trailing_update(double* A, int lda, int n, int b
               cf[mi][ni][v] = (r < M && c < nc) ? C[idx(r, c, lda)] : 0.0;
             }
         double acc[2][4][4];
-#pragma unroll
-        for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-          for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-            for (int v = 0; v < 4; ++v) acc[mi][ni][v] = 0.0;
-        for (int k0 = 0; k0 < kp; k0 += 4) {
-          const int kk = k0 + t;
-          const bool kok = kk < kd;
-          double a[2][2];
-#pragma unroll
-          for (int mi = 0; mi < 2; ++mi) {
-            const int r = rb + mi * 16 + g;
-            a[mi][0] = (kok && r < M) ? L21[r + kk * pr] : 0.0;
-            a[mi][1] = (kok && r + 8 < M) ? L21[r + 8 + kk * pr] : 0.0;
-          }
-          double bf[4];
-#pragma unroll
-          for (int ni = 0; ni < 4; ++ni) bf[ni] = Bh[(wn * 32 + ni * 8 + g) * kLdb + kk];
+        if constexpr (TERMS == 0) {
 #pragma unroll
           for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
-            for (int ni = 0; ni < 4; ++ni) mma_f64(acc[mi][ni], a[mi][0], a[mi][1], bf[ni]);
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+              for (int v = 0; v < 4; ++v) acc[mi][ni][v] = 0.0;
+          for (int k0 = 0; k0 < kp; k0 += 4) {
+            const int kk = k0 + t;
+            const bool kok = kk < kd;
+            double a[2][2];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi) {
+              const int r = rb + mi * 16 + g;
+              a[mi][0] = (kok && r < M) ? L21[r + kk * pr] : 0.0;
+              a[mi][1] = (kok && r + 8 < M) ? L21[r + 8 + kk * pr] : 0.0;
+            }
+            double bf[4];
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) bf[ni] = Bh[(wn * 32 + ni * 8 + g) * kLdb + kk];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+              for (int ni = 0; ni < 4; ++ni) mma_f64(acc[mi][ni], a[mi][0], a[mi][1], bf[ni]);
+          }
+        } else {
+          // m16n8k16 fragments: A (row r, k) at r = g / g + 8 and k = 2t, 2t + 1,
+          // 2t + 8, 2t + 9 of the 16-deep step; B (k, column) at the same k
+          // for column g; C as the FP64 fragments above
+          float facc[2][4][4];
+#pragma unroll
+          for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+              for (int v = 0; v < 4; ++v) facc[mi][ni][v] = 0.0f;
+          for (int k0 = 0; k0 < kd; k0 += 16) {
+            uint32_t af[TERMS][2][4], bfr[TERMS][4][2];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+              for (int h = 0; h < 4; ++h) {  // register h: rows g (+8 for odd h), k pair
+                const int r = rb + mi * 16 + g + 8 * (h & 1);
+                const int kk = k0 + 2 * t + 8 * (h >> 1);
+                __nv_bfloat16 lo[TERMS], hi[TERMS];
+                split_pieces<TERMS>((r < M && kk < kd) ? L21[r + kk * pr] : 0.0, lo);
+                split_pieces<TERMS>((r < M && kk + 1 < kd) ? L21[r + (kk + 1) * pr] : 0.0, hi);
+#pragma unroll
+                for (int q = 0; q < TERMS; ++q) af[q][mi][h] = pack_bf16(lo[q], hi[q]);
+              }
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                const double* bc = Bh + (wn * 32 + ni * 8 + g) * kLdb;
+                const int kk = k0 + 2 * t + 8 * h;
+                __nv_bfloat16 lo[TERMS], hi[TERMS];
+                split_pieces<TERMS>(kk < kd ? bc[kk] : 0.0, lo);
+                split_pieces<TERMS>(kk + 1 < kd ? bc[kk + 1] : 0.0, hi);
+#pragma unroll
+                for (int q = 0; q < TERMS; ++q) bfr[q][ni][h] = pack_bf16(lo[q], hi[q]);
+              }
+#pragma unroll
+            for (int d = 0; d < TERMS; ++d)
+#pragma unroll
+              for (int i = 0; i <= d; ++i)
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                  for (int ni = 0; ni < 4; ++ni) mma_bf16(facc[mi][ni], af[i][mi], bfr[d - i][ni]);
+          }
+#pragma unroll
+          for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+              for (int v = 0; v < 4; ++v) acc[mi][ni][v] = (double)facc[mi][ni][v];
         }
 #pragma unroll
         for (int mi = 0; mi < 2; ++mi)
@@ -602,6 +686,7 @@ __device__ __forceinline__ void active_argmax(const double* A, int lda, int n, i
     }
 }
 
+template <int TERMS>
 __device__ __forceinline__ void getrf_one(double* A, int n, int* ipiv, int* jpiv, int* info,
                                           int nb, double thr, double* P, int pr, double* Bs,
                                           Smem& s, unsigned long long* ties) {
@@ -619,14 +704,14 @@ __device__ __forceinline__ void getrf_one(double* A, int n, int* ipiv, int* jpiv
     __syncthreads();  // panel written back, move list complete
     permute_outside(A, lda, n, b, w, s);
     if (stop < 0) {
-      if (e < n) trailing_update(A, lda, n, b, w, e, P, pr, Bs);
+      if (e < n) trailing_update<TERMS>(A, lda, n, b, w, e, P, pr, Bs);
       b = e;
       continue;
     }
     // column k has no acceptable pivot: bring the columns right of the panel
     // up to date for the executed steps, then search the whole active block
     const int k = b + stop;
-    if (e < n && stop > 0) trailing_update(A, lda, n, b, stop, e, P, pr, Bs);
+    if (e < n && stop > 0) trailing_update<TERMS>(A, lda, n, b, stop, e, P, pr, Bs);
     __syncthreads();
     double bv, bs;
     int br, bc;
@@ -658,6 +743,7 @@ __device__ __forceinline__ void getrf_one(double* A, int n, int* ipiv, int* jpiv
   }
 }
 
+template <int TERMS>
 __global__ void __launch_bounds__(kThreads, 1) batched_getrf_kernel(Params p) {
   extern __shared__ __align__(16) double dsm[];
   __shared__ Smem s;
@@ -674,7 +760,7 @@ __global__ void __launch_bounds__(kThreads, 1) batched_getrf_kernel(Params p) {
     const int bk = bucket_of(n);  // selected without indexing the parameter array
     const int nb = bk == 0 ? p.nb_bucket[0] : bk == 1 ? p.nb_bucket[1] : bk == 2 ? p.nb_bucket[2]
                                                                                  : p.nb_bucket[3];
-    getrf_one(p.base + p.offsets[i], n, p.ipiv + p.rec_offsets[i], p.jpiv + p.rec_offsets[i],
+    getrf_one<TERMS>(p.base + p.offsets[i], n, p.ipiv + p.rec_offsets[i], p.jpiv + p.rec_offsets[i],
               p.info + i, nb, p.threshold, P, p.pr, Bs, s, p.ties);
   }
 }
@@ -785,7 +871,7 @@ namespace {
 
 bool valid_batch_options(const dp_batch_options* o) {
   if (!(o->threshold >= 0.0) || std::isinf(o->threshold)) return false;
-  if (o->precision != DP_PRECISION_FP64) return false;
+  if (!dp::valid_precision(o->precision)) return false;
   for (int i = 0; i < DP_BATCH_BUCKETS; ++i)
     if (o->nb_bucket[i] < 1 || o->nb_bucket[i] > DP_BATCH_MAX_NB) return false;
   return true;
@@ -830,13 +916,19 @@ int launch_raw(int count, int max_n, int sms, const int* d_n, const long long* d
   for (int i = 0; i < DP_BATCH_BUCKETS; ++i) p.nb_bucket[i] = opt.nb_bucket[i];
   p.pr = panel_ld(max_n);
   const size_t smem = dynamic_smem(max_n);
-  if (!dp::ensure_smem((const void*)batched_getrf_kernel, smem)) return DP_CUDA_FAILURE;
-  const int per_sm = dp::occupancy_once((const void*)batched_getrf_kernel, kThreads, smem);
+  const int terms = dp::mixed_terms(opt.precision);
+  const void* fn = terms == 3   ? (const void*)batched_getrf_kernel<3>
+                   : terms == 2 ? (const void*)batched_getrf_kernel<2>
+                                : (const void*)batched_getrf_kernel<0>;
+  if (!dp::ensure_smem(fn, smem)) return DP_CUDA_FAILURE;
+  const int per_sm = dp::occupancy_once(fn, kThreads, smem);
   if (per_sm < 1) return DP_CUDA_FAILURE;
   const int grid = std::max(1, std::min(count, sms * per_sm));
   if (cudaMemsetAsync(d_queue, 0, kQueueBytes, st) != cudaSuccess) return DP_CUDA_FAILURE;
   dp::note_launch();
-  batched_getrf_kernel<<<grid, kThreads, smem, st>>>(p);
+  void* args[] = {&p};
+  if (cudaLaunchKernel(fn, dim3(grid), dim3(kThreads), args, smem, st) != cudaSuccess)
+    return DP_CUDA_FAILURE;
   return cudaGetLastError() == cudaSuccess ? DP_SUCCESS : DP_CUDA_FAILURE;
 }
 

@@ -59,9 +59,13 @@ size_t panel_smem_bytes(int w, int rows_per_cta);
 // panel_factor_kernel) to columns [c0, c1) and [c2, c3).  gate_begin >= 0:
 // do nothing when state->stop_k is in [0, gate_begin) (a panel before this
 // one stopped; its own stop, at or after gate_begin, still applies).
+// [s0, s1) within [c2, c3): when no panel stopped (state->stop_k < 0) and the
+// panel is at most laswp_solve_max_width() wide, also solve the panel's block
+// rows of those columns with its unit lower triangle (U12 = L11^{-1} A12).
+int laswp_solve_max_width();
 void launch_laswp(double* a, long long lda, int begin, int nblock, const int* swap_block,
                   const int* swap_extra, const State* state, int c0, int c1, int c2, int c3,
-                  cudaStream_t s, int gate_begin = -1);
+                  cudaStream_t s, int gate_begin = -1, int s0 = 0, int s1 = 0);
 
 // Swap lists of up to kSwapSeqLists consecutive panels (kSwapSeqEntries
 // entries in all) applied in order by one launch of laswp_seq_kernel.

@@ -28,6 +28,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 #include "dp_device.cuh"
@@ -429,6 +430,11 @@ size_t mixed_scratch_bytes(int max_rows, int max_cols, int max_k, int terms) {
 
 namespace mixed {
 
+// CTAs of the tensor-core update (dp_mixed_gemm_grid): 0 one per SM
+// (persistent over the tiles), g > 0 at most g, -1 one per tile (an SM frees
+// as soon as its tile is done, so a panel waiting for SMs starts sooner).
+std::atomic<int> g_grid{0};
+
 template <int TERMS>
 int launch(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
            double* C, long long ldc, void* scratch, int* status, cudaStream_t s) {
@@ -453,7 +459,9 @@ int launch(int M, int N, int K, const double* A, long long lda, const double* B,
         !make_map(&tm.b[q], bp + (size_t)q * N * kp, N, kp))
       return kLibraryFailure;
   const int tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN);
-  const int grid = std::max(1, std::min(tiles, sm_count()));
+  const int gp = g_grid.load(std::memory_order_relaxed);
+  const int cap = gp == 0 ? sm_count() : gp < 0 ? tiles : gp;
+  const int grid = std::max(1, std::min(tiles, cap));
   dp::note_launch();
   gemm_bf16x3_kernel<TERMS><<<grid, kThreadsP, smem_bytes<TERMS>(), s>>>(tm, M, N, kp / BK, C, ldc,
                                                                         status);
@@ -505,4 +513,9 @@ extern "C" int dp_schur_update_mixed_device(int M, int N, int K, const double* A
   if (cudaStreamSynchronize(st) != cudaSuccess && rc == kOk) rc = kCudaFailure;
   if (rc != kOk) cudaGetLastError();
   return rc == kOk ? h : rc;
+}
+
+extern "C" int dp_mixed_gemm_grid(int policy) {
+  if (policy < -1 || policy > 65536) return -2;
+  return dp::mixed::g_grid.exchange(policy);
 }

@@ -66,7 +66,8 @@ int device_info(DeviceInfo& out) {
                              d.smem_optin - 1024) != cudaSuccess)
       return kCudaFailure;
     d.max_cluster = 0;
-    for (int r : {256, 512, 1024}) {  // the register-sub-panel cluster kernels
+    // the register-sub-panel cluster kernels, one instance per rows-per-thread
+    for (int r = 256; r <= panel_reg_max_rows(); r *= 2) {
       const void* f = panel_reg_kernel_for(r);
       if (!f || cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      d.smem_optin - 1024) != cudaSuccess ||
@@ -468,13 +469,16 @@ struct BlockInv {
   double* copy = nullptr;  // ldt x (columns) doubles
 };
 
+// `solved`: the block rows already hold U12 (the panel's laswp solved them).
 int update_columns(double* a, long long lda, int m, int s0, int W, int r_gemm, int c0, int n_end,
                    cudaStream_t st, Recorder& rec, void* mixed_ws = nullptr,
                    int* status = nullptr, int terms = 2, const int* gate = nullptr,
-                   const BlockInv* bi = nullptr) {
+                   const BlockInv* bi = nullptr, bool solved = false) {
   const int nc = n_end - c0;
   if (W <= 0 || nc <= 0) return kOk;
-  if (bi && bi->T && W > trsm_max_width() && W <= bi->ldt) {
+  if (solved) {
+    // U12 in place
+  } else if (bi && bi->T && W > trsm_max_width() && W <= bi->ldt) {
     rec.begin(DP_KFAM_TRSM);
     launch_copy_block(a + idx(s0, c0, lda), lda, bi->copy, W, W, nc, st);
     launch_gemm_minus(W, nc, W, bi->T, bi->ldt, bi->copy, W, a + idx(s0, c0, lda), lda, st, gate);
@@ -750,10 +754,15 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
         // swaps inside the block, then the rest of the block: both skip
         // themselves if this panel or an earlier one stopped (the swaps of
         // the stopping panel itself still apply)
+        // (panels up to laswp_solve_max_width() wide: U12 of the block rows
+        // solved by the laswp kernel right after their permutation)
+        const bool fused = w <= laswp_solve_max_width();
         rec.begin(DP_KFAM_LASWP);
-        launch_laswp(a, lda, b, w, pp.swap_block, pp.swap_extra, ws.state, B, b, e, E, st, b);
-        rec.end(0.0, 16.0 * 2.0 * w * (double)(E - B - w), 1);
-        update_columns(a, lda, m, b, w, e, e, E, st, rec, nullptr, nullptr, 2, stop_word);
+        launch_laswp(a, lda, b, w, pp.swap_block, pp.swap_extra, ws.state, B, b, e, E, st, b,
+                     fused ? e : 0, fused ? E : 0);
+        rec.end(fused ? (double)w * (w - 1) * (E - e) : 0.0, 16.0 * 2.0 * w * (double)(E - B - w), 1);
+        update_columns(a, lda, m, b, w, e, e, E, st, rec, nullptr, nullptr, 2, stop_word, nullptr,
+                       fused);
         DP_CHECK_CUDA(cudaGetLastError());
         unread = true;
         b = e;
@@ -762,19 +771,26 @@ int factorize(int m, int n, double* a, long long lda, const Options& o, Workspac
       if (int err = read_state(hs, ws, st)) return err;
       if (hs.status != kOk) return hs.status;
       const double moved = (double)(hs.block_changed + hs.swap_count);
+      // (the laswp kernel also solves the block rows of [e, E) unless the
+      // panel stopped, which it reads from the state)
+      const bool fused = w <= laswp_solve_max_width();
       rec.begin(DP_KFAM_LASWP);
       if (la) {
-        launch_laswp(a, lda, b, w, pp.swap_block, pp.swap_extra, ws.state, B, b, e, E, st);
+        launch_laswp(a, lda, b, w, pp.swap_block, pp.swap_extra, ws.state, B, b, e, E, st, -1,
+                     fused ? e : 0, fused ? E : 0);
         rec.end(0.0, 16.0 * moved * (double)(E - B - w), 1);
       } else {
-        launch_laswp(a, lda, b, w, ws.swap_block, ws.swap_extra, ws.state, 0, b, e, n, st);
+        launch_laswp(a, lda, b, w, ws.swap_block, ws.swap_extra, ws.state, 0, b, e, n, st, -1,
+                     fused ? e : 0, fused ? E : 0);
         rec.end(0.0, 16.0 * moved * (double)(n - w), 1);
       }
       if (hs.stop_k >= 0) {
         stop = hs.stop_k;
         break;
       }
-      update_columns(a, lda, m, b, w, e, e, E, st, rec);  // rest of the outer block
+      // rest of the outer block (U12 solved by the laswp kernel: no stop)
+      update_columns(a, lda, m, b, w, e, e, E, st, rec, nullptr, nullptr, 2, nullptr, nullptr,
+                     fused);
       DP_CHECK_CUDA(cudaGetLastError());
       b = e;
     }

@@ -21,19 +21,33 @@ namespace {
 constexpr int kLaswpThreads = 256;
 constexpr int kMaxSwapEntries = 512;  // 2 * maximum panel width
 constexpr int kPerLane = kMaxSwapEntries / 32;
+constexpr int kSolveW = 64;           // widest panel whose block rows laswp_kernel solves
 
+// Also, for the columns [s0, s1) (a subset of [c2, c3)) and a panel of at most
+// kSolveW columns that did not stop (state->stop_k < 0): U12 = L11^{-1} of the
+// panel's block rows right after they are permuted, L11 the panel's unit
+// lower triangle (the in-block TRSM, delayed_lu/delayed_dgetrf.cpp:72-74,
+// fused: one warp per column, rows begin + lane and begin + 32 + lane, the
+// entries of step k passed by shuffle, the same order of operations per row
+// as the TRSM kernel).
 __global__ void __launch_bounds__(kLaswpThreads)
 laswp_kernel(double* a, long long lda, int begin, int nblock, const int* swap_block,
              const int* swap_extra, const State* state, int c0, int c1, int c2, int c3,
-             int gate_begin) {
+             int gate_begin, int s0, int s1) {
   __shared__ int s_dst[kMaxSwapEntries];
   __shared__ int s_src[kMaxSwapEntries];
   __shared__ int s_count;
-  if (gate_begin >= 0) {
-    const int sk = state->stop_k;
-    if (sk >= 0 && sk < gate_begin) return;  // an earlier panel stopped: this one never ran
-  }
+  __shared__ double s_l[kSolveW * kSolveW];  // s_l[k * kSolveW + i] = L11(i, k), i > k
+  const int sk = state->stop_k;
+  if (gate_begin >= 0 && sk >= 0 && sk < gate_begin) return;  // an earlier panel stopped
+  const bool solve = s0 < s1 && sk < 0 && nblock <= kSolveW;
   const int tid = threadIdx.x;
+  if (solve) {
+    for (int e = tid; e < kSolveW * kSolveW; e += blockDim.x) {
+      const int k = e / kSolveW, i = e - k * kSolveW;
+      s_l[e] = (i > k && i < nblock) ? a[idx(begin + i, begin + k, lda)] : 0.0;
+    }
+  }
   const int nextra = min(state->swap_count, kMaxSwapEntries - nblock);
   if (tid == 0) s_count = 0;
   __syncthreads();
@@ -64,7 +78,7 @@ laswp_kernel(double* a, long long lda, int begin, int nblock, const int* swap_bl
   }
   __syncthreads();
   const int total = s_count;
-  if (total == 0) return;
+  if (total == 0 && !solve) return;
 
   const int lane = tid & 31;
   const int warps = blockDim.x >> 5;
@@ -86,6 +100,20 @@ laswp_kernel(double* a, long long lda, int begin, int nblock, const int* swap_bl
       if (i < total) ac[s_dst[i]] = v[j];
     }
     __syncwarp();
+    if (solve && col >= s0 && col < s1) {  // (warp-uniform)
+      double* bc = ac + begin;
+      double x0 = lane < nblock ? bc[lane] : 0.0;
+      double x1 = 32 + lane < nblock ? bc[32 + lane] : 0.0;
+      for (int k = 0; k < nblock - 1; ++k) {
+        const double xk = __shfl_sync(0xffffffffu, k < 32 ? x0 : x1, k & 31);
+        // only rows below k (an infinite or NaN x_k must not reach the others)
+        if (lane > k) x0 = fma(-s_l[k * kSolveW + lane], xk, x0);
+        if (32 + lane > k) x1 = fma(-s_l[k * kSolveW + 32 + lane], xk, x1);
+      }
+      if (lane < nblock) bc[lane] = x0;
+      if (32 + lane < nblock) bc[32 + lane] = x1;
+      __syncwarp();
+    }
   }
 }
 
@@ -216,15 +244,17 @@ int grid_for(long long work, int threads, int cap) {
 
 void launch_laswp(double* a, long long lda, int begin, int nblock, const int* swap_block,
                   const int* swap_extra, const State* state, int c0, int c1, int c2, int c3,
-                  cudaStream_t s, int gate_begin) {
+                  cudaStream_t s, int gate_begin, int s0, int s1) {
   const long long ncols = (long long)(c1 - c0) + (c3 - c2);
   if (ncols <= 0 || nblock <= 0) return;
   const int warps = kLaswpThreads / 32;
   const int grid = grid_for(ncols, warps, 148 * 16);
   dp::note_launch();
   laswp_kernel<<<grid, kLaswpThreads, 0, s>>>(a, lda, begin, nblock, swap_block, swap_extra,
-                                              state, c0, c1, c2, c3, gate_begin);
+                                              state, c0, c1, c2, c3, gate_begin, s0, s1);
 }
+
+int laswp_solve_max_width() { return kSolveW; }
 
 int launch_laswp_seq(double* a, long long lda, const int* blk, const int* ext, int base,
                      const int* widths, int lists, int c0, int c1, int c2, int c3,

@@ -417,6 +417,12 @@ def gemm_tile(tile: int) -> int:
     return lib().dp_gemm_tile(int(tile))
 
 
+def mixed_gemm_grid(policy: int) -> int:
+    """dp_mixed_gemm_grid: CTAs of the tensor-core update, 0 one per SM
+    (persistent), g > 0 at most g, -1 one per tile.  Returns the previous setting."""
+    return lib().dp_mixed_gemm_grid(int(policy))
+
+
 def block_solve(mode: int) -> int:
     """dp_block_solve: triangular solves of the outer blocks, 0 automatic (= 1),
     1 by inverse (one FP64 tensor-core GEMM per block), 2 by substitution.

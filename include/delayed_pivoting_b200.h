@@ -214,7 +214,14 @@ void dp_factor_destroy(dp_factor *factor, void *stream);
 
 typedef struct dp_batch_options {
   double threshold;                /* accept a pivot iff |alpha| > threshold */
-  int precision;                   /* DP_PRECISION_FP64 */
+  int precision;                   /* DP_PRECISION_FP64 (the single-matrix semantics and
+                                      records), or DP_PRECISION_MIXED_BF16X3 / _BF16X6: the
+                                      trailing updates A22 -= L21 U12 as BF16 split
+                                      products (3 / 6, FP32 accumulation, on mma.sync
+                                      m16n8k16), panels, U12 solves, searches and pivot
+                                      decisions in FP64; factors for FP64 refinement,
+                                      records may differ where a decision is within the
+                                      update's rounding */
   int nb_bucket[DP_BATCH_BUCKETS]; /* panel width per order bucket, 1..DP_BATCH_MAX_NB */
   int reserved[2];
 } dp_batch_options;
@@ -403,6 +410,11 @@ int dp_gemm_tile(int tile);
  * most g, g < 0 one CTA per -g blocks of 64 rows (at most 32).  Returns the
  * previous setting, or -2000 for a setting outside [-1024, 1024]. */
 int dp_tri_solve_grid(int policy);
+
+/* CTAs of the tensor-core (mixed) update (tuning; no result bit depends on
+ * it): 0 automatic (one per SM, persistent over the tiles), g > 0 at most g,
+ * -1 one per tile.  Returns the previous setting, or -2 for an invalid one. */
+int dp_mixed_gemm_grid(int policy);
 
 /* How the factorisations solve the triangular systems of their outer blocks
  * (U12 = L11^{-1} A12 for blocks wider than 64 rows): 0 automatic (= 1),

@@ -385,3 +385,65 @@ def test_batched_nan_inputs_follow_the_reference_gpu_rule(built):
         assert info[i] == oinfo
         assert np.array_equal(ip[i], oi) and np.array_equal(jp[i], oj)
     assert b.last_report()["near_ties"] == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,bound", [(1, 3e-3), (2, 1e-5)])
+def test_batched_mixed_forms(built, precision, bound):
+    """The mixed forms of the batched launch (BF16 split trailing updates,
+    3 or 6 products with FP32 accumulation; panels, solves and pivot decisions
+    in FP64): relative residual ||PAQ - LU|| / ||A|| at the level of the
+    update's rounding, the same delays as the FP64 form (exact zero columns
+    stay exactly zero), graph replay bitwise equal to the direct launch, and
+    FP64 refinement with the mixed factors reaching 1e-14 on a well-conditioned
+    matrix."""
+    import delayed_pivoting as dp
+    import oracle as orc
+
+    torch = _torch()
+    ns, nz = dp.batch_orders(200, 5150)
+    opt = dp.batch_options(precision=precision)
+    b64, host, fac64, ip64, jp64, info64 = run_batch(ns, nz, 5150)
+    b, host2, fac, ipiv, jpiv, info = run_batch(ns, nz, 5150, options=opt)
+    assert np.array_equal(host, host2)
+    assert np.array_equal(info, info64)
+    _, _, facg, ipg, jpg, infog = run_batch(ns, nz, 5150, options=opt, graph=True)
+    assert np.array_equal(fac, facg) and np.array_equal(ipiv, ipg) and np.array_equal(info, infog)
+    ip = split_records(ipiv, ns)
+    jp = split_records(jpiv, ns)
+    worst = 0.0
+    for i in range(len(ns)):
+        n = int(ns[i])
+        a = matrix_at(host, b.offsets[i], n)
+        f = matrix_at(fac, b.offsets[i], n)
+        r, an = orc.residual(a, f, n, n, int(info[i]), ip[i], jp[i])
+        worst = max(worst, r / an)
+    assert worst <= bound, worst
+    # FP64 refinement with the mixed factors of a full-rank matrix
+    i = int(np.argmax(np.where(info == ns, ns, 0)))
+    n = int(ns[i])
+    a = matrix_at(host, b.offsets[i], n)
+    f = matrix_at(fac, b.offsets[i], n)
+    L = np.tril(f, -1) + np.eye(n)
+    U = np.triu(f)
+
+    def solve(rhs):
+        x = rhs.copy()
+        for k in range(n):  # P: the row swaps in step order
+            x[[k, ip[i][k]]] = x[[ip[i][k], k]]
+        x = np.linalg.solve(U, np.linalg.solve(L, x))
+        for k in range(n - 1, -1, -1):  # Q: the column swaps undone in reverse
+            x[[k, jp[i][k]]] = x[[jp[i][k], k]]
+        return x
+
+    rng = np.random.default_rng(7)
+    xt = rng.standard_normal(n)
+    rhs = a @ xt
+    x = solve(rhs)
+    for _ in range(10):
+        r = rhs - a @ x
+        if np.abs(r).max() / (np.abs(a).max() * np.abs(x).max() * n) <= 1e-16:
+            break
+        x = x + solve(r)
+    berr = np.abs(rhs - a @ x).max() / (np.abs(a).sum(axis=1).max() * np.abs(x).max() + np.abs(rhs).max())
+    assert berr <= 1e-14, berr
