@@ -430,9 +430,11 @@ size_t mixed_scratch_bytes(int max_rows, int max_cols, int max_k, int terms) {
 
 namespace mixed {
 
-// CTAs of the tensor-core update (dp_mixed_gemm_grid): 0 one per SM
-// (persistent over the tiles), g > 0 at most g, -1 one per tile (an SM frees
-// as soon as its tile is done, so a panel waiting for SMs starts sooner).
+// CTAs of the tensor-core update (dp_mixed_gemm_grid): 0 automatic = one
+// per tile (an SM frees as soon as its tile is done, so the panel stream's
+// clusters, waiting for whole SMs, start sooner: a mixed n = 16384 LU took
+// 78.6 ms against 89.1 with one persistent CTA per SM), g > 0 at most g, -1
+// one per SM (persistent over the tiles).
 std::atomic<int> g_grid{0};
 
 template <int TERMS>
@@ -460,7 +462,7 @@ int launch(int M, int N, int K, const double* A, long long lda, const double* B,
       return kLibraryFailure;
   const int tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN);
   const int gp = g_grid.load(std::memory_order_relaxed);
-  const int cap = gp == 0 ? sm_count() : gp < 0 ? tiles : gp;
+  const int cap = gp == 0 ? tiles : gp < 0 ? sm_count() : gp;
   const int grid = std::max(1, std::min(tiles, cap));
   dp::note_launch();
   gemm_bf16x3_kernel<TERMS><<<grid, kThreadsP, smem_bytes<TERMS>(), s>>>(tm, M, N, kp / BK, C, ldc,

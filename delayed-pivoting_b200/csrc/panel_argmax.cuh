@@ -74,6 +74,17 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// D = A B + C on the FP64 tensor path, one 16 x 8 x 4 step (a0 = A(g, t),
+// a1 = A(g + 8, t), b0 = B(t, g); c = C(g, 2t), C(g, 2t + 1), C(g + 8, 2t),
+// C(g + 8, 2t + 1) with g = lane / 4, t = lane % 4).
+__device__ __forceinline__ void mma_f64(double (&c)[4], double a0, double a1, double b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+      "{%0,%1,%2,%3};\n"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a0), "d"(a1), "d"(b0));
+}
+
 // ---- cluster exchange by transaction barriers ------------------------------
 // A CTA expects a known number of bytes per exchange on a barrier in its own
 // shared memory; its peers write them with st.async, each store completing

@@ -509,34 +509,60 @@ __global__ void __launch_bounds__(kT, 1) panel_reg_kernel(PanelParams p) {
       const long long g = first + q;
       if (g >= row0 && g < row0 + rows_here) sm[c * RP + (int)(g - row0)] = S.psave[q * W1 + c];
     }
-    // f. rank-kd update of the rows below the sub-panel's pivots; the next
-    //    sub-panel's first candidate
+    // f. rank-kd update of the rows below the sub-panel's pivots on the FP64
+    //    tensor path (mma.sync.m16n8k4, the kd <= 8 steps as two k4 steps):
+    //    warp w takes rows [32 w + 256 i, + 32) in 16 x 8 tiles over the
+    //    columns [send, w), C read from and written to shared memory; rows
+    //    above the sub-panel's last pivot or beyond the CTA's keep their
+    //    values.  Then the next sub-panel's first candidate.
+    {
+      const double* __restrict__ ps = S.psave;
+      const int g = lane >> 2, t4 = lane & 3;
+      const int lim = (int)max(0LL, min((long long)rows_here, first + kd - row0));
+      const int ncol = w - send;
+#pragma unroll
+      for (int i = 0; i < RPT; ++i)
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+          const int rb = warp * 32 + i * kT + mt * 16;
+          if (rb >= rows_here || rb + 16 <= lim) continue;  // (warp-uniform)
+          const bool ok0 = rb + g < rows_here, ok1 = rb + g + 8 < rows_here;
+          double a[2][2];
+#pragma unroll
+          for (int ks = 0; ks < 2; ++ks) {
+            const int k = 4 * ks + t4;
+            a[ks][0] = (k < kd && ok0) ? -sm[(base + k) * RP + rb + g] : 0.0;
+            a[ks][1] = (k < kd && ok1) ? -sm[(base + k) * RP + rb + g + 8] : 0.0;
+          }
+          const bool st0 = ok0 && rb + g >= lim, st1 = ok1 && rb + g + 8 >= lim;
+          for (int c0 = 0; c0 < ncol; c0 += 8) {
+            double b[2];
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks) {
+              const int k = 4 * ks + t4;
+              b[ks] = (k < kd && c0 + g < ncol) ? ps[k * W1 + send + c0 + g] : 0.0;
+            }
+            const int ca = send + c0 + 2 * t4;  // this lane's columns ca, ca + 1
+            double c[4];
+            c[0] = (ok0 && ca < w) ? sm[ca * RP + rb + g] : 0.0;
+            c[1] = (ok0 && ca + 1 < w) ? sm[(ca + 1) * RP + rb + g] : 0.0;
+            c[2] = (ok1 && ca < w) ? sm[ca * RP + rb + g + 8] : 0.0;
+            c[3] = (ok1 && ca + 1 < w) ? sm[(ca + 1) * RP + rb + g + 8] : 0.0;
+            panel::mma_f64(c, a[0][0], a[0][1], b[0]);
+            panel::mma_f64(c, a[1][0], a[1][1], b[1]);
+            if (st0 && ca < w) sm[ca * RP + rb + g] = c[0];
+            if (st0 && ca + 1 < w) sm[(ca + 1) * RP + rb + g] = c[1];
+            if (st1 && ca < w) sm[ca * RP + rb + g + 8] = c[2];
+            if (st1 && ca + 1 < w) sm[(ca + 1) * RP + rb + g + 8] = c[3];
+          }
+        }
+    }
+    __syncthreads();  // every warp's tiles are stored
     mine = LocalBest{0.0, -1, 0, 0.0};
-    const double* __restrict__ ps = S.psave;
 #pragma unroll
     for (int i = 0; i < RPT; ++i) {
       const int r = tid + i * kT;
-      if (r >= rows_here || row0 + r < first + kd) continue;
-      double* __restrict__ row = sm + r;
-      double l[kS];
-#pragma unroll
-      for (int t = 0; t < kS; ++t) l[t] = t < kd ? row[(base + t) * RP] : 0.0;
-      {
-        double xs = row[send * RP];
-#pragma unroll
-        for (int t = 0; t < kS; ++t)
-          if (t < kd) xs = fma(-l[t], ps[t * W1 + send], xs);
-        row[send * RP] = xs;
-        offer_x(mine, mine_x, xs, r);
-      }
-#pragma unroll 4
-      for (int c = send + 1; c < w; ++c) {
-        double xc = row[c * RP];
-#pragma unroll
-        for (int t = 0; t < kS; ++t)
-          if (t < kd) xc = fma(-l[t], ps[t * W1 + c], xc);
-        row[c * RP] = xc;
-      }
+      if (r < rows_here && row0 + r >= first + kd) offer_x(mine, mine_x, sm[send * RP + r], r);
     }
     __syncthreads();  // the next sub-panel's columns are final in shared memory
     // released to the readers of the next sub-panel end (phase A); the

@@ -76,6 +76,31 @@ __device__ __forceinline__ void atomic_max_pos(double* addr, double v) {
   atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
 }
 
+// Largest max |u_ii| / min |u_ii| of mixed-precision factors kept for
+// refinement (see factor_create).
+constexpr double kMixedPivotRatio = 1e8;
+
+// out[0] = max_i |D(i, i)|, out[1] = min_i |D(i, i)| of the n x n matrix D
+// (out[0] zero and out[1] +inf on entry; NaN reported as +inf in both).
+__global__ void diag_range_kernel(const double* __restrict__ D, long long ldd, int n, double* out) {
+  double hi = 0.0, lo = __longlong_as_double(0x7ff0000000000000ll);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = fabs(D[idx(i, i, ldd)]);
+    hi = (v == v) ? fmax(hi, v) : __longlong_as_double(0x7ff0000000000000ll);
+    lo = (v == v) ? fmin(lo, v) : lo;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    hi = fmax(hi, __shfl_down_sync(0xffffffffu, hi, off));
+    lo = fmin(lo, __shfl_down_sync(0xffffffffu, lo, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_pos(out, hi);
+    atomicMin(reinterpret_cast<unsigned long long*>(out + 1),
+              (unsigned long long)__double_as_longlong(lo));
+  }
+}
+
 // out[c] = max_i |X(i, c)| (out must be zero on entry); NaN is reported as +inf.
 __global__ void colmax_kernel(const double* __restrict__ X, long long ldx, int n, int nrhs,
                               double* out) {
@@ -554,8 +579,37 @@ int factor_create(Factor** out, int n, const double* A, int lda, int precision, 
         cudaStreamSynchronize(st) != cudaSuccess)
       status = kCudaFailure;
   }
-  cudaFreeAsync(normA, st);
   if (status == kOk) status = factorize(*f, A, lda, precision, st);
+  if (status == kOk && f->precision != DP_PRECISION_FP64 && f->info == n) {
+    // Screen of the mixed-precision factors: max |u_ii| / min |u_ii| bounds
+    // kappa(U) from below, and refinement contracts only while kappa times
+    // the factors' error (about 2^-24 for BF16x6) stays well below one; a
+    // ratio beyond kMixedPivotRatio means refinement would stall, so the
+    // factors are replaced by plain FP64 ones before any solve.
+    double range[2] = {0.0, INFINITY};
+    double* scr = nullptr;
+    if (status == kOk &&
+        cudaMallocAsync(reinterpret_cast<void**>(&scr), 2 * sizeof(double), st) != cudaSuccess) {
+      cudaGetLastError();
+      status = kAllocationFailed;
+    }
+    if (status == kOk) {
+      if (cudaMemcpyAsync(scr, range, sizeof(range), cudaMemcpyHostToDevice, st) != cudaSuccess)
+        status = kCudaFailure;
+      dp::note_launch();
+      diag_range_kernel<<<std::min(64, (n + 255) / 256), 256, 0, st>>>(f->lu, n, n, scr);
+      if (status == kOk &&
+          (cudaMemcpyAsync(range, scr, sizeof(range), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+           cudaStreamSynchronize(st) != cudaSuccess))
+        status = kCudaFailure;
+      cudaFreeAsync(scr, st);
+    }
+    if (status == kOk && !(range[0] <= kMixedPivotRatio * range[1])) {
+      f->refactored = 1;
+      status = factorize(*f, A, lda, DP_PRECISION_FP64, st);
+    }
+  }
+  cudaFreeAsync(normA, st);
   if (status != kOk) {
     factor_destroy(f, st);
     return status;

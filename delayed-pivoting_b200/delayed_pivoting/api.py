@@ -418,8 +418,8 @@ def gemm_tile(tile: int) -> int:
 
 
 def mixed_gemm_grid(policy: int) -> int:
-    """dp_mixed_gemm_grid: CTAs of the tensor-core update, 0 one per SM
-    (persistent), g > 0 at most g, -1 one per tile.  Returns the previous setting."""
+    """dp_mixed_gemm_grid: CTAs of the tensor-core update, 0 automatic (one per
+    tile), g > 0 at most g, -1 one per SM (persistent).  Returns the previous setting."""
     return lib().dp_mixed_gemm_grid(int(policy))
 
 

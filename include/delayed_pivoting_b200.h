@@ -176,7 +176,11 @@ int dp_gesv_ir_device(int n, int nrhs, const double *d_a, int lda, double *d_b, 
  * unmodified meanwhile. */
 typedef struct dp_factor dp_factor;
 /* Factor d_a (n x n, device, not modified) at `precision` (DP_PRECISION_*).
- * Synchronises `stream`.  A singular matrix gives a factor with info < n. */
+ * Synchronises `stream`.  A singular matrix gives a factor with info < n.
+ * Mixed-precision factors whose pivot range max |u_ii| / min |u_ii| exceeds
+ * 1e8 (a lower bound on kappa(U) at which refinement from ~2^-24 factors
+ * would stall) are replaced by plain FP64 factors at once (dp_ir_result
+ * .refactored = 1 on its solves). */
 int dp_factor_create(dp_factor **factor, int n, const double *d_a, int lda, int precision,
                      void *stream);
 /* info of the factorisation, precision of the factors held now (a stalled
@@ -406,14 +410,14 @@ int dp_schur_update_mixed_device(int M, int N, int K, const double *A, int lda, 
 int dp_gemm_tile(int tile);
 
 /* CTAs of one triangular-solve launch of the solve / refinement path (tuning;
- * no result bit depends on it): 0 automatic (min(row blocks, 32)), g > 0 at
+ * no result bit depends on it): 0 automatic (min(row blocks, SMs)), g > 0 at
  * most g, g < 0 one CTA per -g blocks of 64 rows (at most 32).  Returns the
  * previous setting, or -2000 for a setting outside [-1024, 1024]. */
 int dp_tri_solve_grid(int policy);
 
 /* CTAs of the tensor-core (mixed) update (tuning; no result bit depends on
- * it): 0 automatic (one per SM, persistent over the tiles), g > 0 at most g,
- * -1 one per tile.  Returns the previous setting, or -2 for an invalid one. */
+ * it): 0 automatic (one per tile), g > 0 at most g, -1 one per SM (persistent
+ * over the tiles).  Returns the previous setting, or -2 for an invalid one. */
 int dp_mixed_gemm_grid(int policy);
 
 /* How the factorisations solve the triangular systems of their outer blocks

@@ -125,3 +125,24 @@ def test_package_exports_every_binding():
     names = re.findall(r"^def ([a-z][a-z0-9_]*)\(", src, re.M)
     assert names
     assert [n for n in names if not hasattr(dp, n)] == []
+
+
+def test_tuning_knobs_validate_and_restore():
+    """The process-wide knobs reject values outside their range (returning the
+    documented error value, leaving the setting unchanged) and return the
+    previous setting; no device work is involved."""
+    import delayed_pivoting as dp
+
+    L = dp.lib()
+    assert dp.block_solve(3) == -1 and dp.block_solve(-1) == -1
+    prev = dp.block_solve(2)
+    assert dp.block_solve(prev) == 2
+    assert dp.mixed_gemm_grid(-2) == -2
+    prev = dp.mixed_gemm_grid(-1)
+    assert dp.mixed_gemm_grid(prev) == -1
+    assert dp.gemm_tile(9) == -1
+    prev = dp.gemm_tile(8)
+    assert dp.gemm_tile(prev) == 8
+    assert L.dp_tri_solve_grid(2000) == -2000
+    prev = L.dp_tri_solve_grid(64)
+    assert L.dp_tri_solve_grid(prev) == 64
