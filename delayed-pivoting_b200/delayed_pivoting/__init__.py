@@ -25,7 +25,7 @@ from .api import (  # noqa: F401
     PRECISION_FP64, PRECISION_MIXED_BF16X3, PRECISION_MIXED_BF16X6, getrf_device_noalloc,
     BATCH_MAX_N, BATCH_MAX_NB, BATCH_BUCKETS, BatchOptions, Batch, BatchError, batch_options,
     batch_autotune, batch_tune_save, batch_tune_load, Factor, Server, ServerOptions, Request,
-    RequestResult, ServerStats, server_options, server_clock, schur_update_device, gemm_tile, block_solve, mixed_gemm_grid,
+    RequestResult, ServerStats, server_options, server_clock, schur_update_device, gemm_tile, block_solve, mixed_gemm_grid, front_factor, extend_add,
     schur_update_mixed_device, GetrfReport, getrf_last_report, getrf_autotune, getrf_tune_save,
     getrf_tune_load,
 )

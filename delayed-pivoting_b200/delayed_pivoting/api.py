@@ -417,6 +417,37 @@ def gemm_tile(tile: int) -> int:
     return lib().dp_gemm_tile(int(tile))
 
 
+def front_factor(m, n, p, d_f, ldf, row_index=None, col_index=None, stream=None):
+    """dp_front_factor: partial delayed LU of a frontal matrix whose leading p
+    rows and columns are fully summed (multifrontal hand-off).  row_index /
+    col_index: int32 arrays of the front's global indices (permuted in place).
+    Returns (status, npiv, ipiv, jpiv); F(npiv:m, npiv:n) is then the
+    contribution block, indexed by row_index[npiv:] and col_index[npiv:]."""
+    L = lib()
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.dp_front_factor.restype = ctypes.c_int
+    L.dp_front_factor.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                  ctypes.c_int, ip, ip, ip, ip, ip, ctypes.c_void_p]
+    ipiv = np.zeros(max(p, 1), dtype=np.int32)
+    jpiv = np.zeros(max(p, 1), dtype=np.int32)
+    k = ctypes.c_int(-1)
+    st = L.dp_front_factor(m, n, p, _dptr(d_f), ldf, _iptr(row_index), _iptr(col_index),
+                           _iptr(ipiv), _iptr(jpiv), ctypes.byref(k), _stream(stream))
+    return st, k.value, ipiv[:p], jpiv[:p]
+
+
+def extend_add(mc, nc, d_c, ldc, d_prow, d_pcol, d_p, ldp, stream=None) -> int:
+    """dp_extend_add: P(prow[i], pcol[j]) += C(i, j) (device arrays; prow /
+    pcol int32 positions in the parent)."""
+    L = lib()
+    vp = ctypes.c_void_p
+    L.dp_extend_add.restype = ctypes.c_int
+    L.dp_extend_add.argtypes = [ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, vp, vp, vp,
+                                ctypes.c_int, vp]
+    return L.dp_extend_add(mc, nc, _dptr(d_c), ldc, _dptr(d_prow), _dptr(d_pcol), _dptr(d_p),
+                           ldp, _stream(stream))
+
+
 def mixed_gemm_grid(policy: int) -> int:
     """dp_mixed_gemm_grid: CTAs of the tensor-core update, 0 automatic (one per
     tile), g > 0 at most g, -1 one per SM (persistent).  Returns the previous setting."""

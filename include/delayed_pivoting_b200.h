@@ -430,6 +430,31 @@ int dp_mixed_gemm_grid(int policy);
  * invalid one. */
 int dp_block_solve(int mode);
 
+/* ---- Multifrontal hand-off (no reference code; the reference's design
+ * document, doc/...LU方法.md:228-457).  A frontal matrix F (m x n, device,
+ * column-major, ldf) whose leading p rows and p columns are fully summed is
+ * factored partially: pivots are chosen inside the fully-summed block only,
+ * with the delayed-pivoting rules of dp_getrf_device on F(0:p, 0:p) (records
+ * ipiv / jpiv: host arrays of p entries, relative to the block; *npiv = k,
+ * its info); the k eliminated pivots' L and U are applied to the whole front,
+ * and F(k:m, k:n) becomes the contribution block for the parent front: the
+ * Schur complement of the k pivots, its first p - k rows and columns the
+ * delayed ones.  row_index / col_index (host, m and n entries, may be NULL):
+ * the front's global row and column indices; their first p entries are
+ * permuted into the factor's order, so row_index[k:m] and col_index[k:n]
+ * index the contribution block.  0 <= p <= min(m, n).  Synchronises
+ * `stream`. */
+int dp_front_factor(int m, int n, int p, double *d_f, int ldf, int *row_index, int *col_index,
+                    int *ipiv, int *jpiv, int *npiv, void *stream);
+/* Extend-add of a child's contribution block into its parent front:
+ * P(prow[i], pcol[j]) += C(i, j) for C (mc x nc, device, ldc); prow / pcol
+ * (device, mc and nc entries) are the positions in the parent of the child's
+ * rows and columns (distinct within one call).  Enqueued on `stream`, does
+ * not synchronise; contributions of several children are ordered by the
+ * stream. */
+int dp_extend_add(int mc, int nc, const double *d_c, int ldc, const int *d_prow,
+                  const int *d_pcol, double *d_p, int ldp, void *stream);
+
 /* delayed_dgetrf_cuda.hpp:63 (delayed_getrf_cuda_status_string). */
 const char *dp_status_string(int status);
 

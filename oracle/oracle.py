@@ -11,6 +11,12 @@ CPU leg of bench.py, never by the product library.
   ``_ref/libref_delayed_lu.so`` by the Makefile beside this file.
 * ``residual`` - ||P A Q - Lbar Ubar||_F and ||A||_F of a compact factor, the
   reconstruction check of delayed_lu_cuda/example.cu:24-80.
+* ``oracle_front`` - the multifrontal hand-off (partial factorisation of a
+  front with p fully-summed rows / columns, contribution block), restated
+  from the reference's design document (doc/...LU方法.md:228-457; the
+  reference has no code for it): the fully-summed block by ``oracle_getrf``,
+  the rest in NumPy.  Only its first step is pinned by the reference; the
+  rest is checked against the Schur-complement identity in the tests.
 * ``_ref/ref_cuda_benchmark`` / ``_ref/ref_cuda_example`` - the reference's own
   GPU build (cuBLAS), and ``_ref/benchmark_on_b200`` / ``_ref/example_on_b200``
   - the same unmodified callers linked against libdelayed_lu_b200.so; see
@@ -116,6 +122,43 @@ def oracle_getrf(a: np.ndarray, m: int | None = None, n: int | None = None, nb: 
                                       ctypes.byref(info), nb, threshold, policy)
     k = min(m, n)
     return ipiv[:k], jpiv[:k], info.value
+
+
+def _composite(rec, size):
+    src = np.arange(size)
+    for k, r in enumerate(rec):
+        src[[k, r]] = src[[r, k]]
+    return src
+
+
+def oracle_front(f: np.ndarray, p: int):
+    """Partial delayed LU of the front `f` (m x n, Fortran float64) whose
+    leading p rows / columns are fully summed; returns (npiv, ipiv, jpiv,
+    out) with `out` the factored front: its first npiv rows / columns L and
+    U, out[npiv:, npiv:] the contribution block (the delayed rows / columns of
+    the fully-summed block first).  Pivots only inside the fully-summed block
+    (delayed_getrf on f[:p, :p]), then its permutations, U12 = L11^-1 F12,
+    L21 = F21 U11^-1 and the Schur updates of the delayed rows / columns and
+    of F22, in the order the device applies them."""
+    m, n = f.shape
+    out = np.array(f, dtype=np.float64, order="F", copy=True)
+    if p == 0:
+        return 0, np.zeros(0, np.int32), np.zeros(0, np.int32), out
+    f11 = np.asfortranarray(out[:p, :p])
+    ipiv, jpiv, k = oracle_getrf(f11, p, p, nb=64)
+    out[:p, :p] = f11
+    rsrc, csrc = _composite(ipiv, p), _composite(jpiv, p)
+    out[:p, p:] = out[rsrc, p:]
+    out[p:, :p] = out[p:, :][:, csrc]
+    if k > 0:
+        L11 = np.tril(out[:k, :k], -1) + np.eye(k)
+        U11 = np.triu(out[:k, :k])
+        out[:k, p:] = np.linalg.solve(L11, out[:k, p:])
+        out[k:p, p:] -= out[k:p, :k] @ out[:k, p:]
+        out[p:, :k] = np.linalg.solve(U11.T, out[p:, :k].T).T
+        out[p:, k:p] -= out[p:, :k] @ out[:k, k:p]
+        out[p:, p:] -= out[p:, :k] @ out[:k, p:]
+    return k, ipiv, jpiv, out
 
 
 def _ref_call(name, a, m, n, threads):
