@@ -113,6 +113,11 @@ void launch_gemm_minus(int M, int N, int K, const double* A, long long lda, cons
                        long long ldb, double* C, long long ldc, cudaStream_t s,
                        const int* gate = nullptr);
 
+// Lower triangle of the symmetric N x N C -= A(N x K) * B(K x N); C's strict
+// upper triangle is not written.
+void launch_gemm_minus_lower(int N, int K, const double* A, long long lda, const double* B,
+                             long long ldb, double* C, long long ldc, cudaStream_t s);
+
 // C(M x N) -= A(M x K) * B(K x N) on the tensor cores (BF16 split into
 // `terms` pieces: 2 -> three products, 3 -> six products; FP32 accumulation in
 // TMEM); scratch of mixed_scratch_bytes(M, N, K, terms) bytes.  Returns a

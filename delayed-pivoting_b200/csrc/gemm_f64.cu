@@ -68,7 +68,7 @@ template <class C>
 __global__ void __launch_bounds__(C::THREADS, C::MINB)
 dgemm_minus_kernel(int M, int N, int K, const double* __restrict__ A, long long lda,
                    const double* __restrict__ B, long long ldb, double* Cm, long long ldc,
-                   const int* gate) {
+                   const int* gate, bool lower) {
   if (gate && *gate >= 0) return;  // an enqueued panel sequence stopped before this update
   extern __shared__ __align__(16) double gsm[];
   double* As = gsm;                         // [STAGES][BK][LDA_S]
@@ -80,6 +80,9 @@ dgemm_minus_kernel(int M, int N, int K, const double* __restrict__ A, long long 
   const int g = lane >> 2, t = lane & 3;
   const long long m0 = (long long)blockIdx.x * C::BM;
   const long long n0 = (long long)blockIdx.y * C::BN;
+  // Lower mode (M == N, C symmetric, its lower triangle only): tiles wholly
+  // above the diagonal have nothing to do.
+  if (lower && m0 + C::BM <= n0) return;
 
   // Prefetch this CTA's C tile into L2 (128-byte lines, in-bounds only).
   {
@@ -187,18 +190,19 @@ dgemm_minus_kernel(int M, int N, int K, const double* __restrict__ A, long long 
       for (int v = 0; v < 4; ++v) {
         const long long r = m0 + wm * C::WTM + mi * 16 + g + 8 * (v >> 1);
         const long long c = n0 + wn * C::WTN + ni * 8 + 2 * t + (v & 1);
-        if (r < M && c < N) Cm[idx(r, c, ldc)] = old[ni][v] - acc[mi][ni][v];
+        if (r < M && c < N && (!lower || r >= c)) Cm[idx(r, c, ldc)] = old[ni][v] - acc[mi][ni][v];
       }
   }
 }
 
 template <class C>
 void launch(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
-            double* Cm, long long ldc, cudaStream_t s, const int* gate) {
+            double* Cm, long long ldc, cudaStream_t s, const int* gate, bool lower = false) {
   dp::ensure_smem((const void*)dgemm_minus_kernel<C>, C::SMEM);
   dim3 grid((M + C::BM - 1) / C::BM, (N + C::BN - 1) / C::BN);
   dp::note_launch();
-  dgemm_minus_kernel<C><<<grid, C::THREADS, C::SMEM, s>>>(M, N, K, A, lda, B, ldb, Cm, ldc, gate);
+  dgemm_minus_kernel<C>
+      <<<grid, C::THREADS, C::SMEM, s>>>(M, N, K, A, lda, B, ldb, Cm, ldc, gate, lower);
 }
 
 // 128 x 128 tiles, 8 warps of 64 x 32, one CTA per SM (212 KB of stages).
@@ -260,6 +264,15 @@ void launch_gemm_minus(int M, int N, int K, const double* A, long long lda, cons
     gemm::launch<gemm::SmallK32>(M, N, K, A, lda, B, ldb, C, ldc, s, gate);
   else
     gemm::launch<gemm::Small4>(M, N, K, A, lda, B, ldb, C, ldc, s, gate);
+}
+
+// Lower triangle of the symmetric N x N block C -= A(N x K) * B(K x N), the
+// strict upper triangle of C untouched (the LDL^T trailing update, where
+// A B = L D L^T is symmetric); 64 x 64 tiles, those above the diagonal exit.
+void launch_gemm_minus_lower(int N, int K, const double* A, long long lda, const double* B,
+                             long long ldb, double* C, long long ldc, cudaStream_t s) {
+  if (N <= 0 || K <= 0) return;
+  gemm::launch<gemm::Small4>(N, N, K, A, lda, B, ldb, C, ldc, s, nullptr, true);
 }
 
 }  // namespace dp

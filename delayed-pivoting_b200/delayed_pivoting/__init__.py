@@ -26,6 +26,7 @@ from .api import (  # noqa: F401
     BATCH_MAX_N, BATCH_MAX_NB, BATCH_BUCKETS, BatchOptions, Batch, BatchError, batch_options,
     batch_autotune, batch_tune_save, batch_tune_load, Factor, Server, ServerOptions, Request,
     RequestResult, ServerStats, server_options, server_clock, schur_update_device, gemm_tile, block_solve, mixed_gemm_grid, front_factor, extend_add,
+    SytrfOptions, sytrf_device, sytrf_host, sytrf_last_report,
     schur_update_mixed_device, GetrfReport, getrf_last_report, getrf_autotune, getrf_tune_save,
     getrf_tune_load,
 )

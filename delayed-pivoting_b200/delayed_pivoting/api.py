@@ -448,6 +448,59 @@ def extend_add(mc, nc, d_c, ldc, d_prow, d_pcol, d_p, ldp, stream=None) -> int:
                            ldp, _stream(stream))
 
 
+class SytrfOptions(ctypes.Structure):
+    """dp_sytrf_options: panel width (0 = 64) and panel-kernel CTAs (0 = automatic)."""
+
+    _fields_ = [("nb", ctypes.c_int), ("grid", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+
+
+def sytrf_device(n, d_a, lda, nb=0, grid=0, stream=None):
+    """dp_sytrf_device_ex: delayed Bunch-Kaufman LDL^T of the symmetric matrix
+    at d_a (device, column-major, lower triangle) in place - the GPU form of
+    the reference's delayed_sytrf_blocked.  Returns (status, perm, piv_size,
+    info)."""
+    L = lib()
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.dp_sytrf_device_ex.restype = ctypes.c_int
+    L.dp_sytrf_device_ex.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ip, ip, ip,
+                                     ctypes.POINTER(SytrfOptions), ctypes.c_void_p]
+    perm = np.zeros(max(n, 1), dtype=np.int32)
+    piv = np.zeros(max(n, 1), dtype=np.int32)
+    info = ctypes.c_int(-1)
+    opt = SytrfOptions(int(nb), int(grid))
+    st = L.dp_sytrf_device_ex(n, _dptr(d_a), lda, _iptr(perm), _iptr(piv), ctypes.byref(info),
+                              ctypes.byref(opt), _stream(stream))
+    return st, perm[:max(n, 0)], piv[:max(n, 0)], info.value
+
+
+def sytrf_host(a):
+    """dp_sytrf_host on a Fortran-ordered float64 array (lda = a.shape[0]),
+    factored in place through the GPU.  Returns (status, perm, piv_size, info)."""
+    assert a.dtype == np.float64 and a.flags.f_contiguous
+    L = lib()
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.dp_sytrf_host.restype = ctypes.c_int
+    L.dp_sytrf_host.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ip, ip, ip]
+    n = a.shape[1]
+    perm = np.zeros(max(n, 1), dtype=np.int32)
+    piv = np.zeros(max(n, 1), dtype=np.int32)
+    info = ctypes.c_int(-1)
+    st = L.dp_sytrf_host(n, a.ctypes.data, a.shape[0], _iptr(perm), _iptr(piv),
+                         ctypes.byref(info))
+    return st, perm[:n], piv[:n], info.value
+
+
+def sytrf_last_report() -> dict:
+    """dp_sytrf_last_report: near-tie report of this thread's last dp_sytrf_* call."""
+    L = lib()
+    L.dp_sytrf_last_report.restype = ctypes.c_int
+    L.dp_sytrf_last_report.argtypes = [ctypes.POINTER(GetrfReport)]
+    r = GetrfReport()
+    if L.dp_sytrf_last_report(ctypes.byref(r)) != SUCCESS:
+        raise RuntimeError("dp_sytrf_last_report failed")
+    return r.as_dict()
+
+
 def mixed_gemm_grid(policy: int) -> int:
     """dp_mixed_gemm_grid: CTAs of the tensor-core update, 0 automatic (one per
     tile), g > 0 at most g, -1 one per SM (persistent).  Returns the previous setting."""

@@ -455,6 +455,43 @@ int dp_front_factor(int m, int n, int p, double *d_f, int ldf, int *row_index, i
 int dp_extend_add(int mc, int nc, const double *d_c, int ldc, const int *d_prow,
                   const int *d_pcol, double *d_p, int ldp, void *stream);
 
+/* ---- Delayed Bunch-Kaufman LDL^T (delayed-bunch-kaufman/delayed_sytrf*.hpp) ----
+ * Symmetric indefinite A (column-major, lda >= n, LOWER triangle read and
+ * written, the strict upper triangle untouched) is factored in place as
+ * P A P^T = L D L^T with Bunch-Kaufman 1x1 / 2x2 pivots (alpha =
+ * (1 + sqrt 17) / 8), nodes whose pivots fail every test delayed to the end:
+ *   perm[pos]     original index at position pos (host, n entries);
+ *   piv_size[pos] 1 (1x1 pivot), 2 (first column of a 2x2 block), 0 (second
+ *                 column of a 2x2 block, or delayed) (host, n entries);
+ *   info          start of the delayed suffix (n when nothing is delayed),
+ *                 -1 on failure;
+ *   L's multipliers below the diagonal (a 2x2 block's start at k + 2), D on
+ *   the diagonal with a 2x2 block's off-diagonal at (k + 1, k), and the
+ *   delayed suffix's trailing block holding its Schur complement.
+ * The records equal the reference's delayed_sytrf_blocked
+ * (delayed_sytrf_blocked.cpp:141) and delayed_sytrf (delayed_sytrf.cpp:175)
+ * wherever no decision is order-sensitive (dp_sytrf_last_report).  NaN never
+ * wins the column search. */
+typedef struct dp_sytrf_options {
+  int nb;    /* panel width, 2..128 (the reference fixes 64); 0 = 64 */
+  int grid;  /* CTAs of the panel kernel; 0 = one per 128 rows, at most one per SM */
+  int reserved[6];
+} dp_sytrf_options;
+
+void dp_sytrf_options_init(dp_sytrf_options *opt);
+/* d_a device memory; synchronises `stream`. */
+int dp_sytrf_device(int n, double *d_a, int lda, int *perm, int *piv_size, int *info,
+                    void *stream);
+int dp_sytrf_device_ex(int n, double *d_a, int lda, int *perm, int *piv_size, int *info,
+                       const dp_sytrf_options *opt, void *stream);
+/* a host memory (copied to the current GPU and back). */
+int dp_sytrf_host(int n, double *a, int lda, int *perm, int *piv_size, int *info);
+/* Near-tie report of the calling thread's last dp_sytrf_* call: decisions
+ * counted, and how many had a comparison (column search runner-up, the three
+ * Bunch-Kaufman tests, the 2x2 determinant test) within a relative
+ * 4 (k + 1) u of flipping. */
+int dp_sytrf_last_report(dp_getrf_report *report);
+
 /* delayed_dgetrf_cuda.hpp:63 (delayed_getrf_cuda_status_string). */
 const char *dp_status_string(int status);
 

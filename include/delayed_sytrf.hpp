@@ -1,0 +1,7 @@
+// Drop-in declaration of the reference's delayed_sytrf (delayed-bunch-kaufman/delayed_sytrf.hpp:15),
+// implemented by libdelayed_lu_b200.so on the current GPU: the same
+// signature and records (perm, piv_size, info), host memory in and out.
+// Invalid arguments and device failures give info = -1.
+#pragma once
+
+void delayed_sytrf(int n, double *a, int lda, int *perm, int *piv_size, int &info);

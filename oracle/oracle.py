@@ -17,6 +17,14 @@ CPU leg of bench.py, never by the product library.
   reference has no code for it): the fully-summed block by ``oracle_getrf``,
   the rest in NumPy.  Only its first step is pinned by the reference; the
   rest is checked against the Schur-complement identity in the tests.
+* ``oracle_sytrf`` - the plain-C restatement (delayed_sytrf_oracle.c) of the
+  blocked delayed Bunch-Kaufman LDL^T
+  (delayed-bunch-kaufman/delayed_sytrf_blocked.cpp:141-358), panel width a
+  parameter; ``ref_sytrf`` - the reference's own ``delayed_sytrf`` /
+  ``delayed_sytrf_blocked`` / ``lapack_sytrf`` compiled into
+  ``_ref/libref_delayed_bk.so``; ``ldl_residual`` - the reconstruction check
+  of delayed-bunch-kaufman/example.cpp:97-160 (P A P^T against L D L^T with
+  the delayed Schur complement as D's trailing block).
 * ``_ref/ref_cuda_benchmark`` / ``_ref/ref_cuda_example`` - the reference's own
   GPU build (cuBLAS), and ``_ref/benchmark_on_b200`` / ``_ref/example_on_b200``
   - the same unmodified callers linked against libdelayed_lu_b200.so; see
@@ -34,9 +42,11 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "liboracle_dp.so"
 REF_SO = HERE / "_ref" / "libref_delayed_lu.so"
+REF_BK_SO = HERE / "_ref" / "libref_delayed_bk.so"
 
 _or = None
 _ref = None
+_refbk = None
 
 
 def build(ref: bool = True) -> None:
@@ -69,6 +79,9 @@ def oracle_lib() -> ctypes.CDLL:
                                       ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _ip(), _ip(),
                                       ctypes.c_void_p, _ip(), _ip(), ctypes.c_void_p]
         L.oracle_max_threads.restype = ctypes.c_int
+        L.oracle_sytrf.restype = ctypes.c_int
+        L.oracle_sytrf.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, _ip(), _ip(),
+                                   ctypes.c_int]
         _or = L
     return _or
 
@@ -237,3 +250,121 @@ def ref_binary(name: str):
     was not built: the reference tree was absent at build time)."""
     p = HERE / "_ref" / name
     return p if p.exists() else None
+
+
+# ----------------------------------------------- delayed Bunch-Kaufman LDL^T
+
+def sym_matrix(n: int, seed: int, lda: int | None = None, zero_nodes=(), zero_diag: bool = False):
+    """A seeded symmetric indefinite test matrix (Fortran, lda >= n): N(0, 1)
+    entries mirrored from the lower triangle; `zero_nodes` rows / columns set to
+    zero (they can only be delayed); `zero_diag` clears the diagonal (every
+    pivot then needs the row test, many become 2x2 blocks)."""
+    lda = n if lda is None else lda
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((n, n))
+    a = np.tril(x) + np.tril(x, -1).T
+    if zero_diag:
+        np.fill_diagonal(a, 0.0)
+    for z in zero_nodes:
+        a[z, :] = 0.0
+        a[:, z] = 0.0
+    out = np.zeros((lda, n), order="F")
+    out[:n, :n] = a
+    return out
+
+
+def rank8_example(n: int = 4096) -> np.ndarray:
+    """The reference's known-answer input (delayed-bunch-kaufman/example.cpp,
+    main): zero except a 2x2 block [[0, 2], [2, 0]] at (2, 3) and the diagonal
+    6, 5, ..., 1 at positions 4..9 - numerical rank 8, so info = 8."""
+    a = np.zeros((n, n), order="F")
+    a[3, 2] = a[2, 3] = 2.0
+    for k in range(6):
+        a[k + 4, k + 4] = float(6 - k)
+    return a
+
+
+def oracle_sytrf(a: np.ndarray, n: int | None = None, nb: int = 64):
+    """Factors `a` (Fortran float64, lda = a.shape[0], lower triangle) in place
+    by the restatement.  Returns (perm, piv_size, info)."""
+    _check(a)
+    n = a.shape[1] if n is None else n
+    perm = np.zeros(max(n, 1), dtype=np.int32)
+    piv = np.zeros(max(n, 1), dtype=np.int32)
+    info = oracle_lib().oracle_sytrf(n, a.ctypes.data, a.shape[0], _p(perm), _p(piv), nb)
+    return perm[:n], piv[:n], info
+
+
+def ref_bk_available() -> bool:
+    return REF_BK_SO.exists()
+
+
+def _refbk_lib() -> ctypes.CDLL:
+    global _refbk
+    if _refbk is None:
+        if not REF_BK_SO.exists():
+            raise RuntimeError(f"reference CPU build missing: {REF_BK_SO}")
+        L = ctypes.CDLL(str(REF_BK_SO))
+        for name in ("ref_delayed_sytrf", "ref_delayed_sytrf_blocked", "ref_lapack_sytrf"):
+            f = getattr(L, name)
+            f.restype = None
+            f.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, _ip(), _ip(), _ip()]
+        L.ref_bk_set_threads.restype = None
+        L.ref_bk_set_threads.argtypes = [ctypes.c_int]
+        _refbk = L
+    return _refbk
+
+
+def ref_sytrf(a: np.ndarray, variant: str = "blocked", threads=None):
+    """The reference's delayed_sytrf_blocked (variant "blocked",
+    delayed_sytrf_blocked.cpp:141), delayed_sytrf ("unblocked",
+    delayed_sytrf.cpp:175) or lapack_sytrf ("lapack", lapack_dsytrf.cpp) on `a`
+    in place.  Returns (perm, piv_size, info)."""
+    _check(a)
+    L = _refbk_lib()
+    if threads is not None:
+        L.ref_bk_set_threads(int(threads))
+    n = a.shape[1]
+    perm = np.zeros(max(n, 1), dtype=np.int32)
+    piv = np.zeros(max(n, 1), dtype=np.int32)
+    info = ctypes.c_int(-1)
+    name = {"blocked": "ref_delayed_sytrf_blocked", "unblocked": "ref_delayed_sytrf",
+            "lapack": "ref_lapack_sytrf"}[variant]
+    getattr(L, name)(n, a.ctypes.data, a.shape[0], _p(perm), _p(piv), ctypes.byref(info))
+    return perm[:n], piv[:n], info.value
+
+
+def ldl_factors(fac: np.ndarray, n: int, piv_size, info: int):
+    """Unit-lower L (n x n, identity on the delayed suffix) and block-diagonal
+    D (1x1 / 2x2 blocks, then the symmetric delayed Schur complement) from a
+    compact factor, as delayed-bunch-kaufman/example.cpp:47-95 reads it."""
+    f = np.asarray(fac)[:n, :n]
+    piv = np.asarray(piv_size)
+    L = np.eye(n)
+    D = np.zeros((n, n))
+    c = 0
+    while c < info:
+        if piv[c] == 2:
+            L[c + 2:, c] = f[c + 2:, c]
+            L[c + 2:, c + 1] = f[c + 2:, c + 1]
+            D[c, c], D[c + 1, c + 1] = f[c, c], f[c + 1, c + 1]
+            D[c + 1, c] = D[c, c + 1] = f[c + 1, c]
+            c += 2
+        else:
+            L[c + 1:, c] = f[c + 1:, c]
+            D[c, c] = f[c, c]
+            c += 1
+    s = np.tril(f[info:, info:])
+    D[info:, info:] = s + np.tril(s, -1).T
+    return L, D
+
+
+def ldl_residual(orig: np.ndarray, fac: np.ndarray, perm, piv_size, info: int) -> float:
+    """max |P A P^T - L D L^T| (example.cpp:146-157), A read from orig's lower
+    triangle."""
+    n = fac.shape[1]
+    a = np.tril(np.asarray(orig)[:n, :n])
+    a = a + np.tril(a, -1).T
+    L, D = ldl_factors(fac, n, piv_size, info)
+    p = np.asarray(perm)
+    return float(np.abs(a[np.ix_(p, p)] - L @ D @ L.T).max()) if n else 0.0

@@ -1,5 +1,6 @@
 /* Declaration-only CBLAS header used to compile the reference CPU sources
- * (delayed_lu/delayed_dgetrf.cpp, delayed_dgetrf_column.cpp, lapack_dgetrf.cpp)
+ * (delayed_lu/delayed_dgetrf.cpp, delayed_dgetrf_column.cpp, lapack_dgetrf.cpp and
+ * delayed-bunch-kaufman/delayed_sytrf.cpp, delayed_sytrf_blocked.cpp, lapack_dsytrf.cpp)
  * unmodified against SciPy's bundled OpenBLAS, whose exported symbols carry a
  * `scipy_` prefix.  Enumerator values are the netlib CBLAS values.  Only the
  * routines that the reference calls are declared.
@@ -25,6 +26,10 @@ typedef CBLAS_ORDER CBLAS_LAYOUT;
 #define cblas_dger scipy_cblas_dger
 #define cblas_dtrsm scipy_cblas_dtrsm
 #define cblas_dgemm scipy_cblas_dgemm
+#define cblas_dgemv scipy_cblas_dgemv
+#define cblas_dsyr scipy_cblas_dsyr
+#define cblas_dsyr2 scipy_cblas_dsyr2
+#define cblas_dsyr2k scipy_cblas_dsyr2k
 
 /* OpenBLAS LP64: blasint == int, CBLAS_INDEX == size_t. */
 unsigned long cblas_idamax(const int n, const double *x, const int incx);
@@ -41,6 +46,18 @@ void cblas_dgemm(CBLAS_ORDER order, CBLAS_TRANSPOSE transa, CBLAS_TRANSPOSE tran
                  const int m, const int n, const int k, const double alpha,
                  const double *a, const int lda, const double *b, const int ldb,
                  const double beta, double *c, const int ldc);
+void cblas_dgemv(CBLAS_ORDER order, CBLAS_TRANSPOSE trans, const int m, const int n,
+                 const double alpha, const double *a, const int lda, const double *x,
+                 const int incx, const double beta, double *y, const int incy);
+void cblas_dsyr(CBLAS_ORDER order, CBLAS_UPLO uplo, const int n, const double alpha,
+                const double *x, const int incx, double *a, const int lda);
+void cblas_dsyr2(CBLAS_ORDER order, CBLAS_UPLO uplo, const int n, const double alpha,
+                 const double *x, const int incx, const double *y, const int incy,
+                 double *a, const int lda);
+void cblas_dsyr2k(CBLAS_ORDER order, CBLAS_UPLO uplo, CBLAS_TRANSPOSE trans, const int n,
+                  const int k, const double alpha, const double *a, const int lda,
+                  const double *b, const int ldb, const double beta, double *c,
+                  const int ldc);
 
 #ifdef __cplusplus
 }
