@@ -1,7 +1,7 @@
 """Benchmark of the B200 delayed-pivoting LU.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload serve|lu|batched]
+                    [--workload serve|lu|batched|ir|stream|update|sytrf]
 
 Workloads (one JSON line on rank 0 each run):
 
@@ -20,6 +20,9 @@ lu  one plain-FP64 delayed_getrf of an n x n N(0,1) matrix with 0.1 % tiny
     GFLOP/s (delayed_lu_cuda/benchmark.cu:67).
 batched  one persistent launch (CUDA graph) factoring 8192 matrices, n
     log-uniform in [32, 512], 0-2 exact-zero columns each; matrices/s.
+sytrf  one delayed Bunch-Kaufman LDL^T (delayed_sytrf_blocked's semantics) of
+    an n x n symmetric N(0,1) matrix, n^3/3 / t in GFLOP/s; the reference arm
+    times the reference's delayed_sytrf_blocked on the host cores.
 
 Inputs are generated once (seeded), kept resident in HBM and restored by a
 device copy before every step, outside the timed region; every step's inputs
@@ -76,10 +79,12 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-lu-key", action="store_true",
                     help="serve: skip the n=16384 plain-LU key of the line")
+    ap.add_argument("--no-sytrf-key", action="store_true",
+                    help="serve: skip the n=16384 LDL^T key of the line")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "mixed3"],
                     help="trailing-update arithmetic of the lu workload: FP64, BF16x6, BF16x3")
     ap.add_argument("--workload", default="serve",
-                    choices=["serve", "lu", "batched", "ir", "stream", "update"])
+                    choices=["serve", "lu", "batched", "ir", "stream", "update", "sytrf"])
     ap.add_argument("--k", type=int, default=256, help="update: inner dimension (outer block)")
     ap.add_argument("--loads", default="0.5,0.7,0.9",
                     help="stream: offered loads as fractions of the measured mixed capacity")
@@ -237,6 +242,8 @@ def run_reference_arm(args):
         return serve_reference_arm(args)
     if args.workload == "batched":
         return batched_reference_arm(args)
+    if args.workload == "sytrf":
+        return sytrf_reference_arm(args)
     if args.workload == "ir":
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no solve or "
                           "refinement path (delayed_getrf factorises only)"}), flush=True)
@@ -281,6 +288,8 @@ def main():
         return run_stream(args)
     if args.workload == "update":
         return run_update(args)
+    if args.workload == "sytrf":
+        return run_sytrf(args)
     return run_lu(args)
 
 
@@ -1012,6 +1021,9 @@ def run_serve(args):
         del pool, rhs
         torch.cuda.empty_cache()
         lu = lu_key(torch, dp, dev, L)
+    sy = None
+    if not args.no_sytrf_key:
+        sy = sytrf_key(torch, dp, dev, cpu=rank == 0 and not args.no_cpu_baseline)
 
     peaks = measured_peaks()
     fam = ["panel", "laswp", "trsm", "gemm", "search", "swap", "other", "gemm_mixed"]
@@ -1052,6 +1064,7 @@ def run_serve(args):
             "clocks": m["clocks"],
             "kernels_mixed_burst": kern,
             "lu_n16384": lu,
+            "sytrf_n16384": sy,
         }
         print(json.dumps(line), flush=True)
     if dist:
@@ -1453,6 +1466,302 @@ def _stats(L):
     L.dp_stats_get(ctypes.byref(s))
     return {"ms": list(s.ms), "flops": list(s.flops), "bytes": list(s.bytes),
             "launches": list(s.launches), "calls": s.calls}
+
+
+
+
+# ---------------------------------------------------------------- sytrf ----
+
+def sytrf_metric(n):
+    return (f"delayed Bunch-Kaufman LDL^T (delayed_sytrf_blocked) GFLOP/s (n^3/3), n={n}, "
+            f"N(0,1) symmetric indefinite")
+
+
+def sytrf_flops(n):
+    return float(n) ** 3 / 3.0
+
+
+def cpu_sytrf_gflops(n, seed, threads):
+    """The reference's delayed_sytrf_blocked (delayed-bunch-kaufman/, compiled
+    into oracle/_ref/) on the host cores; the C restatement ('port') when the
+    reference was not built.  Returns (GFLOP/s, seconds, kind, info)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+    import delayed_pivoting as dp
+
+    a = dp.symmetric_matrix(n, seed)
+    t0 = time.perf_counter()
+    if orc.ref_bk_available():
+        _, _, info = orc.ref_sytrf(a, "blocked", threads=threads)
+        kind = "reference"
+    else:
+        _, _, info = orc.oracle_sytrf(a)
+        kind = "port"
+    t = time.perf_counter() - t0
+    return sytrf_flops(n) / t / 1e9, t, kind, info
+
+
+def sytrf_records_check(dp, n=4096):
+    """Records of the GPU path on the seeded n = 4096 case against the
+    reference's (tests/golden/sytrf/sym_4096.npz, written by the reference's
+    own delayed_sytrf_blocked), with the near-tie report."""
+    import torch
+
+    gold = ROOT / "tests" / "golden" / "sytrf" / f"sym_{n}.npz"
+    a = dp.symmetric_matrix(n, n)
+    d = torch.from_numpy(np.ascontiguousarray(a.T)).cuda()
+    st, perm, piv, info = dp.sytrf_device(n, d, n)
+    rep = dp.sytrf_last_report()
+    out = {"n": n, "status": st, "info": info, "near_tie_report": rep}
+    if gold.exists():
+        with np.load(gold) as z:
+            out["records_match_reference"] = bool(
+                np.array_equal(z["perm"], perm) and np.array_equal(z["piv_size"], piv)
+                and int(z["info"]) == info)
+    del d
+    return out
+
+
+def sytrf_key(torch, dp, dev, n=16384, steps=2, cpu=True):
+    """f4 check carried by the default line: delayed Bunch-Kaufman LDL^T of a
+    seeded n = 16384 symmetric matrix (CUDA events), the records check at
+    n = 4096, and the reference's CPU code on the same n = 4096 case."""
+    stream = torch.cuda.current_stream(dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(n)
+    orig = torch.randn(n, n, dtype=torch.float64, device=dev, generator=g)
+    work = torch.empty_like(orig)
+    ms = []
+    for i in range(steps + 1):
+        work.copy_(orig)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st, _, _, info = dp.sytrf_device(n, work, n, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        if st != 0:
+            raise RuntimeError(f"dp_sytrf_device: status {st}")
+        if i:
+            ms.append(e0.elapsed_time(e1))
+    del orig, work
+    torch.cuda.empty_cache()
+    t = statistics.mean(ms)
+    out = {"n": n, "ms_per_factorisation": t, "gflops": sytrf_flops(n) / (t * 1e-3) / 1e9,
+           "step_ms": [round(x, 3) for x in ms], "info": info,
+           "records_check": sytrf_records_check(dp)}
+    if cpu:
+        threads = os.cpu_count() or 1
+        gc, tc, kind, _ = cpu_sytrf_gflops(4096, 4096, threads)
+        out["cpu_reference_n4096"] = {"gflops": gc, "seconds": tc, "kind": kind,
+                                      "cores": threads}
+    return out
+
+
+def run_sytrf(args):
+    import ctypes
+
+    import torch
+    import delayed_pivoting as dp
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+
+        dist = dist_mod
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+
+    n = args.n
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(args.seed + rank)
+    # column-major storage; only the lower triangle is read
+    orig = torch.randn(n, n, dtype=torch.float64, device=dev, generator=gen)
+    work = torch.empty_like(orig)
+    stream = torch.cuda.current_stream(dev)
+    L = dp.lib()
+    L.dp_stats_families.restype = ctypes.c_uint
+    L.dp_stats_families.argtypes = [ctypes.c_uint]
+
+    def step():
+        work.copy_(orig)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st, _, piv, info = dp.sytrf_device(n, work, n, nb=args.nb, stream=stream)
+        e1.record(stream)
+        if st != 0:
+            raise RuntimeError(f"dp_sytrf_device: status {st}")
+        return e0, e1, info, piv
+
+    L.dp_stats_enable(1)  # warm-up also warms the library's event pool
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    L.dp_stats_enable(0)
+    if dist:
+        dist.barrier()
+    # timed steps record the panel family only (the roofline kernel)
+    L.dp_stats_reset()
+    L.dp_stats_families(1 << 0)
+    L.dp_stats_enable(1)
+    events = []
+    l0 = L.dp_kernel_launches()
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        for _ in range(args.steps):
+            events.append(step())
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    launches = L.dp_kernel_launches() - l0
+    L.dp_stats_enable(0)
+    ms = sum(e0.elapsed_time(e1) for e0, e1, _, _ in events)
+    info, piv = events[-1][2], events[-1][3]
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    stats = _stats(L)
+    L.dp_stats_reset()
+    L.dp_stats_families(0xFFFFFFFF)
+    L.dp_stats_enable(1)
+    step()
+    torch.cuda.synchronize()
+    L.dp_stats_enable(0)
+    fam_stats = _stats(L)
+    L.dp_stats_reset()
+
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+        src = orig.cpu()
+        k = max(1, min(args.steps, 3))
+        e2e_s = 0.0
+        for i in range(k + 1):
+            host.copy_(src)
+            hnp = host.numpy().T  # Fortran view of the pinned buffer
+            t0 = time.perf_counter()
+            st, _, _, _ = dp.sytrf_host(hnp)  # H2D, factorisation, D2H; synchronous
+            if st != 0:
+                raise RuntimeError(f"dp_sytrf_host: status {st}")
+            if i:
+                e2e_s += time.perf_counter() - t0
+        e2e_ms = e2e_s / k * 1e3
+        if dist:
+            t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e = {"value": world * sytrf_flops(n) / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": n * n * 8, "d2h_bytes_per_step": n * n * 8 + 2 * n * 4,
+               "ms_per_step": e2e_ms, "api": "dp_sytrf_host (delayed_sytrf_blocked drop-in)"}
+
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    pl = max(stats["launches"][0], 1)
+    panel_avg_ms = stats["ms"][0] / pl
+    panel_bytes = stats["bytes"][0] / pl
+    achieved = panel_bytes / (panel_avg_ms * 1e-3) / 1e9 if panel_avg_ms > 0 else 0.0
+    roofline = {"bound": "hbm", "kernel": "bk_panel_kernel (cooperative, grid barrier per phase)",
+                "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks.get("hbm_gbs")
+                else "fallback 6650 GB/s (MEASURED_PEAKS.json absent)",
+                "traffic": None, "algorithmic_bytes_per_launch": panel_bytes,
+                "avg_launch_ms": panel_avg_ms, "launches_timed": stats["launches"][0],
+                "note": "latency-bound: every pivot step is 2-3 grid barriers with a decision "
+                        "between them; bytes are 32 per row per factored column"}
+    fp64 = fp64_peak_tflops(torch, dev)
+    value = world * sytrf_flops(n) * args.steps / (ms * 1e-3) / 1e9
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        gc, tc, kind, _ = cpu_sytrf_gflops(args.cpu_n, args.seed, threads)
+        cpu = {"value": gc, "unit": UNIT, "cores": threads, "kind": kind,
+               "sample": f"one delayed_sytrf_blocked of n={args.cpu_n} (seeded N(0,1) symmetric),"
+                         f" {tc:.2f} s, OpenBLAS {threads} threads"}
+        n1 = max(256, args.cpu_n // 2)
+        g1, t1, kind1, _ = cpu_sytrf_gflops(n1, args.seed, 1)
+        cpu["one_thread"] = {"value": g1, "unit": UNIT, "cores": 1, "kind": kind1,
+                             "sample": f"one delayed_sytrf_blocked of n={n1}, {t1:.2f} s"}
+    if rank == 0:
+        fam = ["panel", "laswp", "trsm", "gemm", "search", "swap", "other", "gemm_mixed"]
+        kern = {}
+        fs = fam_stats
+        for i, nm in enumerate(fam):
+            if fs["launches"][i] == 0:
+                continue
+            kern[nm] = {"ms_per_step": fs["ms"][i], "launches_per_step": fs["launches"][i],
+                        "share": fs["ms"][i] / max(ms / args.steps, 1e-9)}
+            if fs["flops"][i]:
+                kern[nm]["tflops"] = fs["flops"][i] / (fs["ms"][i] * 1e-3) / 1e12
+            if fs["bytes"][i]:
+                kern[nm]["gbs"] = fs["bytes"][i] / (fs["ms"][i] * 1e-3) / 1e9
+        upd = kern.get("gemm", {})
+        line = {
+            "metric": sytrf_metric(n), "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: N(0,1) (torch Philox, seeded per rank), lower triangle read",
+            "config": {"workload": f"delayed_sytrf_blocked n={n} (single matrix)", "n": n,
+                       "nb": args.nb or 64, "parallelism": f"replicas x{world}", "info": info,
+                       "pivots_2x2": int((piv == 2).sum()),
+                       "l2": f"input {8 * n * n / 2**30:.2f} GiB " + (
+                           "> L2 (no flush needed)" if 8 * n * n > 126e6 else "<= L2")},
+            "roofline": roofline,
+            "update_roofline": {"bound": "tensor", "kernel": "dgemm_minus_kernel lower (DMMA)",
+                                "achieved": upd.get("tflops"), "peak": fp64, "unit": "TFLOP/s",
+                                "frac": (upd.get("tflops") or 0.0) / fp64 if fp64 else None,
+                                "peak_source": "cuBLAS DGEMM 8192^3 measured live"},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "gpu_launches_per_step": launches / max(args.steps, 1),
+            "step_ms": [round(e0.elapsed_time(e1), 3) for e0, e1, _, _ in events],
+            "clocks": clk.summary(),
+            "kernels": kern,
+            "records_check": sytrf_records_check(dp),
+            "fp64_peak_tflops": fp64,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def sytrf_reference_arm(args):
+    """The reference's own delayed_sytrf_blocked on the host cores, each step a
+    bounded sample (n = --cpu-n) of the n = --n workload, in GFLOP/s (n^3/3)."""
+    threads = os.cpu_count() or 1
+    n = args.cpu_n
+    times, kind = [], None
+    for i in range(args.warmup + args.steps):
+        _, t, kind, _ = cpu_sytrf_gflops(n, args.seed, threads)
+        if i >= args.warmup:
+            times.append(t)
+    tot = sum(times)
+    value = sytrf_flops(n) * len(times) / tot / 1e9
+    line = {
+        "impl": "reference", "metric": sytrf_metric(args.n), "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tot / len(times) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic: N(0,1) PCG64 seeded symmetric",
+        "config": {"workload": f"delayed_sytrf_blocked n={args.n}", "sample_n": n,
+                   "threads": threads},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"one delayed_sytrf_blocked of n={n} per step (bounded sample "
+                                   f"of the n={args.n} workload), OpenBLAS {threads} threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 if __name__ == "__main__":

@@ -33,6 +33,7 @@
 #include "delayed_pivoting_b200.h"
 #include "dp_device.cuh"
 #include "dp_kernels.h"
+#include "dp_stats.h"
 
 namespace dp {
 namespace bk {
@@ -44,7 +45,8 @@ constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
 constexpr int kRowsPerWarp = 8;  // a warp: 8 rows x 4 interleaved groups of panel columns
 constexpr int kRowsPerCta = kWarps * kRowsPerWarp;
-constexpr int kMaxNb = 128;
+constexpr int kMaxNb = 64;  // panel width limit (register-cached L entries)
+constexpr int kPartsPerLane = 5;  // per-CTA partials one lane reduces: grid <= 160 CTAs
 constexpr int kDefaultNb = 64;
 
 // Largest magnitude, runner-up magnitude and the first index of the largest.
@@ -136,15 +138,17 @@ __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
 }
 
 // Grid barrier over a monotonic arrival counter (all CTAs are co-resident:
-// cooperative launch).  The wait is bounded: after kSpinLimitNs the CTA
-// records kDeviceTimeout and the caller returns.
+// cooperative launch): the CTA's writes, ordered before thread 0 by the CTA
+// barrier, are published by its release add; the acquire load that sees
+// every arrival orders the CTA's later reads after all CTAs' writes.  The
+// wait is bounded: after kSpinLimitNs the CTA records kDeviceTimeout and the
+// caller returns.
 __device__ __forceinline__ bool grid_barrier(unsigned int* ctr, unsigned int& target, int* status,
                                              int* s_ok) {
   target += gridDim.x;
   __syncthreads();
   if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(ctr, 1u);
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(ctr) : "memory");
     int ok = 1;
     unsigned long long t0 = 0;
     unsigned int it = 0;
@@ -160,19 +164,24 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* ctr, unsigned int& ta
         }
       }
     }
-    __threadfence();
     *s_ok = ok;
   }
   __syncthreads();
   return *s_ok != 0;
 }
 
-// Closeness of one comparison x >= y of two magnitudes: min / max (1 = tie).
-__device__ __forceinline__ double closeness(double x, double y) {
+// Near-tie bookkeeping of one comparison x >= y of two magnitudes:
+// closeness = min / max (1 = tie); `near` when closeness >= 1 - tol, and
+// `closest` the largest closeness seen.  The division only runs when the
+// ratio can raise `closest`.
+__device__ __forceinline__ void tally(double x, double y, double tol, bool& near,
+                                      double& closest) {
   x = fabs(x);
   y = fabs(y);
   const double hi = fmax(x, y), lo = fmin(x, y);
-  return hi > 0.0 && isfinite(hi) ? lo / hi : 0.0;
+  if (!(hi > 0.0) || !isfinite(hi)) return;
+  if (lo >= (1.0 - tol) * hi) near = true;
+  if (lo > closest * hi) closest = lo / hi;
 }
 
 // stable_2x2 (delayed_sytrf_blocked.cpp:108-124); also returns |det| and the
@@ -189,21 +198,13 @@ __device__ __forceinline__ bool stable_2x2(double a, double b, double c, double&
   return det > thr;
 }
 
-// sum_j L(i, pb + j) * w[j] over the panel's pw columns: lane (q, r) of a
-// warp takes row i = 8-row slice + r and the columns j = q (mod 4); the four
-// partial sums are added by shuffles, so every lane of the row gets the sum.
-__device__ __forceinline__ double panel_dot(const double* a, long long lda, long long i, int n,
-                                            int pb, int pw, const double* s_w, int q) {
-  double s = 0.0;
-  if (i < n) {
-    const double* lp = a + i + (long long)pb * lda;
-#pragma unroll 4
-    for (int j = q; j < pw; j += 4) s = fma(ld(lp + (long long)j * lda), s_w[j], s);
-  }
-  s += __shfl_xor_sync(~0u, s, 8);
-  s += __shfl_xor_sync(~0u, s, 16);
-  return s;
-}
+// Rows of a panel are owned for the whole launch: slot s of CTA b holds the
+// rows pb + (s G + b) 128 + [0, 128), a warp 8 of them; lane (q, r) of a warp
+// serves row r of its 8 and keeps that row's panel columns j = q (mod 4) of
+// L in registers (lr[t] = L(i, pb + q + 4 t)).  The panel products of phases
+// A and B then read one global element per row; a row whose panel entries
+// move (the two rows of a swap) reloads them after the step.
+constexpr int kQ = kMaxNb / 4;  // cached L entries per lane and slot
 
 __device__ __forceinline__ void swap_d(double* x, double* y) {
   const double t = ld(x);
@@ -211,6 +212,67 @@ __device__ __forceinline__ void swap_d(double* x, double* y) {
   *y = t;
 }
 
+// The swap's far parts: rows x, y of the columns < c, and W's rows x, y
+// (WT columns) over the pw panel columns.  A thread's first element of each
+// is loaded before either is stored, so both loads share one round trip.
+__device__ __forceinline__ void swap_far(double* a, long long lda, double* wt, long long ldwt,
+                                         long long x, long long y, long long c, int pw,
+                                         long long gt, long long gstride) {
+  double u0 = 0.0, u1 = 0.0, w0 = 0.0, w1 = 0.0;
+  const bool ha = gt < c, hw = gt < pw;
+  if (ha) {
+    u0 = ld(a + x + gt * lda);
+    u1 = ld(a + y + gt * lda);
+  }
+  if (hw) {
+    w0 = ld(wt + gt + x * ldwt);
+    w1 = ld(wt + gt + y * ldwt);
+  }
+  if (ha) {
+    a[x + gt * lda] = u1;
+    a[y + gt * lda] = u0;
+  }
+  if (hw) {
+    wt[gt + x * ldwt] = w1;
+    wt[gt + y * ldwt] = w0;
+  }
+  for (long long i = gt + gstride; i < c; i += gstride) swap_d(a + x + i * lda, a + y + i * lda);
+}
+
+// sum over the cached panel columns of L(i, :) w, reduced over the row's 4 lanes.
+__device__ __forceinline__ double row_dot(const double (&lr)[kQ], const double* s_w, int q) {
+  double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+  for (int t = 0; t < kQ; t += 2) {
+    s0 = fma(lr[t], s_w[q + 4 * t], s0);
+    s1 = fma(lr[t + 1], s_w[q + 4 * t + 4], s1);
+  }
+  double s = s0 + s1;
+  s += __shfl_xor_sync(~0u, s, 8);
+  s += __shfl_xor_sync(~0u, s, 16);
+  return s;
+}
+
+// lr <- L(i, pb + j) for the lane's columns j < pw (zero beyond).
+__device__ __forceinline__ void load_row(double (&lr)[kQ], const double* a, long long lda,
+                                         long long i, int pb, int pw, int q) {
+#pragma unroll
+  for (int t = 0; t < kQ; ++t) {
+    const int j = q + 4 * t;
+    lr[t] = j < pw ? ld(a + i + (long long)(pb + j) * lda) : 0.0;
+  }
+}
+
+// lr's entry for panel column j <- v, in the lane that caches column j.
+__device__ __forceinline__ void set_entry(double (&lr)[kQ], int q, int j, double v) {
+  if ((j & 3) != q) return;
+  const int tj = j >> 2;
+#pragma unroll
+  for (int t = 0; t < kQ; ++t)
+    if (t == tj) lr[t] = v;
+}
+
+template <int RPT>
 __global__ void __launch_bounds__(kThreads, 1) bk_panel_kernel(Params P, int parity) {
   __shared__ double s_w[kMaxNb];
   __shared__ Top2 s_t[kWarps];
@@ -233,22 +295,39 @@ __global__ void __launch_bounds__(kThreads, 1) bk_panel_kernel(Params P, int par
   int k = st->k, e = st->e;
   const int pb = k;
   int pw = 0;
-  const long long rstride = (long long)G * kRowsPerCta;
   const long long gt = (long long)blockIdx.x * kThreads + tid;
   const long long gstride = (long long)G * kThreads;
   unsigned long long checked = 0, nnear = 0;
   double closest = 0.0;
 
+  long long rowi[RPT];
+  double lr[RPT][kQ], cv[RPT], rv[RPT], av[RPT], a1[RPT];
+#pragma unroll
+  for (int s = 0; s < RPT; ++s) {
+    rowi[s] = pb + ((long long)s * G + blockIdx.x) * kRowsPerCta + warp * kRowsPerWarp + r8;
+    cv[s] = rv[s] = av[s] = a1[s] = 0.0;
+#pragma unroll
+    for (int t = 0; t < kQ; ++t) lr[s][t] = 0.0;
+  }
+  long long rl0 = -1, rl1 = -1;  // rows whose cached entries are reloaded before phase A
+
   while (k < e && pw < P.nb) {
     // ---- phase A: column k of the panel-updated matrix, top-2 below the diagonal
-    for (int j = tid; j < pw; j += kThreads) s_w[j] = ld(P.wt + j + (long long)k * ldwt);
+#pragma unroll
+    for (int s = 0; s < RPT; ++s) {
+      const long long i = rowi[s];
+      av[s] = (i >= k && i < n) ? ld(a + i + (long long)k * lda) : 0.0;
+      if (i == rl0 || i == rl1) load_row(lr[s], a, lda, i, pb, pw, q);
+    }
+    for (int j = tid; j < kMaxNb; j += kThreads) s_w[j] = j < pw ? ld(P.wt + j + (long long)k * ldwt) : 0.0;
     __syncthreads();
     Top2 t{-1.0, -1.0, INT_MAX, 0};
-    for (long long base = k + (long long)blockIdx.x * kRowsPerCta; base < n; base += rstride) {
-      const long long i = base + warp * kRowsPerWarp + r8;
-      const double s = panel_dot(a, lda, i, n, pb, pw, s_w, q);
-      if (q == 0 && i < n) {
-        const double v = ld(a + i + (long long)k * lda) - s;
+#pragma unroll
+    for (int s = 0; s < RPT; ++s) {
+      const double v = av[s] - row_dot(lr[s], s_w, q);
+      cv[s] = v;
+      const long long i = rowi[s];
+      if (q == 0 && i >= k && i < n) {
         P.col[i] = v;
         if (i > k && i < e) consider(t, fabs(v), (int)i);
       }
@@ -264,16 +343,23 @@ __global__ void __launch_bounds__(kThreads, 1) bk_panel_kernel(Params P, int par
     if (!grid_barrier(ctr, target, &st->status, &s_ok)) return;
 
     // ---- phase B: the decision's inputs (every CTA reduces the same partials)
+    const double dkk = ld(P.col + k);  // issued before the partials' loads: one round trip
     if (warp == 0) {
-      Top2 u{-1.0, -1.0, INT_MAX, 0};
-      for (int b = lane; b < G; b += 32) {
-        Top2 c;
-        c.v = ld(&P.cpart[b].v);
-        c.v2 = ld(&P.cpart[b].v2);
-        c.i = __ldcg(&P.cpart[b].i);
-        c.pad = 0;
-        u = merge(u, c);
+      // all of the lane's partials in flight at once (G <= 32 kPartsPerLane)
+      Top2 c[kPartsPerLane];
+#pragma unroll
+      for (int r = 0; r < kPartsPerLane; ++r) {
+        const int b = lane + 32 * r;
+        c[r] = Top2{-1.0, -1.0, INT_MAX, 0};
+        if (b < G) {
+          c[r].v = ld(&P.cpart[b].v);
+          c[r].v2 = ld(&P.cpart[b].v2);
+          c[r].i = __ldcg(&P.cpart[b].i);
+        }
       }
+      Top2 u = c[0];
+#pragma unroll
+      for (int r = 1; r < kPartsPerLane; ++r) u = merge(u, c[r]);
       u = warp_top2(u);
       if (lane == 0) s_best = u;
     }
@@ -289,23 +375,30 @@ __global__ void __launch_bounds__(kThreads, 1) bk_panel_kernel(Params P, int par
         p = k + 1;
       }
     }
-    const double dkk = ld(P.col + k);
     const double akk = fabs(dkk);
     const bool any = fmax(akk, colmax) > 0.0;
     const bool c1 = any && akk >= kAlpha * colmax;
-    double rowmax = 0.0, dpp = 0.0;
+    double rowmax = 0.0, dpp = 0.0, d10 = 0.0, rowk = 0.0, rowk1 = 0.0, colk1 = 0.0;
     if (any && !c1) {
       // candidate row p over [k, n): symmetric A(p, i) - L(i, :) W(p, :)^T
-      __syncthreads();
-      for (int j = tid; j < pw; j += kThreads) s_w[j] = ld(P.wt + j + (long long)p * ldwt);
+      double sy[RPT];
+#pragma unroll
+      for (int s = 0; s < RPT; ++s) {
+        const long long i = rowi[s];
+        sy[s] = (i >= k && i < n) ? (i <= p ? ld(a + p + i * lda) : ld(a + i + (long long)p * lda))
+                                  : 0.0;
+        // A(i, k + 1): the old values a 2x2 step's swap relocates
+        a1[s] = (i > k && i < n) ? ld(a + i + (long long)(k + 1) * lda) : 0.0;
+      }
+      for (int j = tid; j < kMaxNb; j += kThreads) s_w[j] = j < pw ? ld(P.wt + j + (long long)p * ldwt) : 0.0;
       __syncthreads();
       double m = 0.0;
-      for (long long base = k + (long long)blockIdx.x * kRowsPerCta; base < n; base += rstride) {
-        const long long i = base + warp * kRowsPerWarp + r8;
-        const double s = panel_dot(a, lda, i, n, pb, pw, s_w, q);
-        if (q == 0 && i < n) {
-          const double sym = i <= p ? ld(a + p + i * lda) : ld(a + i + (long long)p * lda);
-          const double v = sym - s;
+#pragma unroll
+      for (int s = 0; s < RPT; ++s) {
+        const double v = sy[s] - row_dot(lr[s], s_w, q);
+        rv[s] = v;
+        const long long i = rowi[s];
+        if (q == 0 && i >= k && i < n) {
           P.row[i] = v;
           if (i < e && i != p) m = fmax(m, fabs(v));
         }
@@ -319,53 +412,67 @@ __global__ void __launch_bounds__(kThreads, 1) bk_panel_kernel(Params P, int par
         if (lane == 0) P.rpart[blockIdx.x] = u;
       }
       if (!grid_barrier(ctr, target, &st->status, &s_ok)) return;
+      // every value the decision and phase C read from other rows, issued
+      // with the partials' loads: one round trip
+      dpp = ld(P.row + p);
+      d10 = ld(P.col + p);
+      rowk = ld(P.row + k);
+      if (k + 1 < n) {
+        rowk1 = ld(P.row + k + 1);
+        colk1 = ld(P.col + k + 1);
+      }
       if (warp == 0) {
-        double u = 0.0;
-        for (int b = lane; b < G; b += 32) u = fmax(u, ld(P.rpart + b));
+        double c[kPartsPerLane];
+#pragma unroll
+        for (int r = 0; r < kPartsPerLane; ++r)
+          c[r] = lane + 32 * r < G ? ld(P.rpart + lane + 32 * r) : 0.0;
+        double u = c[0];
+#pragma unroll
+        for (int r = 1; r < kPartsPerLane; ++r) u = fmax(u, c[r]);
         u = warp_max(u);
         if (lane == 0) s_rowmax = u;
       }
       __syncthreads();
       rowmax = s_rowmax;
-      dpp = ld(P.row + p);
     }
 
     // ---- the decision (delayed_sytrf_blocked.cpp:192-235), identical in every CTA
     const double app = fabs(dpp);
     const double tol = 4.0 * (double)(k + 1) * kUnit;
-    double close = (best.v2 >= 0.0 && best.v > 0.0) ? closeness(best.v2, best.v) : 0.0;
+    bool near = false;
+    if (best.v2 >= 0.0) tally(best.v2, best.v, tol, near, closest);
     int kind = kDelay;
-    double d10 = 0.0, det = 0.0, thr = 0.0;
+    double det = 0.0, thr = 0.0;
     if (any) {
-      close = fmax(close, closeness(akk, kAlpha * colmax));
+      tally(akk, kAlpha * colmax, tol, near, closest);
       if (c1) {
         kind = kOne;
       } else {
         const double c2r = kAlpha * colmax * (colmax / rowmax);
-        close = fmax(close, closeness(akk, c2r));
+        tally(akk, c2r, tol, near, closest);
         if (akk >= c2r) {
           kind = kOne;
         } else {
-          close = fmax(close, closeness(app, kAlpha * rowmax));
+          tally(app, kAlpha * rowmax, tol, near, closest);
           if (app >= kAlpha * rowmax) {
             kind = kOneSwap;
           } else {
-            d10 = ld(P.col + p);
             const bool ok2 = stable_2x2(dkk, d10, dpp, det, thr);
-            close = fmax(close, closeness(det, thr));
+            tally(det, thr, tol, near, closest);
             if (ok2) kind = pw + 2 > P.nb ? kBreak : kTwo;
           }
         }
       }
     }
-    if (blockIdx.x == 0 && tid == 0 && kind != kBreak) {
+    if (kind != kBreak) {  // counted by thread 0 of CTA 0; every thread tracks `closest`
       ++checked;
-      if (close >= 1.0 - tol) ++nnear;
-      closest = fmax(closest, close);
+      if (near) ++nnear;
     }
     if (kind == kBreak) break;  // the 2x2 block starts the next panel (:245-248)
 
-    // ---- phase C: swap and new columns in one pass over the rows
+    // ---- phase C: the swap's far parts (columns < k) over all threads, the
+    // new column(s) by the rows' owners from their own materialised values
+    rl0 = rl1 = -1;
     if (kind == kDelay) {
       const int x = k, y = e - 1;
       if (x != y) {
@@ -373,49 +480,75 @@ __global__ void __launch_bounds__(kThreads, 1) bk_panel_kernel(Params P, int par
           if (i < x) swap_d(a + x + i * lda, a + y + i * lda);
           else if (i == x) swap_d(a + x + (long long)x * lda, a + y + (long long)y * lda);
           else if (i < y) swap_d(a + i + (long long)x * lda, a + y + i * lda);
-          else if (i == y) { const int t0 = P.perm[x]; P.perm[x] = P.perm[y]; P.perm[y] = t0; }
-          else swap_d(a + i + (long long)x * lda, a + i + (long long)y * lda);
+          else if (i > y) swap_d(a + i + (long long)x * lda, a + i + (long long)y * lda);
+        }
+        if (gt == gstride - 1) {
+          const int t0 = P.perm[x];
+          P.perm[x] = P.perm[y];
+          P.perm[y] = t0;
         }
         for (long long j = gt; j < pw; j += gstride) swap_d(P.wt + j + x * ldwt, P.wt + j + y * ldwt);
+        rl0 = x;
+        rl1 = y;
       }
       e -= 1;
     } else if (kind == kOne) {
       const double d = dkk;
-      for (long long i = gt + k; i < n; i += gstride) {
+      if (gt == 0) P.piv[k] = 1;
+#pragma unroll
+      for (int s = 0; s < RPT; ++s) {
+        const long long i = rowi[s];
+        if (i < k || i >= n) continue;
         if (i == k) {
-          a[i + i * lda] = d;
-          P.wt[pw + i * ldwt] = d;
-          P.piv[k] = 1;
+          if (q == 0) {
+            a[i + i * lda] = d;
+            P.wt[pw + i * ldwt] = d;
+          }
         } else {
-          const double c = ld(P.col + i);
-          a[i + (long long)k * lda] = c / d;
-          P.wt[pw + i * ldwt] = c;
+          const double l = cv[s] / d;
+          if (q == 0) {
+            a[i + (long long)k * lda] = l;
+            P.wt[pw + i * ldwt] = cv[s];
+          }
+          set_entry(lr[s], q, pw, l);
         }
       }
       k += 1;
       pw += 1;
     } else if (kind == kOneSwap) {  // x = k, y = p: column k is rebuilt from `row`
+      // owned rows first (the old A(i, k) the swap relocates is phase A's av),
+      // then the swap's columns < k and W's rows
       const double d = dpp;
-      for (long long i = gt; i < n; i += gstride) {
-        if (i < k) {
-          swap_d(a + k + i * lda, a + p + i * lda);
-        } else if (i == k) {
-          a[p + (long long)p * lda] = ld(a + k + (long long)k * lda);
-          a[k + (long long)k * lda] = d;
-          P.wt[pw + i * ldwt] = d;
-          P.piv[k] = 1;
-          const int t0 = P.perm[k];
-          P.perm[k] = P.perm[p];
-          P.perm[p] = t0;
+      if (gt == gstride - 1) {  // a thread with no column of the swap below (unless n > 512 G)
+        P.piv[k] = 1;
+        const int t0 = P.perm[k];
+        P.perm[k] = P.perm[p];
+        P.perm[p] = t0;
+      }
+#pragma unroll
+      for (int s = 0; s < RPT; ++s) {
+        const long long i = rowi[s];
+        if (i < k || i >= n) continue;
+        if (i == k) {
+          if (q == 0) {
+            a[p + (long long)p * lda] = av[s];
+            a[k + (long long)k * lda] = d;
+            P.wt[pw + i * ldwt] = d;
+          }
         } else {
-          const double b = i == p ? ld(P.row + k) : ld(P.row + i);
-          if (i < p) a[p + i * lda] = ld(a + i + (long long)k * lda);
-          else if (i > p) a[i + (long long)p * lda] = ld(a + i + (long long)k * lda);
-          a[i + (long long)k * lda] = b / d;
-          P.wt[pw + i * ldwt] = b;
+          const double b = i == p ? rowk : rv[s];
+          const double l = b / d;
+          if (q == 0) {
+            if (i < p) a[p + i * lda] = av[s];
+            else if (i > p) a[i + (long long)p * lda] = av[s];
+            a[i + (long long)k * lda] = l;
+            P.wt[pw + i * ldwt] = b;
+          }
+          set_entry(lr[s], q, pw, l);
         }
       }
-      for (long long j = gt; j < pw; j += gstride) swap_d(P.wt + j + k * ldwt, P.wt + j + p * ldwt);
+      swap_far(a, lda, P.wt, ldwt, k, p, k, pw, gt, gstride);
+      rl0 = p;
       k += 1;
       pw += 1;
     } else {  // kTwo: x = k + 1, y = p; columns k, k + 1 from `col`, `row`
@@ -425,41 +558,56 @@ __global__ void __launch_bounds__(kThreads, 1) bk_panel_kernel(Params P, int par
       const double s00 = d00 / sc, s10 = d10 / sc, s11 = d11 / sc;
       const double inv = 1.0 / (sc * (s00 * s11 - s10 * s10));
       const long long k1 = k + 1;
-      for (long long i = gt; i < n; i += gstride) {
-        if (i < k) {
-          if (sw) swap_d(a + k1 + i * lda, a + p + i * lda);
-        } else if (i == k) {
-          a[k + (long long)k * lda] = d00;
-          a[k1 + (long long)k * lda] = d10;
-          P.wt[pw + i * ldwt] = d00;
-          P.wt[pw + 1 + i * ldwt] = d10;
-          P.piv[k] = 2;
-          P.piv[k1] = 0;
-        } else if (i == k1) {
-          if (sw) {
-            a[p + (long long)p * lda] = ld(a + k1 + k1 * lda);
-            const int t0 = P.perm[k1];
-            P.perm[k1] = P.perm[p];
-            P.perm[p] = t0;
-          }
-          a[k1 + k1 * lda] = d11;
-          P.wt[pw + i * ldwt] = d10;
-          P.wt[pw + 1 + i * ldwt] = d11;
-        } else {
-          const long long src = (sw && i == p) ? k1 : i;
-          const double b0 = ld(P.col + src), b1 = ld(P.row + src);
-          if (sw) {
-            if (i < p) a[p + i * lda] = ld(a + i + k1 * lda);
-            else if (i > p) a[i + (long long)p * lda] = ld(a + i + k1 * lda);
-          }
-          a[i + (long long)k * lda] = (s11 * b0 - s10 * b1) * inv;
-          a[i + k1 * lda] = (s00 * b1 - s10 * b0) * inv;
-          P.wt[pw + i * ldwt] = b0;
-          P.wt[pw + 1 + i * ldwt] = b1;
+      if (gt == gstride - 1) {
+        P.piv[k] = 2;
+        P.piv[k1] = 0;
+        if (sw) {
+          const int t0 = P.perm[k1];
+          P.perm[k1] = P.perm[p];
+          P.perm[p] = t0;
         }
       }
-      if (sw)
-        for (long long j = gt; j < pw; j += gstride) swap_d(P.wt + j + k1 * ldwt, P.wt + j + p * ldwt);
+#pragma unroll
+      for (int s = 0; s < RPT; ++s) {
+        const long long i = rowi[s];
+        if (i < k || i >= n) continue;
+        if (i == k) {
+          if (q == 0) {
+            a[k + (long long)k * lda] = d00;
+            a[k1 + (long long)k * lda] = d10;
+            P.wt[pw + i * ldwt] = d00;
+            P.wt[pw + 1 + i * ldwt] = d10;
+          }
+        } else if (i == k1) {
+          if (q == 0) {
+            if (sw) a[p + (long long)p * lda] = a1[s];  // old A(k + 1, k + 1)
+            a[k1 + k1 * lda] = d11;
+            P.wt[pw + i * ldwt] = d10;
+            P.wt[pw + 1 + i * ldwt] = d11;
+          }
+        } else {
+          const bool moved = sw && i == p;
+          const double b0 = moved ? colk1 : cv[s], b1 = moved ? rowk1 : rv[s];
+          const double l0 = (s11 * b0 - s10 * b1) * inv;
+          const double l1 = (s00 * b1 - s10 * b0) * inv;
+          if (q == 0) {
+            if (sw) {  // old A(i, k + 1), loaded with the row
+              if (i < p) a[p + i * lda] = a1[s];
+              else if (i > p) a[i + (long long)p * lda] = a1[s];
+            }
+            a[i + (long long)k * lda] = l0;
+            a[i + k1 * lda] = l1;
+            P.wt[pw + i * ldwt] = b0;
+            P.wt[pw + 1 + i * ldwt] = b1;
+          }
+          set_entry(lr[s], q, pw, l0);
+          set_entry(lr[s], q, pw + 1, l1);
+        }
+      }
+      if (sw) {
+        swap_far(a, lda, P.wt, ldwt, k1, p, k, pw, gt, gstride);
+        rl0 = p;
+      }
       k += 2;
       pw += 2;
     }
@@ -475,6 +623,19 @@ __global__ void __launch_bounds__(kThreads, 1) bk_panel_kernel(Params P, int par
     st->closest = fmax(st->closest, closest);
   }
 }
+
+// Kernel instance for RPT rows per lane (slots), nullptr beyond kMaxSlots.
+constexpr int kMaxSlots = 4;
+const void* panel_kernel_for(int slots) {
+  switch (slots) {
+    case 1: return (const void*)bk_panel_kernel<1>;
+    case 2: return (const void*)bk_panel_kernel<2>;
+    case 3:
+    case 4: return (const void*)bk_panel_kernel<4>;
+    default: return nullptr;
+  }
+}
+
 
 __global__ void bk_init_kernel(int n, int* perm, int* piv, State* st) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -505,13 +666,16 @@ int panel_ctas_max() {
   int sms = 0, coop = 0, per = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-  if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bk::bk_panel_kernel,
+  if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bk::bk_panel_kernel<4>,
                                                               bk::kThreads, 0) != cudaSuccess)
     return 0;
   return per > 0 ? sms : 0;
 }
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// Mean panel columns in the products of a launch that factored w columns.
+double pw_avg_dot(int w) { return w > 0 ? 0.5 * (w - 1) : 0.0; }
 
 }  // namespace
 
@@ -532,7 +696,9 @@ int sytrf_device(int n, double* d_a, int lda, int* perm, int* piv_size, int* inf
   const int gmax = panel_ctas_max();
   if (gmax <= 0) return kCudaFailure;
   int G = grid > 0 ? grid : (n + bk::kRowsPerCta - 1) / bk::kRowsPerCta;
-  G = std::max(1, std::min(G, gmax));
+  G = std::max(1, std::min({G, gmax, 32 * bk::kPartsPerLane}));
+  // each lane caches the panel rows of at most kMaxSlots slots of 128 rows per CTA
+  if ((long long)n > (long long)G * bk::kRowsPerCta * bk::kMaxSlots) return kInvalidArgument;
 
   const size_t b_wt = align256((size_t)nb * n * sizeof(double));
   const size_t b_vec = align256((size_t)n * sizeof(double));
@@ -572,19 +738,32 @@ int sytrf_device(int n, double* d_a, int lda, int* perm, int* piv_size, int* inf
   P.nb = nb;
 
   int status = kOk;
+  // dp_stats families: panel launches, the lower DMMA updates, the record init
+  Recorder rec(s);
+  rec.begin(DP_KFAM_OTHER);
   note_launch();
   bk::bk_init_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, P.perm, P.piv, P.st);
+  rec.end(0.0, 8.0 * n + sizeof(bk::State), 1);
   if (cudaGetLastError() != cudaSuccess) status = kCudaFailure;
   int pb = 0, e = n, parity = 0;
   while (status == kOk) {
     void* args[] = {(void*)&P, (void*)&parity};
     note_launch();
-    if (cudaLaunchCooperativeKernel((const void*)bk::bk_panel_kernel, dim3(G), dim3(bk::kThreads),
-                                    args, 0, s) != cudaSuccess ||
+    rec.begin(DP_KFAM_PANEL);
+    const long long per_slot = (long long)G * bk::kRowsPerCta;
+    const int slots = (int)((n - pb + per_slot - 1) / per_slot);
+    if (cudaLaunchCooperativeKernel(bk::panel_kernel_for(slots), dim3(G), dim3(bk::kThreads), args,
+                                    0, s) != cudaSuccess ||
         cudaMemcpyAsync(h, P.st, sizeof(bk::State), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess) {
       status = kCudaFailure;
       break;
+    }
+    {
+      // algorithmic traffic of the launch: per factored column the column and
+      // row reads and the L and W column writes over the rows below pb
+      const double w = (double)(h->k - pb), rows = (double)(n - pb);
+      rec.end(4.0 * w * rows * pw_avg_dot(h->k - pb), 32.0 * w * rows, 1);
     }
     if (h->status != kOk) {
       status = h->status;
@@ -597,9 +776,14 @@ int sytrf_device(int n, double* d_a, int lda, int* perm, int* piv_size, int* inf
     }
     e = h->e;
     // finish_panel: the trailing block [k, n), delayed suffix included
-    if (k > pb && k < n)
+    if (k > pb && k < n) {
+      const double t = (double)(n - k), w = (double)(k - pb);
+      rec.begin(DP_KFAM_GEMM);
       launch_gemm_minus_lower(n - k, k - pb, d_a + k + (long long)pb * lda, lda,
                               P.wt + (long long)k * nb, nb, d_a + k + (long long)k * lda, lda, s);
+      // lower triangle: t (t + 1) w flops; C read and written once, L and W read
+      rec.end(t * (t + 1.0) * w, 8.0 * t * (t + 1.0) + 16.0 * t * w, 1);
+    }
     pb = k;
     parity ^= 1;
     if (k >= e) break;
@@ -612,6 +796,7 @@ int sytrf_device(int n, double* d_a, int lda, int* perm, int* piv_size, int* inf
     status = kCudaFailure;
   cudaFreeAsync(ws, s);
   if (cudaStreamSynchronize(s) != cudaSuccess && status == kOk) status = kCudaFailure;
+  rec.flush(status == kOk);
   if (status == kOk) {
     *info = e;
     g_bk_report.decisions = (long long)h->checked;

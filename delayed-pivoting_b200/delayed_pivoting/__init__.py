@@ -32,5 +32,5 @@ from .api import (  # noqa: F401
 )
 from .inputs import (  # noqa: F401
     normal_matrix, plant_columns, mt64_nth, planted_matrix, uniform_stream, normal_vector,
-    batch_orders, batch_matrix_seed, fill_batch, batch_matrix,
+    batch_orders, batch_matrix_seed, fill_batch, batch_matrix, symmetric_matrix,
 )

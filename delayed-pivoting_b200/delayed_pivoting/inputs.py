@@ -97,3 +97,22 @@ def batch_matrix(ns, n_zero, seed: int, i: int) -> np.ndarray:
     """Matrix i of fill_batch as an (n x n) Fortran array."""
     n = int(ns[i])
     return planted_matrix(n, n, batch_matrix_seed(seed, i), 0, int(n_zero[i]))
+
+
+def symmetric_matrix(n: int, seed: int, lda: int | None = None, zero_nodes=(),
+                     zero_diag: bool = False) -> np.ndarray:
+    """Seeded symmetric indefinite matrix for the LDL^T path (Fortran, lda >=
+    n): N(0, 1) entries of NumPy's PCG64 stream (default_rng(seed)), the lower
+    triangle mirrored to the upper; `zero_nodes` rows / columns cleared (they
+    can only be delayed), `zero_diag` clears the diagonal."""
+    lda = n if lda is None else lda
+    x = np.random.default_rng(seed).standard_normal((n, n))
+    a = np.tril(x) + np.tril(x, -1).T
+    if zero_diag:
+        np.fill_diagonal(a, 0.0)
+    for z in zero_nodes:
+        a[z, :] = 0.0
+        a[:, z] = 0.0
+    out = np.zeros((lda, n), order="F")
+    out[:n, :n] = a
+    return out

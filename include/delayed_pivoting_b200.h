@@ -473,8 +473,9 @@ int dp_extend_add(int mc, int nc, const double *d_c, int ldc, const int *d_prow,
  * wherever no decision is order-sensitive (dp_sytrf_last_report).  NaN never
  * wins the column search. */
 typedef struct dp_sytrf_options {
-  int nb;    /* panel width, 2..128 (the reference fixes 64); 0 = 64 */
-  int grid;  /* CTAs of the panel kernel; 0 = one per 128 rows, at most one per SM */
+  int nb;    /* panel width, 2..64 (the reference fixes 64); 0 = 64 */
+  int grid;  /* CTAs of the panel kernel; 0 = one per 128 rows, at most one per SM.
+                n may not exceed 512 rows per CTA (75776 with one CTA per SM). */
   int reserved[6];
 } dp_sytrf_options;
 

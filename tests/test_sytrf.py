@@ -29,6 +29,17 @@ def load(name):
     return a, g
 
 
+def test_package_generator_equals_oracle_generator():
+    """bench.py builds its inputs with the package's generator, the fixtures
+    with the oracle's: the two recipes must agree bit for bit."""
+    import delayed_pivoting as dp
+
+    for n, seed, lda, z, zd in ((7, 1, 7, (), False), (333, 7, 340, (40,), False),
+                                (257, 6, 257, (0, 1, 2), True), (4096, 4096, 4096, (), False)):
+        np.testing.assert_array_equal(dp.symmetric_matrix(n, seed, lda, z, zd),
+                                      orc.sym_matrix(n, seed, lda, z, zd))
+
+
 def test_fixtures_present():
     assert len(CASES) >= 15
     assert "rank8_4096" in CASES and "sym_4096" in CASES
@@ -106,7 +117,7 @@ def test_c_abi_argument_checks_need_no_device():
     assert L.dp_sytrf_device(4, 0x1000, 3, P, Q, ctypes.byref(info), None) == dp.INVALID_ARGUMENT
     assert L.dp_sytrf_device(4, None, 4, P, Q, ctypes.byref(info), None) == dp.INVALID_ARGUMENT
     assert L.dp_sytrf_device(4, 0x1000, 4, None, Q, ctypes.byref(info), None) == dp.INVALID_ARGUMENT
-    for nb in (1, 129, -5):
+    for nb in (1, 65, -5):
         st, *_ = dp.sytrf_device(4, 0x1000, 4, nb=nb)
         assert st == dp.INVALID_ARGUMENT
     assert dp.sytrf_device(4, 0x1000, 4, grid=-1)[0] == dp.INVALID_ARGUMENT
@@ -168,14 +179,27 @@ def test_gpu_records_match_reference(built, name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("nb,grid", [(2, 0), (3, 1), (17, 2), (64, 5), (128, 0), (64, 148)])
+@pytest.mark.parametrize("nb,grid", [(2, 0), (3, 4), (17, 8), (64, 5), (48, 0), (64, 148),
+                                     (64, 16)])
 def test_gpu_panel_width_and_grid_keep_records(built, nb, grid):
+    """Panel widths 2..64 and CTA counts giving 1, 2 and 4 cached 128-row
+    slots per CTA (grid 16, 8, 4 on n = 2048) keep the records."""
     a, g = load("sym_2048_zero8")
     st, perm, piv, info, f, rep = _gpu_factor(a, nb=nb, grid=grid)
     assert st == 0 and rep["near_ties"] == 0
     assert info == int(g["info"])
     np.testing.assert_array_equal(perm, g["perm"])
     np.testing.assert_array_equal(piv, g["piv_size"])
+
+
+@pytest.mark.gpu
+def test_gpu_rejects_grid_too_small_for_n(built):
+    import delayed_pivoting as dp
+
+    torch = _torch()
+    d = torch.zeros(600, 600, dtype=torch.float64, device="cuda")
+    assert dp.sytrf_device(600, d, 600, grid=1)[0] == dp.INVALID_ARGUMENT  # > 512 rows per CTA
+    assert dp.sytrf_device(600, d, 600, grid=2)[0] == dp.SUCCESS
 
 
 @pytest.mark.gpu
