@@ -53,7 +53,7 @@ def build(ref: bool = True) -> None:
     """Compiles the oracle (and, when the reference tree exists, the reference)."""
     targets = ["oracle"]
     if ref and Path(os.environ.get("DP_REFERENCE", "/root/reference")).exists():
-        targets += ["ref", "refgpu"]
+        targets += ["ref", "refgpu", "refbk"]
     env = dict(os.environ)
     if "DP_REFERENCE" in os.environ:
         env["REF"] = os.environ["DP_REFERENCE"]

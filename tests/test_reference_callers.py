@@ -64,3 +64,39 @@ def test_reference_own_cuda_example_on_b200():
                        timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "FAIL" not in r.stdout
+
+
+# ---- delayed Bunch-Kaufman: delayed-bunch-kaufman/example.cpp, unmodified ----
+
+PASS_LINE = "总体比较结果：通过"  # the caller's own "overall comparison: pass" line
+
+
+def test_bk_caller_links_this_library():
+    """The reference's LDL^T caller, built against include/delayed_sytrf*.hpp,
+    takes delayed_sytrf and delayed_sytrf_blocked from libdelayed_lu_b200.so
+    (lapack_sytrf, the caller's comparison, from the reference's source)."""
+    p = _binary("bk_example_on_b200")
+    ldd = subprocess.run(["ldd", str(p)], capture_output=True, text=True).stdout
+    assert "libdelayed_lu_b200.so" in ldd and "not found" not in ldd
+    undef = subprocess.run(["nm", "-D", "--undefined-only", str(p)], capture_output=True,
+                           text=True).stdout
+    assert "_Z13delayed_sytrfiPdiPiS0_Ri" in undef
+    assert "_Z21delayed_sytrf_blockediPdiPiS0_Ri" in undef
+
+
+def test_bk_caller_passes_on_the_reference():
+    """The same caller on the reference's CPU sources: its rank-8 known answer
+    (info 8 for both delayed variants, reconstruction within 100 u rank)."""
+    r = subprocess.run([str(_binary("bk_example_ref"))], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0 and PASS_LINE in r.stdout, r.stdout + r.stderr
+
+
+@pytest.mark.gpu
+def test_bk_caller_passes_on_this_library():
+    """The unmodified caller's known-answer check on the GPU path: info == 8
+    from delayed_sytrf and delayed_sytrf_blocked, both reconstructions within
+    100 u rank, LAPACK's as well."""
+    r = subprocess.run([str(_binary("bk_example_on_b200"))], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0 and PASS_LINE in r.stdout, r.stdout + r.stderr
