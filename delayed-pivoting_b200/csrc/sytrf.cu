@@ -708,12 +708,8 @@ int sytrf_device(int n, double* d_a, int lda, int* perm, int* piv_size, int* inf
   const size_t total = b_wt + 2 * b_vec + b_cp + b_rp + 2 * b_int + align256(sizeof(bk::State));
   char* ws = nullptr;
   if (cudaMallocAsync((void**)&ws, total, s) != cudaSuccess) return kAllocationFailed;
-  bk::State* h = nullptr;
-  if (cudaHostAlloc((void**)&h, sizeof(bk::State), cudaHostAllocDefault) != cudaSuccess) {
-    cudaFreeAsync(ws, s);
-    cudaStreamSynchronize(s);
-    return kAllocationFailed;
-  }
+  bk::State hs;  // the panel kernel's state, read after each launch (a few bytes)
+  bk::State* h = &hs;
   bk::Params P;
   char* c = ws;
   P.wt = (double*)c;
@@ -804,7 +800,6 @@ int sytrf_device(int n, double* d_a, int lda, int* perm, int* piv_size, int* inf
     g_bk_report.max_closeness = h->closest;
     g_bk_report.info = e;
   }
-  cudaFreeHost(h);
   return status;
 }
 
