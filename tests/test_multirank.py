@@ -91,3 +91,24 @@ def test_reference_arm_prints_on_rank_zero_only(rank, prints):
     else:
         assert lines == []
 
+
+
+@pytest.mark.parametrize("rank,prints", [(0, True), (1, False)])
+def test_sytrf_reference_arm_prints_on_rank_zero_only(rank, prints):
+    """The LDL^T reference arm (the reference's delayed_sytrf_blocked, or its
+    restatement) runs and prints on rank 0 alone; other ranks exit 0."""
+    env = dict(os.environ, RANK=str(rank), WORLD_SIZE="2", LOCAL_RANK=str(rank))
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference",
+                        "--workload", "sytrf", "--gpus", "2", "--cpu-n", "256", "--steps", "1",
+                        "--warmup", "0"],
+                       env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if prints:
+        assert len(lines) == 1
+        line = json.loads(lines[0])
+        assert line["impl"] == "reference" and line["value"] > 0
+        assert line["cpu_baseline"]["kind"] in ("reference", "port")
+        assert line["e2e"]["h2d_bytes_per_step"] == 0
+    else:
+        assert lines == []
