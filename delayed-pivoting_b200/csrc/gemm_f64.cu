@@ -78,11 +78,20 @@ dgemm_minus_kernel(int M, int N, int K, const double* __restrict__ A, long long 
   const int lane = tid & 31, warp = tid >> 5;
   const int wm = warp / C::WARPS_N, wn = warp % C::WARPS_N;
   const int g = lane >> 2, t = lane & 3;
-  const long long m0 = (long long)blockIdx.x * C::BM;
-  const long long n0 = (long long)blockIdx.y * C::BN;
-  // Lower mode (M == N, C symmetric, its lower triangle only): tiles wholly
-  // above the diagonal have nothing to do.
-  if (lower && m0 + C::BM <= n0) return;
+  long long m0, n0;
+  if (lower) {
+    // Lower mode (M == N, C symmetric, its lower triangle only; BM == BN): a
+    // 1-D grid over the tiles (bi, bj) with bj <= bi, t = bi (bi + 1) / 2 + bj.
+    const long long t = blockIdx.x;
+    long long bi = (long long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((bi + 1) * (bi + 2) / 2 <= t) ++bi;
+    while (bi * (bi + 1) / 2 > t) --bi;
+    m0 = bi * C::BM;
+    n0 = (t - bi * (bi + 1) / 2) * C::BN;
+  } else {
+    m0 = (long long)blockIdx.x * C::BM;
+    n0 = (long long)blockIdx.y * C::BN;
+  }
 
   // Prefetch this CTA's C tile into L2 (128-byte lines, in-bounds only).
   {
@@ -200,6 +209,14 @@ void launch(int M, int N, int K, const double* A, long long lda, const double* B
             double* Cm, long long ldc, cudaStream_t s, const int* gate, bool lower = false) {
   dp::ensure_smem((const void*)dgemm_minus_kernel<C>, C::SMEM);
   dim3 grid((M + C::BM - 1) / C::BM, (N + C::BN - 1) / C::BN);
+  if (lower) {  // the lower-triangle tile grid needs square tiles
+    if constexpr (C::BM == C::BN) {
+      const unsigned nt = grid.x;
+      grid = dim3(nt * (nt + 1) / 2);
+    } else {
+      return;
+    }
+  }
   dp::note_launch();
   dgemm_minus_kernel<C>
       <<<grid, C::THREADS, C::SMEM, s>>>(M, N, K, A, lda, B, ldb, Cm, ldc, gate, lower);
@@ -268,7 +285,8 @@ void launch_gemm_minus(int M, int N, int K, const double* A, long long lda, cons
 
 // Lower triangle of the symmetric N x N block C -= A(N x K) * B(K x N), the
 // strict upper triangle of C untouched (the LDL^T trailing update, where
-// A B = L D L^T is symmetric); 64 x 64 tiles, those above the diagonal exit.
+// A B = L D L^T is symmetric); 64 x 64 tiles, only those on or below the
+// diagonal launched.
 void launch_gemm_minus_lower(int N, int K, const double* A, long long lda, const double* B,
                              long long ldb, double* C, long long ldc, cudaStream_t s) {
   if (N <= 0 || K <= 0) return;
