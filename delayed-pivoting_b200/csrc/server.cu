@@ -322,8 +322,10 @@ void dp_server::large_worker() {
     std::shared_ptr<Resident> keep;
     if (r0.factor_id == 0) {
       Factor* f = nullptr;
-      const int status =
-          dp::factor_create(&f, r0.n, r0.d_a, r0.lda, opt.precision, st, opt.panel_rows);
+      // mixed factors only from mixed_min_n up, where they are faster than FP64
+      const int prec = opt.mixed_min_n < 0 || r0.n >= opt.mixed_min_n ? opt.precision
+                                                                       : DP_PRECISION_FP64;
+      const int status = dp::factor_create(&f, r0.n, r0.d_a, r0.lda, prec, st, opt.panel_rows);
       out[0].status = status;
       out[0].info = f ? f->info : -1;
       if (f) out[0].factor_ms = f->factor_ms;
@@ -716,6 +718,10 @@ void dp_server::small_worker() {
   cudaStreamDestroy(st);
 }
 
+// Default order from which a mixed server factors in mixed precision (the
+// measured crossover of factor + refined solve against FP64 on B200).
+constexpr int kMixedMinN = 12288;
+
 extern "C" {
 
 void dp_server_options_init(dp_server_options* o) {
@@ -728,6 +734,7 @@ void dp_server_options_init(dp_server_options* o) {
   o->small_max_batch = 2048;
   o->max_iter = 10;
   o->tol = 1e-14;
+  o->mixed_min_n = kMixedMinN;
 }
 
 double dp_server_clock(void) { return clock_s(); }
@@ -744,11 +751,12 @@ int dp_server_create(dp_server** out, const dp_server_options* opt) {
     if (o.small_max_batch == 0) o.small_max_batch = 2048;
     if (o.max_iter == 0) o.max_iter = 10;
     if (o.tol == 0.0) o.tol = 1e-14;
+    if (o.mixed_min_n == 0) o.mixed_min_n = kMixedMinN;
   }
   if (o.large_workers == 0) o.large_workers = 6;
   if (!dp::valid_precision(o.precision) ||
       o.large_workers < 1 || o.large_workers > 64 || o.small_max_n > DP_BATCH_MAX_N ||
-      o.panel_rows < 0 ||
+      o.panel_rows < 0 || o.mixed_min_n < -1 ||
       o.small_max_batch < 1 || o.max_iter < 0 || !(o.tol > 0.0))
     return DP_INVALID_ARGUMENT;
   auto* s = new (std::nothrow) dp_server;

@@ -86,7 +86,8 @@ class ServerOptions(ctypes.Structure):
         ("max_iter", ctypes.c_int),
         ("tol", ctypes.c_double),
         ("panel_rows", ctypes.c_int),
-        ("reserved", ctypes.c_int * 3),
+        ("mixed_min_n", ctypes.c_int),
+        ("reserved", ctypes.c_int * 2),
     ]
 
 

@@ -291,7 +291,12 @@ typedef struct dp_server_options {
   double tol;          /* backward-error target; 0: 1e-14 */
   int panel_rows;      /* rows per CTA of the large factorisations' cluster panels (fewer CTAs
                           per panel: less SM time, more latency); 0: the library default (256) */
-  int reserved[3];
+  int mixed_min_n;     /* with a mixed `precision`, blocked factorisations of a lower order use
+                          FP64 factors: measured on B200, the BF16-split update and its
+                          refinement cost more than the FP64 factorisation below n ~ 12,000
+                          (factor + refined solve, kappa <= 1e4: 8192 -> 39.6 against 38.4 ms,
+                          12288 -> 69 against 81 ms); 0: 12288, -1: every order mixed */
+  int reserved[2];
 } dp_server_options;
 
 void dp_server_options_init(dp_server_options *opt);

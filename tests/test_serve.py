@@ -23,6 +23,15 @@ def test_server_options_defaults():
     assert o.budget_bytes == 160 << 30
     assert o.precision == dp.PRECISION_MIXED_BF16X6
     assert o.small_max_n == dp.BATCH_MAX_N and o.max_iter == 10 and o.tol == TOL
+    assert o.mixed_min_n == 12288  # mixed factors only where they beat FP64
+
+
+def test_server_rejects_bad_mixed_min_n_before_device_work():
+    import ctypes
+
+    h = ctypes.c_void_p()
+    o = dp.server_options(mixed_min_n=-2)
+    assert dp.lib().dp_server_create(ctypes.byref(h), ctypes.byref(o)) == dp.INVALID_ARGUMENT
 
 
 # ---------------------------------------------------------------- GPU ----
@@ -171,7 +180,8 @@ SIZES = [16, 40, 64, 100, 200, 300, 511, 513, 700, 1200, 37, 450, 900]
 def test_server_mixed_stream(precision):
     torch = _torch()
     reqs = make_requests(torch, 3, SIZES, [1e2, 1e5, 1e10])
-    srv = dp.Server(precision=precision, large_workers=3)
+    # mixed factors for every blocked order (the default keeps FP64 below 12288)
+    srv = dp.Server(precision=precision, large_workers=3, mixed_min_n=-1)
     out = run_server(srv, reqs)
     st = srv.stats()
     srv.close()
@@ -194,6 +204,26 @@ def test_server_mixed_stream(precision):
 
 
 @pytest.mark.gpu
+def test_server_routes_orders_below_mixed_min_n_to_fp64():
+    """A mixed server factors blocked requests of order < mixed_min_n in FP64
+    and the others in mixed precision; both meet the backward-error target."""
+    torch = _torch()
+    reqs = make_requests(torch, 9, [600, 900], [1e2])
+    srv = dp.Server(precision=dp.PRECISION_MIXED_BF16X6, large_workers=2, mixed_min_n=800)
+    out = run_server(srv, reqs)
+    srv.close()
+    for q in reqs:
+        r0 = out[q["id"]][0]
+        assert r0.status == 0 and r0.backward_error <= TOL
+        want = dp.PRECISION_FP64 if q["n"] < 800 else dp.PRECISION_MIXED_BF16X6
+        assert r0.precision == want, (q["n"], r0.precision)
+    srv = dp.Server(precision=dp.PRECISION_MIXED_BF16X6, large_workers=2)  # default 12288
+    out = run_server(srv, make_requests(torch, 10, [900], [1e2]))
+    srv.close()
+    assert all(r.precision == dp.PRECISION_FP64 for r, _ in out.values())
+
+
+@pytest.mark.gpu
 def test_server_result_alone_equals_result_in_mix():
     """Each request alone (submitted and awaited one by one: no follow-up is
     coalesced) and in the mix (all at once: a factorisation's follow-ups are
@@ -204,7 +234,7 @@ def test_server_result_alone_equals_result_in_mix():
     coalescing) stay bitwise equal."""
     torch = _torch()
     reqs = make_requests(torch, 5, SIZES, [1e3, 1e6, 1e10])
-    srv = dp.Server(precision=dp.PRECISION_MIXED_BF16X6, large_workers=4)
+    srv = dp.Server(precision=dp.PRECISION_MIXED_BF16X6, large_workers=4, mixed_min_n=-1)
     alone = run_server(srv, reqs, together=False)
     mix = run_server(srv, reqs, together=True)
     srv.close()
