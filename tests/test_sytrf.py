@@ -100,6 +100,25 @@ def test_oracle_against_reference_on_fresh_inputs(seed):
     assert np.abs(f - g).max() <= 1e-10 * max(1.0, np.abs(g).max())
 
 
+@pytest.mark.skipif(not orc.ref_bk_available(), reason="reference build absent")
+def test_oracle_against_reference_random_sweep():
+    """60 seeded shapes (n 1..129, lda n..n+3, 0-3 zero nodes, 30 % with a
+    cleared diagonal): the restatement's records equal the compiled
+    reference's delayed_sytrf_blocked on every one."""
+    rng = np.random.default_rng(5)
+    for c in range(60):
+        n = int(rng.integers(1, 130))
+        lda = n + int(rng.integers(0, 4))
+        z = tuple(sorted({int(x) for x in rng.integers(0, n, size=int(rng.integers(0, 4)))}))
+        a = orc.sym_matrix(n, 1000 + c, lda, z, bool(rng.random() < 0.3))
+        f, g = a.copy(order="F"), a.copy(order="F")
+        r_or = orc.oracle_sytrf(f)
+        r_ref = orc.ref_sytrf(g, "blocked")
+        assert r_or[2] == r_ref[2], (c, n)
+        np.testing.assert_array_equal(r_or[0], r_ref[0])
+        np.testing.assert_array_equal(r_or[1], r_ref[1])
+
+
 def test_c_abi_argument_checks_need_no_device():
     import delayed_pivoting as dp
 
