@@ -51,6 +51,10 @@ sys.path.insert(0, str(ROOT / "delayed-pivoting_b200"))
 # ncu on B200: DRAM bytes (read + write) of one dgemm_minus_kernel launch on
 # an 8192 x 8192 x 256 update per algorithmic byte (16 M N + 8 K (M + N)).
 DMMA_DRAM_PER_ALGORITHMIC_BYTE = 1060.07e6 / 1107.30e6
+# ncu on B200: DRAM bytes of one bk_panel_kernel launch (n = 4096, 64 columns
+# over 3781 rows: 28.153 GB/s x 419.52 us) per algorithmic byte (32 B per row
+# per factored column).
+BK_PANEL_DRAM_PER_ALGORITHMIC_BYTE = (28.153166e9 * 419.52e-6) / (32.0 * 64 * 3781)
 
 
 def lu_metric(n):
@@ -1696,7 +1700,11 @@ def run_sytrf(args):
                 "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks.get("hbm_gbs")
                 else "fallback 6650 GB/s (MEASURED_PEAKS.json absent)",
-                "traffic": None, "algorithmic_bytes_per_launch": panel_bytes,
+                "traffic": panel_bytes * BK_PANEL_DRAM_PER_ALGORITHMIC_BYTE,
+                "traffic_source": "ncu dram__bytes of one n = 4096 panel launch "
+                                  "(profiles/bk_panel_kernel_sytrf_n4096.md), scaled by the "
+                                  "launch's algorithmic bytes",
+                "algorithmic_bytes_per_launch": panel_bytes,
                 "avg_launch_ms": panel_avg_ms, "launches_timed": stats["launches"][0],
                 "note": "latency-bound: every pivot step is 2-3 grid barriers with a decision "
                         "between them; bytes are 32 per row per factored column"}
