@@ -1508,10 +1508,11 @@ def sytrf_flops(n):
     return float(n) ** 3 / 3.0
 
 
-def cpu_sytrf_gflops(n, seed, threads):
+def cpu_sytrf_gflops(n, seed, threads, variant="blocked"):
     """The reference's delayed_sytrf_blocked (delayed-bunch-kaufman/, compiled
-    into oracle/_ref/) on the host cores; the C restatement ('port') when the
-    reference was not built.  Returns (GFLOP/s, seconds, kind, info)."""
+    into oracle/_ref/; `variant` "lapack": its LAPACK dsytrf wrapper) on the
+    host cores; the C restatement ('port') when the reference was not built.
+    Returns (GFLOP/s, seconds, kind, info)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as orc
     import delayed_pivoting as dp
@@ -1519,7 +1520,7 @@ def cpu_sytrf_gflops(n, seed, threads):
     a = dp.symmetric_matrix(n, seed)
     t0 = time.perf_counter()
     if orc.ref_bk_available():
-        _, _, info = orc.ref_sytrf(a, "blocked", threads=threads)
+        _, _, info = orc.ref_sytrf(a, variant, threads=threads)
         kind = "reference"
     else:
         _, _, info = orc.oracle_sytrf(a)
@@ -1717,6 +1718,12 @@ def run_sytrf(args):
         cpu = {"value": gc, "unit": UNIT, "cores": threads, "kind": kind,
                "sample": f"one delayed_sytrf_blocked of n={args.cpu_n} (seeded N(0,1) symmetric),"
                          f" {tc:.2f} s, OpenBLAS {threads} threads"}
+        if kind == "reference":
+            gl, tl, _, _ = cpu_sytrf_gflops(args.cpu_n, args.seed, threads, "lapack")
+            cpu["lapack_dsytrf"] = {"value": gl, "unit": UNIT, "cores": threads,
+                                    "sample": f"LAPACK dsytrf('L') + dsyconv through the "
+                                              f"reference's lapack_sytrf, same n={args.cpu_n} "
+                                              f"matrix, {tl:.2f} s"}
         n1 = max(256, args.cpu_n // 2)
         g1, t1, kind1, _ = cpu_sytrf_gflops(n1, args.seed, 1)
         cpu["one_thread"] = {"value": g1, "unit": UNIT, "cores": 1, "kind": kind1,
@@ -1779,6 +1786,12 @@ def sytrf_reference_arm(args):
             times.append(t)
     tot = sum(times)
     value = sytrf_flops(n) * len(times) / tot / 1e9
+    lapack = None
+    if kind == "reference":
+        gl, tl, _, _ = cpu_sytrf_gflops(n, args.seed, threads, "lapack")
+        lapack = {"value": gl, "unit": UNIT, "cores": threads, "seconds": tl,
+                  "sample": f"LAPACK dsytrf('L') + dsyconv through the reference's lapack_sytrf, "
+                            f"n={n}"}
     line = {
         "impl": "reference", "metric": sytrf_metric(args.n), "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -1788,7 +1801,8 @@ def sytrf_reference_arm(args):
                    "threads": threads},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
                          "sample": f"one delayed_sytrf_blocked of n={n} per step (bounded sample "
-                                   f"of the n={args.n} workload), OpenBLAS {threads} threads"},
+                                   f"of the n={args.n} workload), OpenBLAS {threads} threads",
+                         "lapack_dsytrf": lapack},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

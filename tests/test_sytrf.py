@@ -144,6 +144,34 @@ def test_c_abi_argument_checks_need_no_device():
     assert st == dp.SUCCESS and info0 == 0
 
 
+def test_host_and_cxx_entry_points_reject_bad_arguments_without_a_device():
+    """dp_sytrf_host and the C++ drop-in delayed_sytrf(_blocked) check their
+    arguments before any device work; the drop-ins set info = -1 like the
+    reference (delayed_sytrf.hpp:13)."""
+    import delayed_pivoting as dp
+
+    L = dp.lib()
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.dp_sytrf_host.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ip, ip, ip]
+    a = np.zeros((4, 4), order="F")
+    perm = np.zeros(4, np.int32)
+    piv = np.zeros(4, np.int32)
+    info = ctypes.c_int(5)
+    P, Q = perm.ctypes.data_as(ip), piv.ctypes.data_as(ip)
+    assert L.dp_sytrf_host(-1, a.ctypes.data, 4, P, Q, ctypes.byref(info)) == dp.INVALID_ARGUMENT
+    assert info.value == -1
+    assert L.dp_sytrf_host(4, a.ctypes.data, 3, P, Q, ctypes.byref(info)) == dp.INVALID_ARGUMENT
+    assert L.dp_sytrf_host(4, None, 4, P, Q, ctypes.byref(info)) == dp.INVALID_ARGUMENT
+    for sym in ("_Z13delayed_sytrfiPdiPiS0_Ri", "_Z21delayed_sytrf_blockediPdiPiS0_Ri"):
+        f = getattr(L, sym)
+        f.restype = None
+        f.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ip, ip, ip]  # int& as pointer
+        for n, lda in ((-1, 1), (4, 3)):
+            info = ctypes.c_int(5)
+            f(n, a.ctypes.data, lda, P, Q, ctypes.byref(info))
+            assert info.value == -1, (sym, n, lda)
+
+
 def test_cxx_drop_in_symbols_exported():
     import subprocess
 
