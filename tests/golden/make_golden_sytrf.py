@@ -4,7 +4,8 @@ delayed_sytrf_blocked.cpp and delayed_sytrf.cpp, compiled unmodified into
 oracle/_ref/libref_delayed_bk.so against OpenBLAS).  Run from the repository
 root:
 
-    python tests/golden/make_golden_sytrf.py
+    python tests/golden/make_golden_sytrf.py            # the 15 fixtures below
+    python tests/golden/make_golden_sytrf.py --large    # also large/sym_16384.npz
 
 Each case is written to tests/golden/sytrf/<name>.npz with the input's recipe
 (size, leading dimension, generator seed, zeroed nodes, cleared diagonal, or
@@ -12,9 +13,15 @@ the reference's own rank-8 known-answer matrix), the blocked reference's
 perm / piv_size / info, and the largest |P A P^T - L D L^T|.  The unblocked
 reference must give the same records, or the case is rejected (it would be
 order-sensitive between two builds of the reference itself).
+
+--large writes tests/golden/sytrf/large/sym_16384.npz from the blocked
+reference alone (the unblocked one, BLAS-2 throughout, is impractically slow
+at that order); with --check-oracle the restatement is run on it as well
+(about a quarter of an hour on 8 cores) and must give the same records.
 """
 from __future__ import annotations
 
+import argparse
 import sys
 from pathlib import Path
 
@@ -46,7 +53,33 @@ CASES = [
 ]
 
 
+def large(check_oracle: bool) -> None:
+    out = OUT / "large"
+    out.mkdir(parents=True, exist_ok=True)
+    n = 16384
+    a = orc.sym_matrix(n, n)
+    f = a.copy(order="F")
+    perm, piv, info = orc.ref_sytrf(f, "blocked")
+    del f
+    if check_oracle:
+        g = a.copy(order="F")
+        p2, v2, i2 = orc.oracle_sytrf(g)
+        if not (np.array_equal(perm, p2) and np.array_equal(piv, v2) and info == i2):
+            raise SystemExit("sym_16384: the restatement's records differ from the reference's")
+    np.savez_compressed(out / f"sym_{n}.npz", perm=perm, piv_size=piv, info=np.int32(info),
+                        n=n, lda=n, seed=n, zero_nodes=np.zeros(0, np.int32), zero_diag=False,
+                        rank8=False, max_error=np.float64(np.nan))
+    print(f"large/sym_{n}: info={info} 2x2={int((piv == 2).sum())}")
+
+
 def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--large", action="store_true")
+    ap.add_argument("--check-oracle", action="store_true")
+    args = ap.parse_args()
+    if args.large:
+        large(args.check_oracle)
+        return
     OUT.mkdir(exist_ok=True)
     cases = [(name, dict(n=n, lda=lda, seed=seed, zero_nodes=np.array(z, dtype=np.int32),
                          zero_diag=zd, rank8=False))

@@ -226,6 +226,30 @@ def test_gpu_records_match_reference(built, name):
 
 
 @pytest.mark.gpu
+def test_gpu_records_match_reference_n16384(built):
+    """The seeded 16384 x 16384 symmetric matrix (2 GiB) against the
+    reference's records (tests/golden/sytrf/large/sym_16384.npz, written by
+    its delayed_sytrf_blocked; the restatement gives the same records), with
+    no order-sensitive decision."""
+    import delayed_pivoting as dp
+
+    torch = _torch()
+    g = np.load(GOLDEN / "large" / "sym_16384.npz")
+    n = int(g["n"])
+    a = dp.symmetric_matrix(n, int(g["seed"]))
+    d = torch.from_numpy(np.ascontiguousarray(a.T)).cuda()
+    del a
+    st, perm, piv, info = dp.sytrf_device(n, d, n)
+    rep = dp.sytrf_last_report()
+    del d
+    torch.cuda.empty_cache()
+    assert st == dp.SUCCESS and rep["near_ties"] == 0, rep
+    assert info == int(g["info"])
+    np.testing.assert_array_equal(perm, g["perm"])
+    np.testing.assert_array_equal(piv, g["piv_size"])
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("nb,grid", [(2, 0), (3, 4), (17, 8), (64, 5), (48, 0), (64, 148),
                                      (64, 16)])
 def test_gpu_panel_width_and_grid_keep_records(built, nb, grid):
