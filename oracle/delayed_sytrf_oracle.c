@@ -59,24 +59,31 @@ static void swap_nodes(int n, double *a, int lda, int x, int y, int *perm, doubl
 }
 
 /* materialize_current_column, :75-88: column `col` (rows col..n-1) of the
- * matrix with this panel's update applied, A(:,col) - L_panel W(col,:)^T. */
+ * matrix with this panel's update applied, A(:,col) - L_panel W(col,:)^T.
+ * `acc` (n doubles): each row's sum over the panel columns, accumulated in
+ * column order j = 0, 1, ... with the rows contiguous in the inner loop. */
 static void mat_column(int n, const double *a, int lda, int pb, int pw, const double *w, int ldw,
-                       int col, double *out) {
-  for (int r = col; r < n; ++r) {
-    double s = 0.0;
-    for (int j = 0; j < pw; ++j) s += a[IDX(r, pb + j, lda)] * w[IDX(col, j, ldw)];
-    out[r] = a[IDX(r, col, lda)] - s;
+                       int col, double *out, double *acc) {
+  for (int r = col; r < n; ++r) acc[r] = 0.0;
+  for (int j = 0; j < pw; ++j) {
+    const double wj = w[IDX(col, j, ldw)];
+    const double *lj = a + IDX(0, pb + j, lda);
+    for (int r = col; r < n; ++r) acc[r] += lj[r] * wj;
   }
+  for (int r = col; r < n; ++r) out[r] = a[IDX(r, col, lda)] - acc[r];
 }
 
-/* materialize_active_row, :90-106: row `row` over the active columns. */
+/* materialize_active_row, :90-106: row `row` over the active columns
+ * (sums accumulated as in mat_column). */
 static void mat_row(const double *a, int lda, int pb, int pw, const double *w, int ldw, int b,
-                    int e, int row, double *out) {
-  for (int c = b; c < e; ++c) {
-    double s = 0.0;
-    for (int j = 0; j < pw; ++j) s += a[IDX(c, pb + j, lda)] * w[IDX(row, j, ldw)];
-    out[c] = sym_lower(a, lda, row, c) - s;
+                    int e, int row, double *out, double *acc) {
+  for (int c = b; c < e; ++c) acc[c] = 0.0;
+  for (int j = 0; j < pw; ++j) {
+    const double wj = w[IDX(row, j, ldw)];
+    const double *lj = a + IDX(0, pb + j, lda);
+    for (int c = b; c < e; ++c) acc[c] += lj[c] * wj;
   }
+  for (int c = b; c < e; ++c) out[c] = sym_lower(a, lda, row, c) - acc[c];
 }
 
 /* stable_2x2, :108-124. */
@@ -101,19 +108,29 @@ static int first_absmax(int n, const double *x) {
 }
 
 /* finish_panel, :126-139: lower triangle of the trailing block minus
- * (L W^T + W L^T) / 2 over the panel's columns. */
+ * (L W^T + W L^T) / 2 over the panel's columns; per element the sum runs over
+ * j = 0, 1, ... (rows contiguous in the inner loop, one sum array per
+ * column). */
 static void finish_panel(int n, double *a, int lda, int begin, int end, const double *w,
                          int ldw) {
   const int width = end - begin;
   if (width <= 0 || n - end <= 0) return;
-#pragma omp parallel for schedule(dynamic, 16)
-  for (int c = end; c < n; ++c)
-    for (int r = c; r < n; ++r) {
-      double s = 0.0;
-      for (int j = 0; j < width; ++j)
-        s += a[IDX(r, begin + j, lda)] * w[IDX(c, j, ldw)] + w[IDX(r, j, ldw)] * a[IDX(c, begin + j, lda)];
-      a[IDX(r, c, lda)] -= 0.5 * s;
+#pragma omp parallel
+  {
+    double *acc = malloc(sizeof(double) * (size_t)n);
+#pragma omp for schedule(dynamic, 16)
+    for (int c = end; c < n; ++c) {
+      if (!acc) continue;
+      for (int r = c; r < n; ++r) acc[r] = 0.0;
+      for (int j = 0; j < width; ++j) {
+        const double wc = w[IDX(c, j, ldw)], ac = a[IDX(c, begin + j, lda)];
+        const double *lj = a + IDX(0, begin + j, lda), *wj = w + IDX(0, j, ldw);
+        for (int r = c; r < n; ++r) acc[r] += lj[r] * wc + wj[r] * ac;
+      }
+      for (int r = c; r < n; ++r) a[IDX(r, c, lda)] -= 0.5 * acc[r];
     }
+    free(acc);
+  }
 }
 
 /* delayed_sytrf_blocked, :141-358, with the panel width as a parameter
@@ -127,13 +144,17 @@ int oracle_sytrf(int n, double *a, int lda, int *perm, int *piv_size, int nb) {
   double *c0 = calloc((size_t)n, sizeof(double));
   double *c1 = calloc((size_t)n, sizeof(double));
   double *rv = calloc((size_t)n, sizeof(double));
-  if (!w || !c0 || !c1 || !rv) { free(w); free(c0); free(c1); free(rv); return -1; }
+  double *acc = calloc((size_t)n, sizeof(double));
+  if (!w || !c0 || !c1 || !rv || !acc) {
+    free(w); free(c0); free(c1); free(rv); free(acc);
+    return -1;
+  }
 
   int pb = 0, e = n;
   while (pb < e) {
     int k = pb, pw = 0;
     while (k < e && pw < nb) {
-      mat_column(n, a, lda, pb, pw, w, ldw, k, c0);
+      mat_column(n, a, lda, pb, pw, w, ldw, k, c0, acc);
       const double akk = fabs(c0[k]);
       int p = k;
       double colmax = 0.0;
@@ -147,7 +168,7 @@ int oracle_sytrf(int n, double *a, int lda, int *perm, int *piv_size, int nb) {
       } else if (akk >= kAlpha * colmax) {
         one = 1; /* criterion 1 (:200-202) */
       } else {
-        mat_row(a, lda, pb, pw, w, ldw, k, e, p, rv);
+        mat_row(a, lda, pb, pw, w, ldw, k, e, p, rv, acc);
         double rowmax = 0.0;
         for (int c = k; c < e; ++c)
           if (c != p) rowmax = fmax(rowmax, fabs(rv[c]));
@@ -169,7 +190,7 @@ int oracle_sytrf(int n, double *a, int lda, int *perm, int *piv_size, int nb) {
       if (one) { /* :250-272 */
         if (piv != k) {
           swap_nodes(n, a, lda, k, piv, perm, w, ldw, pw);
-          mat_column(n, a, lda, pb, pw, w, ldw, k, c0);
+          mat_column(n, a, lda, pb, pw, w, ldw, k, c0, acc);
         }
         const double d = c0[k];
         a[IDX(k, k, lda)] = d;
@@ -184,8 +205,8 @@ int oracle_sytrf(int n, double *a, int lda, int *perm, int *piv_size, int nb) {
       }
       /* 2x2 block, :274-330 */
       swap_nodes(n, a, lda, k + 1, piv, perm, w, ldw, pw);
-      mat_column(n, a, lda, pb, pw, w, ldw, k, c0);
-      mat_column(n, a, lda, pb, pw, w, ldw, k + 1, c1);
+      mat_column(n, a, lda, pb, pw, w, ldw, k, c0, acc);
+      mat_column(n, a, lda, pb, pw, w, ldw, k + 1, c1, acc);
       const double d00 = c0[k], d10 = c0[k + 1], d11 = c1[k + 1];
       a[IDX(k, k, lda)] = d00;
       a[IDX(k + 1, k, lda)] = d10;
@@ -212,6 +233,6 @@ int oracle_sytrf(int n, double *a, int lda, int *perm, int *piv_size, int nb) {
     finish_panel(n, a, lda, pb, k, w, ldw);
     pb = k;
   }
-  free(w); free(c0); free(c1); free(rv);
+  free(w); free(c0); free(c1); free(rv); free(acc);
   return e;
 }

@@ -17,7 +17,7 @@ order-sensitive between two builds of the reference itself).
 --large writes tests/golden/sytrf/large/sym_16384.npz from the blocked
 reference alone (the unblocked one, BLAS-2 throughout, is impractically slow
 at that order); with --check-oracle the restatement is run on it as well
-(about a quarter of an hour on 8 cores) and must give the same records.
+(a few minutes on 8 cores) and must give the same records.
 """
 from __future__ import annotations
 
