@@ -1,7 +1,7 @@
 """Benchmark of the B200 delayed-pivoting LU.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload serve|lu|batched|ir|stream|update|sytrf]
+                    [--workload serve|lu|batched|ir|stream|update|sytrf|front]
 
 Workloads (one JSON line on rank 0 each run):
 
@@ -23,6 +23,9 @@ batched  one persistent launch (CUDA graph) factoring 8192 matrices, n
 sytrf  one delayed Bunch-Kaufman LDL^T (delayed_sytrf_blocked's semantics) of
     an n x n symmetric N(0,1) matrix, n^3/3 / t in GFLOP/s; the reference arm
     times the reference's delayed_sytrf_blocked on the host cores.
+front  one multifrontal hand-off (dp_front_factor) of an n x n front with n/2
+    fully-summed rows / columns, partial-LU flops / t in GFLOP/s; the
+    reference has no code for it, so its arm reports "unavailable".
 
 Inputs are generated once (seeded), kept resident in HBM and restored by a
 device copy before every step, outside the timed region; every step's inputs
@@ -88,7 +91,8 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "mixed3"],
                     help="trailing-update arithmetic of the lu workload: FP64, BF16x6, BF16x3")
     ap.add_argument("--workload", default="serve",
-                    choices=["serve", "lu", "batched", "ir", "stream", "update", "sytrf"])
+                    choices=["serve", "lu", "batched", "ir", "stream", "update", "sytrf",
+                             "front"])
     ap.add_argument("--k", type=int, default=256, help="update: inner dimension (outer block)")
     ap.add_argument("--loads", default="0.5,0.7,0.9",
                     help="stream: offered loads as fractions of the measured mixed capacity")
@@ -248,6 +252,8 @@ def run_reference_arm(args):
         return batched_reference_arm(args)
     if args.workload == "sytrf":
         return sytrf_reference_arm(args)
+    if args.workload == "front":
+        return front_reference_arm(args)
     if args.workload == "ir":
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no solve or "
                           "refinement path (delayed_getrf factorises only)"}), flush=True)
@@ -294,6 +300,8 @@ def main():
         return run_update(args)
     if args.workload == "sytrf":
         return run_sytrf(args)
+    if args.workload == "front":
+        return run_front(args)
     return run_lu(args)
 
 
@@ -1806,6 +1814,173 @@ def sytrf_reference_arm(args):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- front ----
+
+def front_metric(n, p):
+    return (f"multifrontal front: partial delayed LU of an {n} x {n} front over its {p} "
+            f"fully-summed rows / columns, GFLOP/s (partial-LU flops)")
+
+
+def front_flops(m, n, k):
+    """Multiply-adds x 2 of eliminating k pivots of an m x n front:
+    sum_{j<k} 2 (m - j - 1)(n - j - 1), to leading order."""
+    k = float(k)
+    return 2.0 * (m * n * k - (m + n) * k * k / 2.0 + k ** 3 / 3.0)
+
+
+def cpu_front_gflops(m, p, seed):
+    """The C restatement of the path (oracle_front: the reference's
+    delayed_getrf rules on the fully-summed block, NumPy for the rest; the
+    reference itself has no code for the hand-off) on the host cores."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+
+    rng = np.random.default_rng(seed)
+    f = np.asfortranarray(rng.standard_normal((m, m)))
+    t0 = time.perf_counter()
+    k, _, _, _ = orc.oracle_front(f, p)
+    t = time.perf_counter() - t0
+    return front_flops(m, m, k) / t / 1e9, t
+
+
+def run_front(args):
+    """One multifrontal hand-off per step: dp_front_factor on an n x n front
+    (N(0,1), torch Philox, seeded per rank) whose leading n / 2 rows and
+    columns are fully summed; the contribution block is F(k:n, k:n)."""
+    import torch
+    import delayed_pivoting as dp
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+
+        dist = dist_mod
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+    n = args.n
+    p = n // 2
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(args.seed + rank)
+    orig = torch.randn(n, n, dtype=torch.float64, device=dev, generator=gen)  # column-major front
+    work = torch.empty_like(orig)
+    stream = torch.cuda.current_stream(dev)
+    L = dp.lib()
+
+    def step():
+        work.copy_(orig)
+        rows = np.arange(n, dtype=np.int32)
+        cols = np.arange(n, dtype=np.int32)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st, k, _, _ = dp.front_factor(n, n, p, work, n, rows, cols, stream=stream)
+        e1.record(stream)
+        if st != 0:
+            raise RuntimeError(f"dp_front_factor: status {st}")
+        return e0, e1, k
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    events = []
+    l0 = L.dp_kernel_launches()
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        for _ in range(args.steps):
+            events.append(step())
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    launches = L.dp_kernel_launches() - l0
+    ms = sum(e0.elapsed_time(e1) for e0, e1, _ in events)
+    k = events[-1][2]
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    flops = front_flops(n, n, k)
+    value = world * flops * args.steps / (ms * 1e-3) / 1e9
+
+    e2e = None
+    if not args.no_e2e:
+        host = orig.cpu().pin_memory()
+        back = torch.empty_like(host).pin_memory()
+        kk = max(1, min(args.steps, 3))
+        e2e_ms = 0.0
+        for i in range(kk + 1):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            work.copy_(host, non_blocking=True)
+            st, _, _, _ = dp.front_factor(n, n, p, work, n, np.arange(n, dtype=np.int32),
+                                          np.arange(n, dtype=np.int32), stream=stream)
+            back.copy_(work, non_blocking=True)
+            e1.record(stream)
+            e1.synchronize()
+            if st != 0:
+                raise RuntimeError(f"dp_front_factor: status {st}")
+            if i:
+                e2e_ms += e0.elapsed_time(e1)
+        e2e_ms /= kk
+        if dist:
+            t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e = {"value": world * flops / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": n * n * 8, "d2h_bytes_per_step": n * n * 8,
+               "ms_per_step": e2e_ms,
+               "api": "dp_front_factor, the front copied from and back to pinned host memory"}
+    fp64 = fp64_peak_tflops(torch, dev)
+    achieved = value / world / 1e3
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        m1 = max(256, min(args.cpu_n, 4096) // 2)
+        gc, tc = cpu_front_gflops(m1, m1 // 2, args.seed)
+        cpu = {"value": gc, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": f"oracle_front (the C restatement of delayed_getrf on the fully-summed "
+                         f"block, NumPy / OpenBLAS for the rest) on a {m1} x {m1} front with "
+                         f"{m1 // 2} fully-summed rows, {tc:.2f} s"}
+    if rank == 0:
+        line = {
+            "metric": front_metric(n, p), "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: N(0,1) front (torch Philox, seeded per rank)",
+            "config": {"workload": f"dp_front_factor n={n} p={p} (single front)", "n": n, "p": p,
+                       "npiv": k, "parallelism": f"replicas x{world}",
+                       "l2": f"front {8 * n * n / 2**30:.2f} GiB > L2 (no flush needed)"},
+            "roofline": {"bound": "tensor", "kernel": "whole call (the DMMA Schur update "
+                         "dominates: partial-LU flops over the call's time)",
+                         "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
+                         "frac": achieved / fp64 if fp64 else None, "traffic": None,
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured live"},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "step_ms": [round(e0.elapsed_time(e1), 3) for e0, e1, _ in events],
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def front_reference_arm(args):
+    print(json.dumps({"impl": "reference", "unavailable": "the reference has no code for the "
+                      "multifrontal hand-off (its design document describes it, "
+                      "doc/...LU方法.md:228-457)"}, ensure_ascii=False), flush=True)
     return 0
 
 
