@@ -136,3 +136,27 @@ def test_extend_add_into_parent(built):
     torch.cuda.synchronize()
     got = dP.cpu().numpy().T
     assert np.abs(got - expect).max() <= 1e-13 * np.abs(expect).max()
+
+
+def test_bench_front_flops_and_reference_arm():
+    """bench.py --workload front: the partial-LU flop count matches the exact
+    sum over the eliminated pivots to leading order, and the reference arm
+    reports that the reference has no code for the hand-off."""
+    import importlib.util
+    import json
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    spec = importlib.util.spec_from_file_location("bench_mod", root / "bench.py")
+    b = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(b)
+    for m, n, k in ((400, 400, 200), (1000, 800, 300)):
+        exact = sum(2 * (m - j - 1) * (n - j - 1) for j in range(k))
+        assert abs(b.front_flops(m, n, k) / exact - 1.0) < 0.01
+    r = subprocess.run([sys.executable, str(root / "bench.py"), "--impl", "reference",
+                        "--workload", "front"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and "unavailable" in line
