@@ -309,19 +309,7 @@ def run_lu(args):
     import torch
     import delayed_pivoting as dp
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist_mod
-        from datetime import timedelta
-
-        dist = dist_mod
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
-                                device_id=dev)
+    world, rank, local, dev, dist = _dist_setup(torch)
 
     n = args.n
     w = workload(n)
